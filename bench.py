@@ -1,0 +1,387 @@
+#!/usr/bin/env python3
+"""Benchmark: S(q) + partials frames/s on the precision-form workload.
+
+Workload (the headline configuration): cubic box L = 220 A, N = 1,000,000 atoms,
+3 types (fractions 0.5 / 0.3 / 0.2, shuffled), uniform base positions plus a
+fresh Gaussian jitter (sigma 0.3 A) per frame, neutron weights b = 4.149, 5.803,
+9.45 fm, q_max = 6 1/A (423^3 modes), nq 500, norm mean, partials on, NUFFT
+tolerance 1e-6, FP32 spread / FFT / deconvolution with FP64 shell accumulation.
+One step = one frame through the hot path.  Synthetic data, seeded.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Under torchrun each rank runs its own frames (frames are independent units)
+and the accumulators are summed once at the end; the rank timings are reduced
+with MAX.  One JSON line is printed by rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "S(q) frames/s at N=1M (FP32 spread/FFT + FP64 accumulation, partials)"
+UNIT = "frames/s"
+N_ATOMS = 1_000_000
+BOX = 220.0
+FRACTIONS = (0.5, 0.3, 0.2)
+B_NEUTRON = (4.149, 5.803, 9.45)
+QMAX, NQ, EPS = 6.0, 500, 1e-6
+JITTER = 0.3
+SEED = 20240601
+
+
+def workload_types(rng):
+    # type_assignment of the reference generator: rounded counts, shuffled.
+    counts = [int(round(f * N_ATOMS)) for f in FRACTIONS[:-1]]
+    counts.append(N_ATOMS - sum(counts))
+    types = np.repeat(np.arange(1, len(FRACTIONS) + 1, dtype=np.int32), counts)
+    rng.shuffle(types)
+    return types
+
+
+def make_frames(nframes, seed):
+    rng = np.random.default_rng(seed)
+    types = workload_types(rng)
+    base = rng.random((N_ATOMS, 3)) * BOX
+    frames = np.empty((nframes, N_ATOMS, 3))
+    for f in range(nframes):
+        frames[f] = base + rng.normal(0.0, JITTER, (N_ATOMS, 3))
+    return types, frames
+
+
+def workload_config(extra=None):
+    cfg = {"workload": "precision form: cubic L=220 A, N=1e6, 3 types 0.5/0.3/0.2, "
+                       "uniform + per-frame N(0,0.3^2) jitter, neutron b=4.149/5.803/9.45 fm, "
+                       "qmax 6 (423^3 modes), nq 500, norm mean, partials, eps 1e-6",
+           "natoms": N_ATOMS, "box": BOX, "qmax": QMAX, "nq": NQ, "eps": EPS,
+           "modes": [423, 423, 423], "l2": "inputs larger than L2 (fine grids > 126 MB)"}
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.idx = device_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# measured peaks
+# ---------------------------------------------------------------------------
+def hbm_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def dram_traffic(kernel):
+    """Per-launch DRAM bytes of a kernel from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "dram_traffic.txt")
+    try:
+        for line in open(path):
+            parts = line.split()
+            if len(parts) >= 2 and not line.startswith("#") and parts[0] == kernel:
+                return float(parts[1])
+    except OSError:
+        pass
+    return None
+
+
+# ---------------------------------------------------------------------------
+# reference arm: the CPU restatement of the reference's CPU path
+# ---------------------------------------------------------------------------
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    cores = os.cpu_count() or 1
+    types, frames = make_frames(1, SEED)
+    w = O.Weights(kind=O.WEIGHT_NEUTRON, amp_const=np.array(B_NEUTRON))
+    cell = np.eye(3) * BOX
+    # one frame is ~10-30 s on a few host cores: run warm-up and steps on one
+    # frame each, at most a bounded number of them
+    t_est0 = time.perf_counter()
+    O.nufft_cpu_sq([frames[0]], types, cell, np.zeros(3), w, 0.0, QMAX, NQ, eps=EPS,
+                   sigma=1.25, workers=cores)
+    t_one = time.perf_counter() - t_est0
+    steps = max(1, min(args.steps, int(150.0 / max(t_one, 1e-3))))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        O.nufft_cpu_sq([frames[0]], types, cell, np.zeros(3), w, 0.0, QMAX, NQ, eps=EPS,
+                       sigma=1.25, workers=cores)
+    dt = time.perf_counter() - t0
+    v = steps / dt
+    sample = ("%d frame(s) of the workload through the CPU restatement of the reference's "
+              "FINUFFT CPU path (ES spread C/OpenMP, pocketfft rfftn, deconvolve + shell sums), "
+              "sigma 1.25, FP64" % steps)
+    print(json.dumps({
+        "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": steps,
+        "warmup": 1, "ms_per_step": 1e3 * dt / steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "impl": "reference", "config": workload_config({"parallelism": "cpu"}),
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def cpu_baseline_sample():
+    from oracle import oracle as O
+    cores = os.cpu_count() or 1
+    types, frames = make_frames(1, SEED)
+    w = O.Weights(kind=O.WEIGHT_NEUTRON, amp_const=np.array(B_NEUTRON))
+    t0 = time.perf_counter()
+    O.nufft_cpu_sq([frames[0]], types, np.eye(3) * BOX, np.zeros(3), w, 0.0, QMAX, NQ, eps=EPS,
+                   sigma=1.25, workers=cores)
+    dt = time.perf_counter() - t0
+    return {"value": 1.0 / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": "1 frame of the workload (N=1e6, 3 types, 423^3 modes) through the CPU "
+                      "restatement of the reference's FINUFFT CPU path, sigma 1.25, FP64, "
+                      "%d threads, %.1f s" % (cores, dt)}
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    from sqcalc_b200 import _lib, build
+
+    build.build()
+    torch.cuda.set_device(local_rank)
+    dist = world > 1
+    if dist:
+        import torch.distributed as td
+        td.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    K, W = args.steps, args.warmup
+    types, frames = make_frames(K + W, SEED + 7919 * rank)
+    prec = _lib.PREC_SINGLE if args.precision == "single" else _lib.PREC_DOUBLE
+    eps = EPS
+    stream = torch.cuda.current_stream()
+    # The plans run on torch's current stream, so torch CUDA events bracket them.
+    mk = lambda timing: _lib.Plan(np.eye(3).reshape(9) * BOX, np.zeros(3), types,  # noqa: E731
+                                  weight=_lib.WEIGHT_NEUTRON, amp_const=np.array(B_NEUTRON),
+                                  qmin=0.0, qmax=QMAX, nq=NQ, norm=_lib.NORM_MEAN,
+                                  partials=True, precision=prec, eps=eps, device=local_rank,
+                                  upsampfac=args.upsampfac, timing=timing,
+                                  stream=stream.cuda_stream)
+
+    # --- device-resident inputs: value --------------------------------------
+    dev = torch.from_numpy(frames).to(f"cuda:{local_rank}")
+    torch.cuda.synchronize()
+    plan = mk(False)
+    fbytes = N_ATOMS * 3 * 8
+    base = dev.data_ptr()
+    for f in range(W):
+        plan.accumulate((base + f * fbytes, 1), where=_lib.DEVICE)
+    plan.sync()
+    if dist:
+        td.barrier()
+    torch.cuda.synchronize()
+    launches0 = plan.launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        t_wall = time.perf_counter()
+        ev0.record(stream)
+        for f in range(W, W + K):
+            plan.accumulate((base + f * fbytes, 1), where=_lib.DEVICE)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        t_wall = time.perf_counter() - t_wall
+    launches = plan.launch_count() - launches0
+    info = plan.info
+    elapsed = ev0.elapsed_time(ev1) * 1e-3
+    if dist:
+        t = torch.tensor([elapsed], dtype=torch.float64, device=f"cuda:{local_rank}")
+        td.all_reduce(t, op=td.ReduceOp.MAX)
+        elapsed = float(t.item())
+    value = K * world / elapsed
+
+    # --- per-stage device times (CUDA events inside the library) -------------
+    tplan = mk(True)
+    for f in range(W):
+        tplan.accumulate((base + f * fbytes, 1), where=_lib.DEVICE)
+    tplan.reset()
+    for f in range(W, W + K):
+        tplan.accumulate((base + f * fbytes, 1), where=_lib.DEVICE)
+    st = tplan.stage_times()
+    tplan.close()
+    nfr = max(st["frames"], 1)
+    stage_ms = {k: st[k] / nfr for k in ("sort_ms", "spread_ms", "fft_ms", "bin_ms")}
+
+    # --- end to end through the C ABI with host buffers -------------------------
+    pinned = torch.from_numpy(frames).pin_memory()
+    pnum = torch.zeros(NQ, dtype=torch.float64).pin_memory()
+    e2e_plan = mk(False)
+    hbase = pinned.data_ptr()
+    import ctypes
+    L = _lib.load()
+    for f in range(W):
+        L.sqn_accumulate_frames(e2e_plan.handle, ctypes.c_void_p(hbase + f * fbytes), 1, _lib.HOST)
+        e2e_plan.peek_num_async(pnum.data_ptr())
+    e2e_plan.sync()
+    if dist:
+        td.barrier()
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for f in range(W, W + K):
+        rc = L.sqn_accumulate_frames(e2e_plan.handle, ctypes.c_void_p(hbase + f * fbytes), 1,
+                                     _lib.HOST)
+        _lib.check(rc, "sqn_accumulate_frames")
+        e2e_plan.peek_num_async(pnum.data_ptr())
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    e2e_t = ev0.elapsed_time(ev1) * 1e-3
+    if dist:
+        t = torch.tensor([e2e_t], dtype=torch.float64, device=f"cuda:{local_rank}")
+        td.all_reduce(t, op=td.ReduceOp.MAX)
+        e2e_t = float(t.item())
+    e2e_value = K * world / e2e_t
+    e2e_plan.close()
+
+    # --- sharded frames: sum the accumulators once ------------------------------
+    if dist:
+        acc = plan.accumulators()
+        t = torch.from_numpy(np.concatenate([acc["num"], acc["partial_num"].reshape(-1)])).to(
+            f"cuda:{local_rank}")
+        td.all_reduce(t)
+    plan.close()
+
+    if rank == 0:
+        # roofline of the dominant kernel of ours (spread or bin)
+        peak, peak_kind = hbm_peak()
+        ntr = info.ntransforms
+        nf = list(info.nf)
+        vol = nf[0] * nf[1] * nf[2]
+        p = 4 if prec == _lib.PREC_SINGLE else 8
+        c1 = nf[0] // 2 + 1
+        spread_bytes = ntr * vol * p + N_ATOMS * (16 if p == 4 else 32)
+        bin_bytes = ntr * (info.nmodes // 2) * 2 * p
+        kern = "spread" if stage_ms["spread_ms"] >= stage_ms["bin_ms"] else "bin"
+        kb = spread_bytes if kern == "spread" else bin_bytes
+        kms = stage_ms["spread_ms"] if kern == "spread" else stage_ms["bin_ms"]
+        achieved = kb / (kms * 1e-3) / 1e9
+        frame_bytes = ntr * (3 * vol * p + (info.nmodes // 2) * 2 * p) + N_ATOMS * (24 + 1)
+        frame_ms = 1e3 * elapsed / K
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
+            "warmup": W, "ms_per_step": 1e3 * elapsed / K, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64acc" if prec == _lib.PREC_SINGLE else "f64",
+            "data": "synthetic (seeded uniform + Gaussian jitter)",
+            "config": workload_config({
+                "parallelism": "frames sharded over %d GPU(s)" % world,
+                "upsampfac": info.upsampfac, "kernel_width": info.kernel_width,
+                "fine_grid": nf, "nmodes_kept": info.nmodes, "ntransforms": ntr}),
+            "roofline": {"bound": "hbm", "kernel": "k_spread" if kern == "spread" else "k_bin",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": dram_traffic("k_" + kern),
+                         "algorithmic_bytes_per_launch": kb, "launch_ms": kms},
+            "pipeline": {"bytes_per_frame": frame_bytes, "ms_per_frame": frame_ms,
+                         "achieved_gbs": frame_bytes / (frame_ms * 1e-3) / 1e9,
+                         "frac": frame_bytes / (frame_ms * 1e-3) / 1e9 / peak,
+                         "stage_ms": stage_ms},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": fbytes,
+                    "d2h_bytes_per_step": NQ * 8},
+            "gpu_launches": launches,
+            "gpu_launches_note": "own kernels (prep, scan, scatter, spread, bin) per frame; "
+                                 "cuFFT kernels not counted",
+            "clocks": clk.summary(),
+            "wall_s": t_wall,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            out["cpu_baseline"] = cpu_baseline_sample()
+        print(json.dumps(out), flush=True)
+    if dist:
+        td.barrier()
+        td.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="single", choices=["single", "double"])
+    ap.add_argument("--upsampfac", type=float, default=0.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

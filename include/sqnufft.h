@@ -1,0 +1,185 @@
+/*
+ * sqnufft -- B200-native static structure factor S(q) for sqcalc.
+ *
+ * C ABI of libsqnufft.so.  Every entry point is extern "C", takes plain
+ * pointers and sizes, never exits or traps, and returns an int status
+ * (0 = ok, 1 = warning, >1 = error; see SQN_ERR_*).
+ *
+ * The boundary sits one level above the one sqcalc uses today.  sqcalc's GPU
+ * method (src/sqc_gpu.f90:108-362) drives cuFINUFFT through iso_c_binding
+ * (src/sqc_cufinufft.f90:183-293): makeplan / setpts / execute / destroy plus
+ * raw cudaMalloc / cudaMemcpy, then downloads the whole T x prod(modes) mode
+ * cube and does the pair sums and the shell binning on the host
+ * (src/sqc_structure_factor.f90:457-643).  Here the library owns the whole
+ * frame accumulate: positions in, FP64 shell accumulators out; the mode cube
+ * never leaves the GPU.  Each entry point below names the reference interface
+ * it replaces.
+ *
+ * Array layouts are the reference's Fortran arrays in memory order:
+ *   cell[9]        a(3,3) column major: cell[3*i + r] = component r of vector a_(i+1)
+ *   pos            frame%pos(3, natoms) per frame, frames back to back
+ *   partial_num    partial_num(ntypes, ntypes, nq), first index fastest
+ *   gnum, gden     flat reciprocal grid of prod(modes) values, index gidx - 1
+ */
+#ifndef SQNUFFT_H
+#define SQNUFFT_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SQN_ABI_VERSION 1
+
+/* Status codes.  Values shared with FINUFFT keep FINUFFT's numbering
+ * (external/finufft/include/finufft_errors.h:5-31). */
+enum {
+  SQN_OK = 0,
+  SQN_WARN_EPS_TOO_SMALL = 1,       /* = FINUFFT_WARN_EPS_TOO_SMALL */
+  SQN_ERR_UPSAMPFAC_TOO_SMALL = 7,  /* = FINUFFT_ERR_UPSAMPFAC_TOO_SMALL */
+  SQN_ERR_ALLOC = 11,               /* = FINUFFT_ERR_ALLOC */
+  SQN_ERR_CUDA = 15,                /* = FINUFFT_ERR_CUDA_FAILURE */
+  SQN_ERR_PLAN_NOTVALID = 16,       /* = FINUFFT_ERR_PLAN_NOTVALID */
+  SQN_ERR_NUM_NU_PTS_INVALID = 20,  /* = FINUFFT_ERR_NUM_NU_PTS_INVALID */
+  SQN_ERR_INVALID_ARGUMENT = 21,    /* = FINUFFT_ERR_INVALID_ARGUMENT */
+  SQN_ERR_ABI_MISMATCH = 40,        /* descriptor built against another ABI version */
+  SQN_ERR_NO_DEVICE = 41,           /* no CUDA device, or device id out of range */
+  SQN_ERR_GRID_TOO_LARGE = 42,      /* prod(modes) above max_grid_modes */
+  SQN_ERR_NO_MODES = 43,            /* no reciprocal lattice point in [qmin, qmax] */
+  SQN_ERR_DEGENERATE_CELL = 44,
+  SQN_ERR_TYPE_ID = 45,             /* a type id outside 1..ntypes */
+  SQN_ERR_CUFFT = 46,               /* cuFFT plan or execution failure */
+  SQN_ERR_TIMEOUT = 47,             /* a bounded device wait gave up */
+  SQN_ERR_NOT_SUPPORTED = 48
+};
+
+enum { SQN_WEIGHT_UNIT = 0, SQN_WEIGHT_NEUTRON = 1, SQN_WEIGHT_XRAY = 2 };
+/* Normalisations of src/sqc_structure_factor.f90:53-55. */
+enum { SQN_NORM_MEAN = 1, SQN_NORM_SELF = 2, SQN_NORM_NATOM = 3 };
+/* DOUBLE: FP64 spread / FFT / deconvolution.  SINGLE: FP32 spread / FFT /
+ * deconvolution; pair products, |rho|^2, shell sums and normalisation FP64. */
+enum { SQN_PREC_DOUBLE = 0, SQN_PREC_SINGLE = 1 };
+/* Where a positions pointer lives. */
+enum { SQN_HOST = 0, SQN_DEVICE = 1 };
+/* sqn_plan_desc.flags */
+enum {
+  SQN_FLAG_TIMING = 1 /* record per-stage CUDA events (sqn_stage_times) */
+};
+
+/* Everything sqcalc's configure + gpu_setup know after the first frame
+ * (src/sqc_structure_factor.f90:313-422, src/sqc_gpu.f90:108-210). */
+typedef struct sqn_plan_desc {
+  int32_t abi_version;      /* SQN_ABI_VERSION */
+  int32_t device;           /* CUDA device id (--gpu-id) */
+  double cell[9];           /* lattice vectors, layout above (cell_t%a) */
+  double origin[3];         /* cell_t%origin */
+  int64_t natoms;
+  const int32_t *type_id;   /* [natoms] LAMMPS type ids in 1..ntypes, host memory, copied */
+  int32_t ntypes;           /* structure_factor_t%ntypes (largest type id) */
+  int32_t weight;           /* SQN_WEIGHT_* (-w) */
+  const double *amp_const;  /* [ntypes] neutron b per type id; NULL for unit / x-ray */
+  const double *xray_coef;  /* [ntypes][9] IT92 a1..a4, b1..b4, c per type id; NULL unless x-ray */
+  double qmin, qmax;        /* --qmin --qmax */
+  int32_t nq;               /* --nq */
+  int32_t norm;             /* SQN_NORM_* (--norm) */
+  int32_t partials;         /* --partials (pair sums per type pair) */
+  int32_t want_grid;        /* --grid (per-mode accumulators) */
+  int32_t precision;        /* SQN_PREC_* (--precision) */
+  int32_t flags;            /* SQN_FLAG_* */
+  double eps;               /* NUFFT tolerance (--eps) */
+  double upsampfac;         /* fine-grid upsampling sigma; 0 = chosen by the plan */
+  int32_t kernel_width;     /* ES kernel width w; 0 = from eps and sigma */
+  int32_t reserved;
+  int64_t max_grid_modes;   /* prod(modes) cap; 0 = sqcalc's 4e8, < 0 = none */
+  void *stream;             /* cudaStream_t to run on, or NULL for a plan-owned stream */
+} sqn_plan_desc;
+
+/* What the plan chose. */
+typedef struct sqn_plan_info {
+  int32_t modes[3];         /* structure_factor_t%modes */
+  int32_t kernel_width;
+  int64_t nf[3];            /* fine grid */
+  int64_t gridpoints;       /* prod(modes) */
+  int64_t nmodes;           /* kept modes with qmin <= |q| <= qmax, q != 0 */
+  double upsampfac;
+  double beta;              /* ES shape parameter */
+  double eps_used;
+  int32_t ntransforms;      /* fine grids per frame: species count or 1 */
+  int32_t nspecies;         /* type ids that have atoms */
+  int64_t device_bytes;     /* device memory the plan holds */
+  int64_t tile[3];          /* spread tile in fine-grid cells */
+} sqn_plan_info;
+
+typedef struct sqn_plan_s sqn_plan;
+
+/* ABI version of the loaded library (compare with SQN_ABI_VERSION). */
+int sqn_abi_version(void);
+
+/* Static text for a status code. */
+const char *sqn_error_string(int code);
+
+/* Descriptor defaults: sqcalc's option defaults (src/sqc_options.f90:51-140:
+ * qmin 0, qmax 20, nq 500, eps 1e-9, norm mean, partials on, unit weights). */
+void sqn_default_desc(sqn_plan_desc *desc);
+
+/* Build the reciprocal grid, the shell map, den / shell_count and every device
+ * buffer, and select the kernel.  Replaces sf_configure's grid setup plus
+ * gpu_setup (src/sqc_gpu.f90:108-210: cudaMalloc of x, y, z, c, fk and
+ * cufinufft[f]_makeplan).  *out is NULL on error. */
+int sqn_plan_create(const sqn_plan_desc *desc, sqn_plan **out);
+
+int sqn_plan_info_get(const sqn_plan *plan, sqn_plan_info *info);
+
+/* Add nframes frames to the accumulators.  pos holds nframes consecutive
+ * frame%pos(3, natoms) blocks in host (SQN_HOST) or device (SQN_DEVICE) memory.
+ * Replaces one gpu_accumulate per frame (src/sqc_gpu.f90:213-362: host wrap,
+ * uploads, cufinufft_setpts / execute, download, host pair sums and binning).
+ * The call returns once the positions have been read; the transforms run
+ * asynchronously on the plan's stream (device positions must stay valid until
+ * sqn_sync). */
+int sqn_accumulate_frames(sqn_plan *plan, const double *pos, int64_t nframes, int32_t where);
+
+/* Wait for all queued work of the plan. */
+int sqn_sync(sqn_plan *plan);
+
+/* Copy the accumulators out (syncs first).  Any pointer may be NULL.
+ *   num[nq], den[nq], shell_count[nq]         structure_factor_t%num, den, shell_count
+ *   partial_num[ntypes*ntypes*nq]             partial_num (zero when partials are off)
+ *   gnum[gridpoints], gden[gridpoints]        gnum, gden (want_grid only)
+ * Replaces reading the Fortran accumulators filled by sf_accumulate_values /
+ * sf_accumulate_partials (src/sqc_structure_factor.f90:481-643). */
+int sqn_get_accumulators(sqn_plan *plan, double *num, double *den, int64_t *shell_count,
+                         double *partial_num, double *gnum, double *gden, int64_t *nframes);
+
+/* Queue a device-to-host copy of num[nq] into host memory (pinned for an
+ * asynchronous copy) on the plan's stream, without waiting. */
+int sqn_peek_num_async(sqn_plan *plan, double *num_host);
+
+/* Normalised results (syncs first); NULL pointers are skipped.
+ *   S_total[nq]                         sf_shell_value  (:657-665)
+ *   S_partial[ntypes*ntypes*nq]         sf_partial_value (:696-719), faber_ziman 0/1
+ *   S_grid[nmodes]                      sf_grid_value (:757-768), kept modes in the
+ *                                       reference's enumeration order (:352-381) */
+int sqn_finalize(sqn_plan *plan, int32_t faber_ziman, double *S_total, double *S_partial,
+                 double *S_grid, int64_t *nframes);
+
+/* Zero the accumulators and the frame count. */
+int sqn_reset(sqn_plan *plan);
+
+/* Per-stage device time summed over the frames since the last reset, in ms:
+ * out[0] wrap+bin sort, out[1] spread, out[2] FFT, out[3] deconvolve+bin,
+ * out[4] frames timed.  Needs SQN_FLAG_TIMING. */
+int sqn_stage_times(sqn_plan *plan, double *out, int32_t n);
+
+/* Number of this library's own kernel launches so far (cuFFT's not counted). */
+int64_t sqn_launch_count(const sqn_plan *plan);
+
+/* Release the plan and its device memory.  Replaces cufinufft_destroy plus the
+ * cudaFree calls of gpu_finalize (src/sqc_gpu.f90:365-404). */
+int sqn_plan_destroy(sqn_plan *plan);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SQNUFFT_H */

@@ -1,0 +1,272 @@
+"""ctypes binding of libsqnufft.so (the C ABI in include/sqnufft.h).
+
+This is the Python counterpart of sqcalc's iso_c_binding module for the GPU
+method (src/sqc_cufinufft.f90): a 1:1 mirror of the C structs and functions,
+nothing more.  The library is loaded from this package directory; a missing or
+stale build is an error, never a silent fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsqnufft.so")
+
+ABI_VERSION = 1
+OK, WARN_EPS_TOO_SMALL = 0, 1
+WEIGHT_UNIT, WEIGHT_NEUTRON, WEIGHT_XRAY = 0, 1, 2
+NORM_MEAN, NORM_SELF, NORM_NATOM = 1, 2, 3
+PREC_DOUBLE, PREC_SINGLE = 0, 1
+HOST, DEVICE = 0, 1
+FLAG_TIMING = 1
+
+# Every symbol include/sqnufft.h declares.
+EXPORTS = (
+    "sqn_abi_version", "sqn_error_string", "sqn_default_desc", "sqn_plan_create",
+    "sqn_plan_info_get", "sqn_accumulate_frames", "sqn_sync", "sqn_get_accumulators",
+    "sqn_peek_num_async", "sqn_finalize", "sqn_reset", "sqn_stage_times", "sqn_launch_count",
+    "sqn_plan_destroy",
+)
+
+
+class SqnDesc(ctypes.Structure):
+    _fields_ = [
+        ("abi_version", ctypes.c_int32),
+        ("device", ctypes.c_int32),
+        ("cell", ctypes.c_double * 9),
+        ("origin", ctypes.c_double * 3),
+        ("natoms", ctypes.c_int64),
+        ("type_id", ctypes.POINTER(ctypes.c_int32)),
+        ("ntypes", ctypes.c_int32),
+        ("weight", ctypes.c_int32),
+        ("amp_const", ctypes.POINTER(ctypes.c_double)),
+        ("xray_coef", ctypes.POINTER(ctypes.c_double)),
+        ("qmin", ctypes.c_double),
+        ("qmax", ctypes.c_double),
+        ("nq", ctypes.c_int32),
+        ("norm", ctypes.c_int32),
+        ("partials", ctypes.c_int32),
+        ("want_grid", ctypes.c_int32),
+        ("precision", ctypes.c_int32),
+        ("flags", ctypes.c_int32),
+        ("eps", ctypes.c_double),
+        ("upsampfac", ctypes.c_double),
+        ("kernel_width", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("max_grid_modes", ctypes.c_int64),
+        ("stream", ctypes.c_void_p),
+    ]
+
+
+class SqnInfo(ctypes.Structure):
+    _fields_ = [
+        ("modes", ctypes.c_int32 * 3),
+        ("kernel_width", ctypes.c_int32),
+        ("nf", ctypes.c_int64 * 3),
+        ("gridpoints", ctypes.c_int64),
+        ("nmodes", ctypes.c_int64),
+        ("upsampfac", ctypes.c_double),
+        ("beta", ctypes.c_double),
+        ("eps_used", ctypes.c_double),
+        ("ntransforms", ctypes.c_int32),
+        ("nspecies", ctypes.c_int32),
+        ("device_bytes", ctypes.c_int64),
+        ("tile", ctypes.c_int64 * 3),
+    ]
+
+
+class SqnError(RuntimeError):
+    def __init__(self, code, where=""):
+        self.code = int(code)
+        super().__init__("%s%s (status %d)" % (where + ": " if where else "",
+                                               error_string(code), self.code))
+
+
+_lib = None
+
+
+def load():
+    """Load libsqnufft.so from the package directory (no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError("libsqnufft.so is not built; run `python -m sqcalc_b200.build` "
+                          "(expected at %s)" % LIB_PATH)
+    L = ctypes.CDLL(LIB_PATH)
+    vp, dp, i64 = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_int64
+    L.sqn_abi_version.restype = ctypes.c_int
+    L.sqn_error_string.argtypes = [ctypes.c_int]
+    L.sqn_error_string.restype = ctypes.c_char_p
+    L.sqn_default_desc.argtypes = [ctypes.POINTER(SqnDesc)]
+    L.sqn_plan_create.argtypes = [ctypes.POINTER(SqnDesc), ctypes.POINTER(vp)]
+    L.sqn_plan_info_get.argtypes = [vp, ctypes.POINTER(SqnInfo)]
+    L.sqn_accumulate_frames.argtypes = [vp, vp, i64, ctypes.c_int32]
+    L.sqn_sync.argtypes = [vp]
+    L.sqn_get_accumulators.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp]
+    L.sqn_peek_num_async.argtypes = [vp, vp]
+    L.sqn_finalize.argtypes = [vp, ctypes.c_int32, vp, vp, vp, vp]
+    L.sqn_reset.argtypes = [vp]
+    L.sqn_stage_times.argtypes = [vp, dp, ctypes.c_int32]
+    L.sqn_launch_count.argtypes = [vp]
+    L.sqn_launch_count.restype = i64
+    L.sqn_plan_destroy.argtypes = [vp]
+    if L.sqn_abi_version() != ABI_VERSION:
+        raise ImportError("libsqnufft.so ABI %d, binding expects %d"
+                          % (L.sqn_abi_version(), ABI_VERSION))
+    _lib = L
+    return L
+
+
+def error_string(code):
+    try:
+        return load().sqn_error_string(int(code)).decode()
+    except ImportError:
+        return "status %d" % code
+
+
+def check(code, where=""):
+    if code > WARN_EPS_TOO_SMALL:
+        raise SqnError(code, where)
+    return code
+
+
+def _ptr(a):
+    return None if a is None else ctypes.c_void_p(a.ctypes.data)
+
+
+class Plan:
+    """One sqn_plan: configure once, accumulate frames, read accumulators."""
+
+    def __init__(self, cell, origin, type_id, ntypes=None, weight=WEIGHT_UNIT, amp_const=None,
+                 xray_coef=None, qmin=0.0, qmax=20.0, nq=500, norm=NORM_MEAN, partials=True,
+                 want_grid=False, precision=PREC_DOUBLE, eps=1e-9, upsampfac=0.0,
+                 kernel_width=0, device=0, max_grid_modes=0, timing=False, stream=None):
+        L = load()
+        self._L = L
+        self.type_id = np.ascontiguousarray(type_id, dtype=np.int32)
+        self.natoms = int(self.type_id.size)
+        self.ntypes = int(ntypes if ntypes is not None else max(int(self.type_id.max()), 1))
+        self.nq = int(nq)
+        self.partials = bool(partials)
+        self.want_grid = bool(want_grid)
+        d = SqnDesc()
+        L.sqn_default_desc(ctypes.byref(d))
+        d.device = int(device)
+        cell = np.ascontiguousarray(np.asarray(cell, dtype=np.float64).reshape(9))
+        for k in range(9):
+            d.cell[k] = float(cell[k])
+        for k in range(3):
+            d.origin[k] = float(origin[k])
+        d.natoms = self.natoms
+        d.type_id = self.type_id.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+        d.ntypes = self.ntypes
+        d.weight = int(weight)
+        self._amp = None if amp_const is None else np.ascontiguousarray(amp_const, dtype=np.float64)
+        self._xc = None if xray_coef is None else np.ascontiguousarray(xray_coef, dtype=np.float64)
+        if self._amp is not None:
+            d.amp_const = self._amp.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        if self._xc is not None:
+            d.xray_coef = self._xc.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        d.qmin, d.qmax, d.nq = float(qmin), float(qmax), self.nq
+        d.norm = int(norm)
+        d.partials = int(bool(partials))
+        d.want_grid = int(bool(want_grid))
+        d.precision = int(precision)
+        d.flags = FLAG_TIMING if timing else 0
+        d.eps = float(eps)
+        d.upsampfac = float(upsampfac)
+        d.kernel_width = int(kernel_width)
+        d.max_grid_modes = int(max_grid_modes)
+        d.stream = stream
+        h = ctypes.c_void_p()
+        self.status = check(L.sqn_plan_create(ctypes.byref(d), ctypes.byref(h)), "sqn_plan_create")
+        self._h = h
+        info = SqnInfo()
+        check(L.sqn_plan_info_get(h, ctypes.byref(info)), "sqn_plan_info_get")
+        self.info = info
+        self.modes = tuple(info.modes)
+        self.nmodes = int(info.nmodes)
+        self.gridpoints = int(info.gridpoints)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def accumulate(self, pos, where=HOST):
+        """pos: (nframes, natoms, 3) or (natoms, 3) float64 host array, or a device
+        pointer (int) with where=DEVICE and an explicit frame count in pos=(ptr, n)."""
+        if where == DEVICE:
+            ptr, n = pos
+            check(self._L.sqn_accumulate_frames(self._h, ctypes.c_void_p(ptr), int(n), DEVICE),
+                  "sqn_accumulate_frames")
+            return
+        a = np.ascontiguousarray(pos, dtype=np.float64)
+        n = 1 if a.ndim == 2 else a.shape[0]
+        if a.size != n * self.natoms * 3:
+            raise ValueError("positions must hold %d atoms per frame" % self.natoms)
+        check(self._L.sqn_accumulate_frames(self._h, _ptr(a), n, HOST), "sqn_accumulate_frames")
+
+    def sync(self):
+        check(self._L.sqn_sync(self._h), "sqn_sync")
+
+    def accumulators(self, grid=False):
+        nq, T = self.nq, self.ntypes
+        num, den = np.zeros(nq), np.zeros(nq)
+        cnt = np.zeros(nq, dtype=np.int64)
+        pn = np.zeros(T * T * nq)
+        gnum = np.zeros(self.gridpoints) if grid else None
+        gden = np.zeros(self.gridpoints) if grid else None
+        nf = ctypes.c_int64()
+        check(self._L.sqn_get_accumulators(self._h, _ptr(num), _ptr(den), _ptr(cnt), _ptr(pn),
+                                           _ptr(gnum), _ptr(gden),
+                                           ctypes.cast(ctypes.byref(nf), ctypes.c_void_p)),
+              "sqn_get_accumulators")
+        return dict(num=num, den=den, shell_count=cnt,
+                    partial_num=pn.reshape(nq, T, T).transpose(2, 1, 0), gnum=gnum, gden=gden,
+                    nframes=int(nf.value))
+
+    def finalize(self, faber_ziman=False, grid=False):
+        nq, T = self.nq, self.ntypes
+        s, sp = np.zeros(nq), np.zeros(T * T * nq)
+        sg = np.zeros(self.nmodes) if grid else None
+        nf = ctypes.c_int64()
+        check(self._L.sqn_finalize(self._h, int(bool(faber_ziman)), _ptr(s), _ptr(sp), _ptr(sg),
+                                   ctypes.cast(ctypes.byref(nf), ctypes.c_void_p)),
+              "sqn_finalize")
+        return s, sp.reshape(nq, T, T).transpose(2, 1, 0), sg, int(nf.value)
+
+    def peek_num_async(self, host_buf_ptr):
+        check(self._L.sqn_peek_num_async(self._h, ctypes.c_void_p(host_buf_ptr)), "sqn_peek")
+
+    def reset(self):
+        check(self._L.sqn_reset(self._h), "sqn_reset")
+
+    def stage_times(self):
+        out = (ctypes.c_double * 5)()
+        check(self._L.sqn_stage_times(self._h, out, 5), "sqn_stage_times")
+        return dict(sort_ms=out[0], spread_ms=out[1], fft_ms=out[2], bin_ms=out[3],
+                    frames=int(out[4]))
+
+    def launch_count(self):
+        return int(self._L.sqn_launch_count(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            self._L.sqn_plan_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

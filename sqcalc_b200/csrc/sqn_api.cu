@@ -1,0 +1,938 @@
+// C ABI of libsqnufft.so: plan set up, per-frame pipeline, accumulators.
+//
+// The plan is the B200 counterpart of three reference objects at once:
+//   * structure_factor_t's grid bookkeeping (src/sqc_structure_factor.f90:313-451),
+//   * cufinufft_structure_factor_t (src/sqc_gpu.f90:108-404),
+//   * the cuFINUFFT type-1 plan it drives (external/finufft/include/cufinufft/impl.h:51-330).
+// Everything per frame stays on the device; only nq-sized accumulators return.
+#include <cufft.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstdint>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "../../include/sqnufft.h"
+#include "sqn_internal.h"
+
+using namespace sqn;
+
+namespace {
+
+constexpr int64_t kRefMaxGridModes = 400000000LL;  // src/sqc_structure_factor.f90:63-64
+
+// ---------------------------------------------------------------------------
+// Host math
+// ---------------------------------------------------------------------------
+
+// determinant3 / inverse3 of src/sqc_cell.f90:131-152; m[3*c + r] = m(r+1, c+1).
+double det3(const double *a) {
+  auto M = [a](int r, int c) { return a[3 * (c - 1) + (r - 1)]; };
+  return M(1, 1) * (M(2, 2) * M(3, 3) - M(2, 3) * M(3, 2)) -
+         M(1, 2) * (M(2, 1) * M(3, 3) - M(2, 3) * M(3, 1)) +
+         M(1, 3) * (M(2, 1) * M(3, 2) - M(2, 2) * M(3, 1));
+}
+
+void inverse3(const double *a, double *inv) {
+  auto M = [a](int r, int c) { return a[3 * (c - 1) + (r - 1)]; };
+  auto I = [inv](int r, int c) -> double & { return inv[3 * (c - 1) + (r - 1)]; };
+  const double det = det3(a);
+  I(1, 1) = (M(2, 2) * M(3, 3) - M(2, 3) * M(3, 2));
+  I(2, 1) = -(M(2, 1) * M(3, 3) - M(2, 3) * M(3, 1));
+  I(3, 1) = (M(2, 1) * M(3, 2) - M(2, 2) * M(3, 1));
+  I(1, 2) = -(M(1, 2) * M(3, 3) - M(1, 3) * M(3, 2));
+  I(2, 2) = (M(1, 1) * M(3, 3) - M(1, 3) * M(3, 1));
+  I(3, 2) = -(M(1, 1) * M(3, 2) - M(1, 2) * M(3, 1));
+  I(1, 3) = (M(1, 2) * M(2, 3) - M(1, 3) * M(2, 2));
+  I(2, 3) = -(M(1, 1) * M(2, 3) - M(1, 3) * M(2, 1));
+  I(3, 3) = (M(1, 1) * M(2, 2) - M(1, 2) * M(2, 1));
+  for (int k = 0; k < 9; ++k) inv[k] = inv[k] / det;
+}
+
+// Smallest even integer >= n whose prime factors are 2, 3 and 5.
+int64_t next235even(int64_t n) {
+  if (n <= 2) return 2;
+  if (n % 2) ++n;
+  for (int64_t c = n;; c += 2) {
+    int64_t d = c;
+    while (d % 2 == 0) d /= 2;
+    while (d % 3 == 0) d /= 3;
+    while (d % 5 == 0) d /= 5;
+    if (d == 1) return c;
+  }
+}
+
+// Kernel width for tolerance eps at upsampling sigma and the ES shape beta, the
+// published exponential-of-semicircle choices (Barnett, Magland, af Klinteberg,
+// SIAM J. Sci. Comput. 41 (2019)) in the form external/finufft/src/cuda/
+// spreadinterp.cpp:59-85 applies them.
+int es_width(double eps, double sigma) {
+  int w;
+  if (sigma == 2.0)
+    w = (int)std::ceil(-std::log10(eps / 10.0));
+  else
+    w = (int)std::ceil(-std::log(eps) / (M_PI * std::sqrt(1.0 - 1.0 / sigma)));
+  return std::max(2, w);
+}
+
+double es_beta(int w, double sigma) {
+  double bw = 2.30;
+  if (w == 2) bw = 2.20;
+  if (w == 3) bw = 2.26;
+  if (w == 4) bw = 2.38;
+  if (sigma != 2.0) bw = 0.97 * M_PI * (1.0 - 1.0 / (2.0 * sigma));
+  return bw * w;
+}
+
+double es_phi_host(double t, int w, double beta) {
+  const double z = 2.0 * t / w;
+  const double zz = z * z;
+  return zz < 1.0 ? std::exp(beta * (std::sqrt(1.0 - zz) - 1.0)) : 0.0;
+}
+
+// n-point Gauss-Legendre rule on [-1, 1] (Newton iteration on P_n).
+void gauss_legendre(int n, std::vector<double> &x, std::vector<double> &wt) {
+  x.assign(n, 0.0);
+  wt.assign(n, 0.0);
+  for (int i = 0; i < n; ++i) {
+    double z = std::cos(M_PI * (i + 0.75) / (n + 0.5)), dp = 0.0;
+    for (int it = 0; it < 100; ++it) {
+      double p0 = 1.0, p1 = z;
+      for (int k = 2; k <= n; ++k) {
+        const double p2 = ((2.0 * k - 1.0) * z * p1 - (k - 1.0) * p0) / k;
+        p0 = p1;
+        p1 = p2;
+      }
+      dp = n * (z * p1 - p0) / (z * z - 1.0);
+      const double dz = p1 / dp;
+      z -= dz;
+      if (std::fabs(dz) < 1e-16) break;
+    }
+    x[i] = z;
+    wt[i] = 2.0 / ((1.0 - z * z) * dp * dp);
+  }
+}
+
+// Fourier transform of the kernel at the integer frequencies 0..kmax of an
+// nf-periodic grid: phihat(k) = 2 int_0^{w/2} phi(t) cos(2 pi k t / nf) dt,
+// by Gauss-Legendre quadrature (cf. external/finufft/src/cuda/common.cu:196-210).
+std::vector<double> kernel_ft(int64_t nf, int w, double beta, int kmax) {
+  const int n = 4 * w + 24;
+  std::vector<double> x, wt;
+  gauss_legendre(n, x, wt);
+  std::vector<double> out(kmax + 1);
+  const double half = 0.5 * w;
+  for (int k = 0; k <= kmax; ++k) {
+    double s = 0.0;
+    for (int i = 0; i < n; ++i) {
+      const double t = 0.5 * half * (x[i] + 1.0);
+      s += 0.5 * half * wt[i] * es_phi_host(t, w, beta) * std::cos(2.0 * M_PI * k * t / (double)nf);
+    }
+    out[k] = 2.0 * s;
+  }
+  return out;
+}
+
+// |q| in the reference's operation order (src/sqc_structure_factor.f90:366-368).
+inline double qlen_ref(const double *b, int h1, int h2, int h3) {
+  double q[3];
+  for (int r = 0; r < 3; ++r) q[r] = b[r] * (double)h1 + b[3 + r] * (double)h2 + b[6 + r] * (double)h3;
+  return std::sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]);
+}
+
+double xray_f_host(const double *c, double q) {
+  double st = q / (4.0 * std::acos(-1.0));
+  st = st * st;
+  double f = c[8];
+  for (int i = 0; i < 4; ++i) f = f + c[i] * std::exp(-c[4 + i] * st);
+  return f;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Plan
+// ---------------------------------------------------------------------------
+
+struct sqn_plan_s {
+  sqn_plan_desc desc{};
+  bool fp64 = false;
+  int device = 0;
+  cudaStream_t stream = nullptr, copy_stream = nullptr;
+  bool own_stream = false;
+  int nsm = 148;
+
+  double cell[9], origin[3], inv[9], recip[9];
+  int modes[3], hm[3];
+  int64_t gridpoints = 0, nmodes = 0;
+  int w = 0;
+  double beta = 0, sigma = 0, eps_used = 0;
+  int64_t nf[3];
+  FrameGeom fg{};
+  BinGeom bg{};
+  int ntr = 0, nspecies = 0, nquant = 1, nrows = 0;
+  int nkeys = 0;
+  std::vector<int> species_type;   // type id of each species
+  std::vector<int64_t> type_counts;  // atoms per type id (index t-1)
+  std::vector<double> amp_sp, xcoef_sp;
+  std::vector<double> den, cnt;    // per shell, from the set-up pass
+
+  double *d_pos[2] = {nullptr, nullptr};
+  uint8_t *d_species = nullptr;
+  int *d_counts = nullptr, *d_starts = nullptr;
+  uint32_t *d_key = nullptr, *d_slot = nullptr;
+  void *d_recs = nullptr, *d_grid = nullptr, *d_G = nullptr;
+  void *d_inv[3] = {nullptr, nullptr, nullptr};
+  void *d_strength = nullptr;
+  double *d_amp = nullptr, *d_xcoef = nullptr, *d_amp_sp = nullptr, *d_xcoef_sp = nullptr,
+         *d_counts_sp = nullptr;
+  int4 *d_rows = nullptr;
+  double *d_acc = nullptr, *d_gnum = nullptr, *d_den = nullptr, *d_cnt = nullptr;
+  cufftHandle fft = 0;
+  bool fft_ok = false;
+  int64_t gnum_half = 0;
+
+  int64_t nframes = 0;
+  int slot_next = 0;
+  cudaEvent_t ev_copied[2] = {nullptr, nullptr}, ev_free[2] = {nullptr, nullptr};
+  bool timing = false;
+  std::vector<cudaEvent_t> tev_pool;  // 5 per timed frame
+  size_t tev_used = 0;
+  double stage_ms[4] = {0, 0, 0, 0};
+  int64_t stage_frames = 0;
+  int64_t launches = 0;
+  int64_t device_bytes = 0;
+  std::vector<void *> allocs;
+};
+
+namespace {
+
+int cuda_status(cudaError_t e) { return e == cudaSuccess ? SQN_OK : SQN_ERR_CUDA; }
+
+template <typename T> int dalloc(sqn_plan *p, T **ptr, size_t count) {
+  *ptr = nullptr;
+  if (count == 0) count = 1;
+  void *v = nullptr;
+  if (cudaMalloc(&v, count * sizeof(T)) != cudaSuccess) {
+    cudaGetLastError();
+    return SQN_ERR_ALLOC;
+  }
+  p->allocs.push_back(v);
+  p->device_bytes += (int64_t)(count * sizeof(T));
+  *ptr = static_cast<T *>(v);
+  return SQN_OK;
+}
+
+void free_plan(sqn_plan *p) {
+  if (!p) return;
+  int cur = 0;
+  cudaGetDevice(&cur);
+  cudaSetDevice(p->device);
+  if (p->stream) cudaStreamSynchronize(p->stream);
+  if (p->copy_stream) cudaStreamSynchronize(p->copy_stream);
+  if (p->fft_ok) cufftDestroy(p->fft);
+  for (void *v : p->allocs) cudaFree(v);
+  for (int i = 0; i < 2; ++i) {
+    if (p->ev_copied[i]) cudaEventDestroy(p->ev_copied[i]);
+    if (p->ev_free[i]) cudaEventDestroy(p->ev_free[i]);
+  }
+  for (cudaEvent_t e : p->tev_pool) cudaEventDestroy(e);
+  if (p->copy_stream) cudaStreamDestroy(p->copy_stream);
+  if (p->own_stream && p->stream) cudaStreamDestroy(p->stream);
+  cudaSetDevice(cur);
+  delete p;
+}
+
+// Rows (h2, h3) of the half space h1 >= 0 that reach |q| <= qmax, with a
+// conservative h1 range; the kernels test every mode exactly.
+std::vector<int4> build_rows(const double *b, const int *hm, double qmax) {
+  std::vector<int4> rows;
+  const double *b1 = b, *b2 = b + 3, *b3 = b + 6;
+  const double A = b1[0] * b1[0] + b1[1] * b1[1] + b1[2] * b1[2];
+  const double qm = qmax * (1.0 + 1e-9) + 1e-12;
+  for (int h3 = -hm[2]; h3 <= hm[2]; ++h3) {
+    for (int h2 = -hm[1]; h2 <= hm[1]; ++h2) {
+      double c[3];
+      for (int r = 0; r < 3; ++r) c[r] = h2 * b2[r] + h3 * b3[r];
+      const double B = 2.0 * (b1[0] * c[0] + b1[1] * c[1] + b1[2] * c[2]);
+      const double C = c[0] * c[0] + c[1] * c[1] + c[2] * c[2] - qm * qm;
+      const double disc = B * B - 4.0 * A * C;
+      if (disc < 0.0) continue;
+      const double sq = std::sqrt(disc);
+      const double r1 = (-B - sq) / (2.0 * A), r2 = (-B + sq) / (2.0 * A);
+      int lo = (int)std::max(0.0, std::floor(r1) - 1.0);
+      const double hi_d = std::min((double)hm[0], std::ceil(r2) + 1.0);
+      if (hi_d < 0.0) continue;
+      const int hi = (int)hi_d;
+      if (lo > hi) continue;
+      rows.push_back(make_int4(h2, h3, lo, hi));
+    }
+  }
+  return rows;
+}
+
+template <typename R> std::vector<R> to_r(const std::vector<double> &v) {
+  return std::vector<R>(v.begin(), v.end());
+}
+
+int setup_plan(sqn_plan *p, const sqn_plan_desc *d) {
+  p->desc = *d;
+  p->desc.type_id = nullptr;
+  p->desc.amp_const = nullptr;
+  p->desc.xray_coef = nullptr;
+  p->fp64 = d->precision == SQN_PREC_DOUBLE;
+  p->timing = (d->flags & SQN_FLAG_TIMING) != 0;
+  int warn = SQN_OK;
+
+  // --- device ----------------------------------------------------------
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
+    cudaGetLastError();
+    return SQN_ERR_NO_DEVICE;
+  }
+  if (d->device < 0 || d->device >= ndev) return SQN_ERR_NO_DEVICE;
+  p->device = d->device;
+  if (cudaSetDevice(p->device) != cudaSuccess) return SQN_ERR_CUDA;
+  cudaDeviceGetAttribute(&p->nsm, cudaDevAttrMultiProcessorCount, p->device);
+  if (d->stream) {
+    p->stream = (cudaStream_t)d->stream;
+  } else {
+    if (cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking) != cudaSuccess)
+      return SQN_ERR_CUDA;
+    p->own_stream = true;
+  }
+  if (cudaStreamCreateWithFlags(&p->copy_stream, cudaStreamNonBlocking) != cudaSuccess)
+    return SQN_ERR_CUDA;
+  for (int i = 0; i < 2; ++i) {
+    if (cudaEventCreateWithFlags(&p->ev_copied[i], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&p->ev_free[i], cudaEventDisableTiming) != cudaSuccess)
+      return SQN_ERR_CUDA;
+  }
+  if (spread_set_attributes() != cudaSuccess) return SQN_ERR_CUDA;
+
+  // --- cell and reciprocal grid (sf_configure, :313-399) --------------------
+  std::memcpy(p->cell, d->cell, sizeof(p->cell));
+  std::memcpy(p->origin, d->origin, sizeof(p->origin));
+  if (det3(p->cell) == 0.0) return SQN_ERR_DEGENERATE_CELL;
+  inverse3(p->cell, p->inv);
+  const double two_pi = 2.0 * std::acos(-1.0);
+  for (int j = 0; j < 3; ++j)
+    for (int r = 0; r < 3; ++r) p->recip[3 * j + r] = two_pi * p->inv[3 * r + j];
+  for (int i = 0; i < 3; ++i) {
+    const double *v = p->cell + 3 * i;
+    const double len = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    if (len <= 0.0) return SQN_ERR_DEGENERATE_CELL;
+    p->modes[i] = std::max(2 * (int)std::ceil(d->qmax * len / two_pi) + 1, 3);
+    p->hm[i] = (p->modes[i] - 1) / 2;
+  }
+  p->gridpoints = (int64_t)p->modes[0] * p->modes[1] * p->modes[2];
+  const int64_t cap = d->max_grid_modes == 0 ? kRefMaxGridModes : d->max_grid_modes;
+  if (cap > 0 && p->gridpoints > cap) return SQN_ERR_GRID_TOO_LARGE;
+  if (!(d->qmax > d->qmin) || d->nq < 1) return SQN_ERR_INVALID_ARGUMENT;
+
+  // --- species (sf_shared_setup + sf_prepare_species, :256-292, :1109-1163) --
+  if (d->natoms < 1 || d->natoms > (int64_t)INT32_MAX / 2) return SQN_ERR_NUM_NU_PTS_INVALID;
+  if (d->ntypes < 1 || !d->type_id) return SQN_ERR_INVALID_ARGUMENT;
+  p->type_counts.assign(d->ntypes, 0);
+  for (int64_t i = 0; i < d->natoms; ++i) {
+    const int t = d->type_id[i];
+    if (t < 1 || t > d->ntypes) return SQN_ERR_TYPE_ID;
+    p->type_counts[t - 1]++;
+  }
+  std::vector<int> species_of_type(d->ntypes + 1, -1);
+  for (int t = 1; t <= d->ntypes; ++t)
+    if (p->type_counts[t - 1] > 0) {
+      species_of_type[t] = (int)p->species_type.size();
+      p->species_type.push_back(t);
+    }
+  p->nspecies = (int)p->species_type.size();
+  if (p->nspecies > 255) return SQN_ERR_NOT_SUPPORTED;
+  const bool xray = d->weight == SQN_WEIGHT_XRAY;
+  if (d->weight == SQN_WEIGHT_NEUTRON && !d->amp_const) return SQN_ERR_INVALID_ARGUMENT;
+  if (xray && !d->xray_coef) return SQN_ERR_INVALID_ARGUMENT;
+  p->amp_sp.assign(p->nspecies, 1.0);
+  p->xcoef_sp.assign(9 * (size_t)p->nspecies, 0.0);
+  for (int s = 0; s < p->nspecies; ++s) {
+    const int t = p->species_type[s];
+    if (d->weight == SQN_WEIGHT_NEUTRON) p->amp_sp[s] = d->amp_const[t - 1];
+    if (xray) std::memcpy(&p->xcoef_sp[9 * s], d->xray_coef + 9 * (size_t)(t - 1), 9 * sizeof(double));
+  }
+  // One transform per species for pair columns or q-dependent weights, else a
+  // single weighted transform (src/sqc_gpu.f90:190-197).
+  p->ntr = (d->partials || xray) ? p->nspecies : 1;
+  if (p->ntr > MAX_FAST_T) return SQN_ERR_NOT_SUPPORTED;
+  p->nquant = 1 + (d->partials ? p->ntr * (p->ntr + 1) / 2 : 0);
+
+  // --- kernel and fine grid ----------------------------------------------
+  double eps = d->eps;
+  const double floor_eps = p->fp64 ? DBL_EPSILON : (double)FLT_EPSILON;
+  if (!(eps > 0.0)) return SQN_ERR_INVALID_ARGUMENT;
+  if (eps < floor_eps) {
+    eps = floor_eps;
+    warn = SQN_WARN_EPS_TOO_SMALL;
+  }
+  p->eps_used = eps;
+  double sigma = d->upsampfac;
+  if (sigma == 0.0) {
+    // Low upsampling keeps the fine grid (and so the FFT, the dominant HBM
+    // traffic) 4x smaller than sigma = 2 whenever a width <= 16 reaches eps.
+    sigma = es_width(eps, 1.25) <= MAX_W ? 1.25 : 2.0;
+  }
+  if (sigma <= 1.0) return SQN_ERR_UPSAMPFAC_TOO_SMALL;
+  int w = d->kernel_width > 0 ? d->kernel_width : es_width(eps, sigma);
+  if (w > MAX_W) {
+    w = MAX_W;
+    warn = SQN_WARN_EPS_TOO_SMALL;
+  }
+  p->w = w;
+  p->sigma = sigma;
+  p->beta = es_beta(w, sigma);
+  for (int i = 0; i < 3; ++i) {
+    int64_t n = (int64_t)std::ceil(sigma * p->modes[i]);
+    n = std::max<int64_t>(n, 2 * w);
+    p->nf[i] = next235even(n);
+  }
+
+  // --- tiles ---------------------------------------------------------------
+  FrameGeom &g = p->fg;
+  const int tmax[3] = {TILE_X, TILE_Y, TILE_Z};
+  for (int i = 0; i < 3; ++i) {
+    g.nf[i] = (int)p->nf[i];
+    g.tile[i] = (int)std::min<int64_t>(tmax[i], p->nf[i]);
+    g.ntile[i] = (int)((p->nf[i] + g.tile[i] - 1) / g.tile[i]);
+    const int need = (w - 1 + g.tile[i] - 1) / g.tile[i] + 1 + (p->nf[i] % g.tile[i] ? 1 : 0);
+    g.nbk[i] = std::min(g.ntile[i], need);
+  }
+  if (g.nbk[0] * g.nbk[1] * g.nbk[2] > MAX_NB) return SQN_ERR_NOT_SUPPORTED;
+  std::memcpy(g.inv, p->inv, sizeof(g.inv));
+  std::memcpy(g.origin, p->origin, sizeof(g.origin));
+  g.w = w;
+  g.beta = p->beta;
+  g.ntr = p->ntr;
+  g.ntiles = g.ntile[0] * g.ntile[1] * g.ntile[2];
+  g.pitch = p->nf[0];
+  g.vol_real = p->nf[0] * p->nf[1] * p->nf[2];
+  g.natoms = d->natoms;
+  if ((int64_t)g.ntiles * p->ntr >= INT32_MAX) return SQN_ERR_NOT_SUPPORTED;
+  p->nkeys = g.ntiles * p->ntr;
+
+  BinGeom &b = p->bg;
+  std::memcpy(b.recip, p->recip, sizeof(b.recip));
+  b.qmin = d->qmin;
+  b.qmax = d->qmax;
+  b.dq = (d->qmax - d->qmin) / (double)d->nq;
+  b.nq = d->nq;
+  for (int i = 0; i < 3; ++i) {
+    b.hm[i] = p->hm[i];
+    b.nf[i] = (int)p->nf[i];
+  }
+  b.c1 = p->nf[0] / 2 + 1;
+  b.vol_cplx = b.c1 * p->nf[1] * p->nf[2];
+  b.ntr = p->ntr;
+  b.nquant = p->nquant;
+  b.partials = d->partials ? 1 : 0;
+  b.xray = xray ? 1 : 0;
+  b.want_grid = d->want_grid ? 1 : 0;
+  b.m2 = p->modes[1];
+  b.norm = d->norm;
+  b.natoms = d->natoms;
+  if (d->norm < 1 || d->norm > 3) return SQN_ERR_INVALID_ARGUMENT;
+
+  // --- device buffers --------------------------------------------------------
+  const int64_t N = d->natoms;
+  const size_t rsz = p->fp64 ? 8 : 4;
+  int st;
+  for (int i = 0; i < 2; ++i)
+    if ((st = dalloc(p, &p->d_pos[i], 3 * (size_t)N))) return st;
+  if ((st = dalloc(p, &p->d_species, (size_t)N))) return st;
+  if ((st = dalloc(p, &p->d_key, (size_t)N))) return st;
+  if ((st = dalloc(p, &p->d_slot, (size_t)N))) return st;
+  if ((st = dalloc(p, &p->d_counts, (size_t)p->nkeys))) return st;
+  if ((st = dalloc(p, &p->d_starts, (size_t)p->nkeys + 1))) return st;
+  {
+    char *v;
+    if ((st = dalloc(p, &v, (size_t)N * (p->fp64 ? sizeof(PointRec<double>) : sizeof(PointRec<float>)))))
+      return st;
+    p->d_recs = v;
+    if ((st = dalloc(p, &v, (size_t)p->ntr * g.vol_real * rsz))) return st;
+    p->d_grid = v;
+    if ((st = dalloc(p, &v, (size_t)p->ntr * b.vol_cplx * 2 * rsz))) return st;
+    p->d_G = v;
+    for (int i = 0; i < 3; ++i) {
+      if ((st = dalloc(p, &v, (size_t)(p->hm[i] + 1) * rsz))) return st;
+      p->d_inv[i] = v;
+    }
+    if ((st = dalloc(p, &v, (size_t)p->nspecies * rsz))) return st;
+    p->d_strength = v;
+  }
+  if ((st = dalloc(p, &p->d_amp, (size_t)p->ntr))) return st;
+  if ((st = dalloc(p, &p->d_xcoef, 9 * (size_t)p->ntr))) return st;
+  if ((st = dalloc(p, &p->d_amp_sp, (size_t)p->nspecies))) return st;
+  if ((st = dalloc(p, &p->d_xcoef_sp, 9 * (size_t)p->nspecies))) return st;
+  if ((st = dalloc(p, &p->d_counts_sp, (size_t)p->nspecies))) return st;
+  if ((st = dalloc(p, &p->d_acc, (size_t)p->nquant * d->nq))) return st;
+  if ((st = dalloc(p, &p->d_den, (size_t)d->nq))) return st;
+  if ((st = dalloc(p, &p->d_cnt, (size_t)d->nq))) return st;
+  if (d->want_grid) {
+    p->gnum_half = (int64_t)(p->hm[0] + 1) * p->modes[1] * p->modes[2];
+    if ((st = dalloc(p, &p->d_gnum, (size_t)p->gnum_half))) return st;
+  }
+
+  // --- constant tables ----------------------------------------------------
+  cudaStream_t s = p->stream;
+  std::vector<uint8_t> sp_of(N);
+  for (int64_t i = 0; i < N; ++i) sp_of[i] = (uint8_t)species_of_type[d->type_id[i]];
+  cudaError_t e = cudaMemcpyAsync(p->d_species, sp_of.data(), (size_t)N, cudaMemcpyHostToDevice, s);
+  for (int i = 0; i < 3 && e == cudaSuccess; ++i) {
+    std::vector<double> ft = kernel_ft(p->nf[i], w, p->beta, p->hm[i]);
+    for (double &v : ft) v = 1.0 / v;
+    if (p->fp64) {
+      e = cudaMemcpyAsync(p->d_inv[i], ft.data(), ft.size() * 8, cudaMemcpyHostToDevice, s);
+    } else {
+      std::vector<float> f = to_r<float>(ft);
+      e = cudaMemcpyAsync(p->d_inv[i], f.data(), f.size() * 4, cudaMemcpyHostToDevice, s);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  }
+  if (e != cudaSuccess) return SQN_ERR_CUDA;
+  {
+    // strength of each species in the spread: 1 per species transform, or its
+    // amplitude in the single weighted transform.
+    std::vector<double> strength(p->nspecies, 1.0);
+    if (p->ntr == 1 && !d->partials && !xray) strength = p->amp_sp;
+    std::vector<double> amp_tr(p->ntr, 1.0), xc_tr(9 * (size_t)p->ntr, 0.0);
+    if (p->ntr > 1 || d->partials || xray) {
+      amp_tr = p->amp_sp;
+      xc_tr = p->xcoef_sp;
+    }
+    std::vector<double> cnt_sp(p->nspecies);
+    for (int k = 0; k < p->nspecies; ++k) cnt_sp[k] = (double)p->type_counts[p->species_type[k] - 1];
+    if (p->fp64) {
+      e = cudaMemcpy(p->d_strength, strength.data(), strength.size() * 8, cudaMemcpyHostToDevice);
+    } else {
+      std::vector<float> f = to_r<float>(strength);
+      e = cudaMemcpy(p->d_strength, f.data(), f.size() * 4, cudaMemcpyHostToDevice);
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(p->d_amp, amp_tr.data(), amp_tr.size() * 8, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(p->d_xcoef, xc_tr.data(), xc_tr.size() * 8, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(p->d_amp_sp, p->amp_sp.data(), p->amp_sp.size() * 8, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(p->d_xcoef_sp, p->xcoef_sp.data(), p->xcoef_sp.size() * 8, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(p->d_counts_sp, cnt_sp.data(), cnt_sp.size() * 8, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return SQN_ERR_CUDA;
+  }
+  if (cudaMemsetAsync(p->d_counts, 0, sizeof(int) * (size_t)p->nkeys, s) != cudaSuccess ||
+      cudaMemsetAsync(p->d_acc, 0, sizeof(double) * (size_t)p->nquant * d->nq, s) != cudaSuccess ||
+      cudaMemsetAsync(p->d_den, 0, sizeof(double) * (size_t)d->nq, s) != cudaSuccess ||
+      cudaMemsetAsync(p->d_cnt, 0, sizeof(double) * (size_t)d->nq, s) != cudaSuccess)
+    return SQN_ERR_CUDA;
+  if (p->d_gnum &&
+      cudaMemsetAsync(p->d_gnum, 0, sizeof(double) * (size_t)p->gnum_half, s) != cudaSuccess)
+    return SQN_ERR_CUDA;
+
+  // --- rows, shell normalisation, kept-mode count --------------------------
+  std::vector<int4> rows = build_rows(p->recip, p->hm, d->qmax);
+  p->nrows = (int)rows.size();
+  if (p->nrows == 0) return SQN_ERR_NO_MODES;
+  if ((st = dalloc(p, &p->d_rows, rows.size()))) return st;
+  if (cudaMemcpy(p->d_rows, rows.data(), rows.size() * sizeof(int4), cudaMemcpyHostToDevice) != cudaSuccess)
+    return SQN_ERR_CUDA;
+  {
+    BinGeom nb = b;
+    nb.ntr = p->nspecies;
+    nb.xray = xray ? 1 : 0;
+    if (launch_norms(p->d_rows, p->nrows, nb, p->d_amp_sp, p->d_xcoef_sp, p->d_counts_sp, p->d_den,
+                     p->d_cnt, p->nsm, s) != cudaSuccess)
+      return SQN_ERR_CUDA;
+    p->launches++;
+    p->den.assign(d->nq, 0.0);
+    p->cnt.assign(d->nq, 0.0);
+    if (cudaMemcpyAsync(p->den.data(), p->d_den, sizeof(double) * d->nq, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaMemcpyAsync(p->cnt.data(), p->d_cnt, sizeof(double) * d->nq, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+      return SQN_ERR_CUDA;
+    double tot = 0.0;
+    for (double c : p->cnt) tot += c;
+    p->nmodes = (int64_t)std::llround(tot);
+    if (p->nmodes == 0) return SQN_ERR_NO_MODES;
+  }
+
+  // --- cuFFT: batched 3D real-to-complex, out of place --------------------
+  {
+    if (cufftCreate(&p->fft) != CUFFT_SUCCESS) return SQN_ERR_CUFFT;
+    p->fft_ok = true;
+    long long n[3] = {p->nf[2], p->nf[1], p->nf[0]};
+    long long inembed[3] = {p->nf[2], p->nf[1], g.pitch};
+    long long onembed[3] = {p->nf[2], p->nf[1], b.c1};
+    size_t ws = 0;
+    if (cufftMakePlanMany64(p->fft, 3, n, inembed, 1, g.vol_real, onembed, 1, b.vol_cplx,
+                            p->fp64 ? CUFFT_D2Z : CUFFT_R2C, p->ntr, &ws) != CUFFT_SUCCESS)
+      return SQN_ERR_CUFFT;
+    p->device_bytes += (int64_t)ws;
+    if (cufftSetStream(p->fft, s) != CUFFT_SUCCESS) return SQN_ERR_CUFFT;
+  }
+  if (cudaStreamSynchronize(s) != cudaSuccess) return SQN_ERR_CUDA;
+  return warn;
+}
+
+template <typename R> int run_frame(sqn_plan *p, const double *dpos, int slot) {
+  const FrameGeom &g = p->fg;
+  cudaStream_t s = p->stream;
+  cudaEvent_t ev[5] = {};
+  if (p->timing) {
+    while (p->tev_pool.size() < p->tev_used + 5) {
+      cudaEvent_t e;
+      if (cudaEventCreate(&e) != cudaSuccess) return SQN_ERR_CUDA;
+      p->tev_pool.push_back(e);
+    }
+    for (int i = 0; i < 5; ++i) ev[i] = p->tev_pool[p->tev_used + i];
+    p->tev_used += 5;
+    cudaEventRecord(ev[0], s);
+  }
+  cudaError_t e = launch_prep<R>(dpos, p->d_species, g, p->d_counts, p->d_key, p->d_slot, s);
+  if (e == cudaSuccess) e = launch_scan(p->d_counts, p->d_starts, p->nkeys, s);
+  if (e == cudaSuccess)
+    e = launch_scatter<R>(dpos, p->d_species, g, p->d_key, p->d_slot, p->d_starts,
+                          (PointRec<R> *)p->d_recs, s);
+  if (e != cudaSuccess) return SQN_ERR_CUDA;
+  if (slot >= 0) cudaEventRecord(p->ev_free[slot], s);
+  if (p->timing) cudaEventRecord(ev[1], s);
+  e = launch_spread<R>((const PointRec<R> *)p->d_recs, p->d_starts, g, (const R *)p->d_strength,
+                       (R *)p->d_grid, s);
+  if (e != cudaSuccess) return SQN_ERR_CUDA;
+  if (p->timing) cudaEventRecord(ev[2], s);
+  cufftResult fr;
+  if (p->fp64)
+    fr = cufftExecD2Z(p->fft, (cufftDoubleReal *)p->d_grid, (cufftDoubleComplex *)p->d_G);
+  else
+    fr = cufftExecR2C(p->fft, (cufftReal *)p->d_grid, (cufftComplex *)p->d_G);
+  if (fr != CUFFT_SUCCESS) return SQN_ERR_CUFFT;
+  if (p->timing) cudaEventRecord(ev[3], s);
+  e = launch_bin<R>(p->d_rows, p->nrows, p->d_G, p->bg, (const R *)p->d_inv[0],
+                    (const R *)p->d_inv[1], (const R *)p->d_inv[2], p->d_amp, p->d_xcoef,
+                    p->d_acc, p->d_gnum, p->nsm, s);
+  if (e != cudaSuccess) return SQN_ERR_CUDA;
+  if (p->timing) cudaEventRecord(ev[4], s);
+  p->launches += 5;
+  p->nframes++;
+  return SQN_OK;
+}
+
+void harvest_timing(sqn_plan *p) {
+  for (size_t k = 0; k + 5 <= p->tev_used; k += 5) {
+    for (int st = 0; st < 4; ++st) {
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, p->tev_pool[k + st], p->tev_pool[k + st + 1]) == cudaSuccess)
+        p->stage_ms[st] += ms;
+      else
+        cudaGetLastError();
+    }
+    p->stage_frames++;
+  }
+  p->tev_used = 0;
+}
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Entry points
+// ---------------------------------------------------------------------------
+
+extern "C" {
+
+int sqn_abi_version(void) { return SQN_ABI_VERSION; }
+
+const char *sqn_error_string(int code) {
+  switch (code) {
+    case SQN_OK: return "ok";
+    case SQN_WARN_EPS_TOO_SMALL: return "warning: requested tolerance below what the precision or kernel width can reach";
+    case SQN_ERR_UPSAMPFAC_TOO_SMALL: return "upsampling factor must exceed 1";
+    case SQN_ERR_ALLOC: return "device memory allocation failed";
+    case SQN_ERR_CUDA: return "CUDA runtime error";
+    case SQN_ERR_PLAN_NOTVALID: return "invalid plan";
+    case SQN_ERR_NUM_NU_PTS_INVALID: return "invalid number of atoms";
+    case SQN_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case SQN_ERR_ABI_MISMATCH: return "descriptor ABI version does not match the library";
+    case SQN_ERR_NO_DEVICE: return "no usable CUDA device";
+    case SQN_ERR_GRID_TOO_LARGE: return "reciprocal grid exceeds the mode limit; reduce --qmax";
+    case SQN_ERR_NO_MODES: return "no reciprocal lattice points fall inside the requested q range";
+    case SQN_ERR_DEGENERATE_CELL: return "degenerate simulation cell";
+    case SQN_ERR_TYPE_ID: return "atom type id outside 1..ntypes";
+    case SQN_ERR_CUFFT: return "cuFFT failure";
+    case SQN_ERR_TIMEOUT: return "device wait timed out";
+    case SQN_ERR_NOT_SUPPORTED: return "configuration not supported by this build";
+    default: return "unknown status";
+  }
+}
+
+void sqn_default_desc(sqn_plan_desc *d) {
+  if (!d) return;
+  std::memset(d, 0, sizeof(*d));
+  d->abi_version = SQN_ABI_VERSION;
+  d->qmin = 0.0;
+  d->qmax = 20.0;
+  d->nq = 500;
+  d->eps = 1e-9;
+  d->norm = SQN_NORM_MEAN;
+  d->partials = 1;
+  d->weight = SQN_WEIGHT_UNIT;
+  d->precision = SQN_PREC_DOUBLE;
+}
+
+int sqn_plan_create(const sqn_plan_desc *desc, sqn_plan **out) {
+  if (!out) return SQN_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (!desc) return SQN_ERR_INVALID_ARGUMENT;
+  if (desc->abi_version != SQN_ABI_VERSION) return SQN_ERR_ABI_MISMATCH;
+  sqn_plan *p = new (std::nothrow) sqn_plan_s();
+  if (!p) return SQN_ERR_ALLOC;
+  int prev = -1;
+  cudaGetDevice(&prev);
+  int st = setup_plan(p, desc);
+  if (st > SQN_WARN_EPS_TOO_SMALL) {
+    free_plan(p);
+    if (prev >= 0) cudaSetDevice(prev);
+    return st;
+  }
+  if (prev >= 0) cudaSetDevice(prev);
+  *out = p;
+  return st;
+}
+
+int sqn_plan_info_get(const sqn_plan *p, sqn_plan_info *info) {
+  if (!p || !info) return SQN_ERR_INVALID_ARGUMENT;
+  std::memset(info, 0, sizeof(*info));
+  for (int i = 0; i < 3; ++i) {
+    info->modes[i] = p->modes[i];
+    info->nf[i] = p->nf[i];
+    info->tile[i] = p->fg.tile[i];
+  }
+  info->kernel_width = p->w;
+  info->gridpoints = p->gridpoints;
+  info->nmodes = p->nmodes;
+  info->upsampfac = p->sigma;
+  info->beta = p->beta;
+  info->eps_used = p->eps_used;
+  info->ntransforms = p->ntr;
+  info->nspecies = p->nspecies;
+  info->device_bytes = p->device_bytes;
+  return SQN_OK;
+}
+
+int sqn_accumulate_frames(sqn_plan *p, const double *pos, int64_t nframes, int32_t where) {
+  if (!p) return SQN_ERR_PLAN_NOTVALID;
+  if (!pos || nframes < 0 || (where != SQN_HOST && where != SQN_DEVICE))
+    return SQN_ERR_INVALID_ARGUMENT;
+  DeviceGuard guard(p->device);
+  const int64_t N = p->desc.natoms;
+  const size_t bytes = sizeof(double) * 3 * (size_t)N;
+  int last_slot = -1;
+  for (int64_t f = 0; f < nframes; ++f) {
+    const double *dpos;
+    int slot = -1;
+    if (where == SQN_HOST) {
+      slot = p->slot_next;
+      p->slot_next ^= 1;
+      // Double buffer: the copy into this slot waits until the frame that used
+      // it last has been sorted, and runs beside the previous frame's spread/FFT.
+      if (cudaStreamWaitEvent(p->copy_stream, p->ev_free[slot], 0) != cudaSuccess ||
+          cudaMemcpyAsync(p->d_pos[slot], pos + 3 * (size_t)N * f, bytes, cudaMemcpyHostToDevice,
+                          p->copy_stream) != cudaSuccess ||
+          cudaEventRecord(p->ev_copied[slot], p->copy_stream) != cudaSuccess ||
+          cudaStreamWaitEvent(p->stream, p->ev_copied[slot], 0) != cudaSuccess)
+        return SQN_ERR_CUDA;
+      dpos = p->d_pos[slot];
+      last_slot = slot;
+    } else {
+      dpos = pos + 3 * (size_t)N * f;
+    }
+    const int st = p->fp64 ? run_frame<double>(p, dpos, slot) : run_frame<float>(p, dpos, slot);
+    if (st != SQN_OK) return st;
+  }
+  // Host positions must have been read before the call returns.
+  if (last_slot >= 0 && cudaEventSynchronize(p->ev_copied[last_slot]) != cudaSuccess)
+    return SQN_ERR_CUDA;
+  return SQN_OK;
+}
+
+int sqn_sync(sqn_plan *p) {
+  if (!p) return SQN_ERR_PLAN_NOTVALID;
+  DeviceGuard guard(p->device);
+  return cuda_status(cudaStreamSynchronize(p->stream));
+}
+
+int sqn_peek_num_async(sqn_plan *p, double *num_host) {
+  if (!p) return SQN_ERR_PLAN_NOTVALID;
+  if (!num_host) return SQN_ERR_INVALID_ARGUMENT;
+  DeviceGuard guard(p->device);
+  return cuda_status(cudaMemcpyAsync(num_host, p->d_acc, sizeof(double) * p->desc.nq,
+                                     cudaMemcpyDeviceToHost, p->stream));
+}
+
+int sqn_get_accumulators(sqn_plan *p, double *num, double *den, int64_t *shell_count,
+                         double *partial_num, double *gnum, double *gden, int64_t *nframes) {
+  if (!p) return SQN_ERR_PLAN_NOTVALID;
+  DeviceGuard guard(p->device);
+  if (cudaStreamSynchronize(p->stream) != cudaSuccess) return SQN_ERR_CUDA;
+  const int nq = p->desc.nq, T = p->desc.ntypes;
+  std::vector<double> acc((size_t)p->nquant * nq);
+  if (cudaMemcpy(acc.data(), p->d_acc, acc.size() * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return SQN_ERR_CUDA;
+  if (num) std::memcpy(num, acc.data(), sizeof(double) * nq);
+  if (den) std::memcpy(den, p->den.data(), sizeof(double) * nq);
+  if (shell_count)
+    for (int s = 0; s < nq; ++s) shell_count[s] = (int64_t)std::llround(p->cnt[s]);
+  if (partial_num) {
+    std::memset(partial_num, 0, sizeof(double) * (size_t)T * T * nq);
+    if (p->desc.partials) {
+      int q = 1;
+      for (int a = 0; a < p->ntr; ++a)
+        for (int c = a; c < p->ntr; ++c, ++q) {
+          const int ta = p->species_type[a], tb = p->species_type[c];
+          for (int s = 0; s < nq; ++s)
+            partial_num[(size_t)(ta - 1) + (size_t)T * ((size_t)(tb - 1) + (size_t)T * s)] =
+                acc[(size_t)q * nq + s];
+        }
+    }
+  }
+  if (gnum || gden) {
+    if (!p->desc.want_grid) return SQN_ERR_INVALID_ARGUMENT;
+    std::vector<double> half((size_t)p->gnum_half);
+    if (gnum &&
+        cudaMemcpy(half.data(), p->d_gnum, half.size() * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+      return SQN_ERR_CUDA;
+    const int *m = p->modes, *hm = p->hm;
+    const bool xray = p->desc.weight == SQN_WEIGHT_XRAY;
+    int64_t g = 0;
+    for (int p3 = 1; p3 <= m[2]; ++p3)
+      for (int p2 = 1; p2 <= m[1]; ++p2)
+        for (int p1 = 1; p1 <= m[0]; ++p1, ++g) {
+          int h1 = p1 - (m[0] + 1) / 2, h2 = p2 - (m[1] + 1) / 2, h3 = p3 - (m[2] + 1) / 2;
+          if (gnum) {
+            int a1 = h1, a2 = h2, a3 = h3;
+            if (h1 < 0) { a1 = -h1; a2 = -h2; a3 = -h3; }
+            gnum[g] = half[((size_t)(a3 + hm[2]) * m[1] + (size_t)(a2 + hm[1])) * (hm[0] + 1) + a1];
+          }
+          if (gden) {
+            gden[g] = 0.0;
+            if (h1 == 0 && h2 == 0 && h3 == 0) continue;
+            const double ql = qlen_ref(p->recip, h1, h2, h3);
+            if (ql > p->desc.qmax || ql < p->desc.qmin) continue;
+            double dd;
+            if (p->desc.norm == SQN_NORM_NATOM) {
+              dd = (double)p->desc.natoms;
+            } else {
+              double sw = 0.0, sw2 = 0.0;
+              for (int k = 0; k < p->nspecies; ++k) {
+                const double w = xray ? xray_f_host(&p->xcoef_sp[9 * k], ql) : p->amp_sp[k];
+                const double c = (double)p->type_counts[p->species_type[k] - 1];
+                sw = sw + c * w;
+                sw2 = sw2 + c * w * w;
+              }
+              dd = p->desc.norm == SQN_NORM_MEAN ? sw * sw / (double)p->desc.natoms : sw2;
+            }
+            gden[g] = dd;
+          }
+        }
+  }
+  if (nframes) *nframes = p->nframes;
+  return SQN_OK;
+}
+
+int sqn_finalize(sqn_plan *p, int32_t faber_ziman, double *S_total, double *S_partial,
+                 double *S_grid, int64_t *nframes) {
+  if (!p) return SQN_ERR_PLAN_NOTVALID;
+  const int nq = p->desc.nq, T = p->desc.ntypes;
+  std::vector<double> num(nq), den(nq), pn;
+  std::vector<int64_t> cnt(nq);
+  if (S_partial) pn.resize((size_t)T * T * nq);
+  int st = sqn_get_accumulators(p, num.data(), den.data(), cnt.data(),
+                                S_partial ? pn.data() : nullptr, nullptr, nullptr, nullptr);
+  if (st) return st;
+  const double frames = (double)std::max<int64_t>(p->nframes, 1);
+  if (S_total)
+    for (int s = 0; s < nq; ++s) S_total[s] = den[s] > 0.0 ? num[s] / (frames * den[s]) : 0.0;
+  if (S_partial) {
+    const double N = (double)p->desc.natoms;
+    for (int s = 0; s < nq; ++s)
+      for (int ib = 1; ib <= T; ++ib)
+        for (int ia = 1; ia <= T; ++ia) {
+          const size_t k = (size_t)(ia - 1) + (size_t)T * ((size_t)(ib - 1) + (size_t)T * s);
+          double v = pn[k] / (frames * N * (double)std::max<int64_t>(cnt[s], 1));
+          if (faber_ziman) {
+            const double xa = (double)p->type_counts[ia - 1] / N, xb = (double)p->type_counts[ib - 1] / N;
+            v = xa * xb <= 0.0 ? 0.0 : (v - (ia == ib ? xa : 0.0)) / (xa * xb) + 1.0;
+          }
+          S_partial[k] = v;
+        }
+  }
+  if (S_grid) {
+    if (!p->desc.want_grid) return SQN_ERR_INVALID_ARGUMENT;
+    std::vector<double> gnum((size_t)p->gridpoints), gden((size_t)p->gridpoints);
+    st = sqn_get_accumulators(p, nullptr, nullptr, nullptr, nullptr, gnum.data(), gden.data(), nullptr);
+    if (st) return st;
+    const int *m = p->modes;
+    int64_t g = 0, im = 0;
+    for (int p3 = 1; p3 <= m[2]; ++p3)
+      for (int p2 = 1; p2 <= m[1]; ++p2)
+        for (int p1 = 1; p1 <= m[0]; ++p1, ++g) {
+          const int h1 = p1 - (m[0] + 1) / 2, h2 = p2 - (m[1] + 1) / 2, h3 = p3 - (m[2] + 1) / 2;
+          if (h1 == 0 && h2 == 0 && h3 == 0) continue;
+          const double ql = qlen_ref(p->recip, h1, h2, h3);
+          if (ql > p->desc.qmax || ql < p->desc.qmin) continue;
+          S_grid[im++] = gden[g] > 0.0 ? gnum[g] / (frames * gden[g]) : 0.0;
+        }
+  }
+  if (nframes) *nframes = p->nframes;
+  return SQN_OK;
+}
+
+int sqn_reset(sqn_plan *p) {
+  if (!p) return SQN_ERR_PLAN_NOTVALID;
+  DeviceGuard guard(p->device);
+  if (cudaStreamSynchronize(p->stream) != cudaSuccess) return SQN_ERR_CUDA;
+  cudaError_t e = cudaMemset(p->d_acc, 0, sizeof(double) * (size_t)p->nquant * p->desc.nq);
+  if (e == cudaSuccess && p->d_gnum) e = cudaMemset(p->d_gnum, 0, sizeof(double) * (size_t)p->gnum_half);
+  p->nframes = 0;
+  p->tev_used = 0;
+  for (double &v : p->stage_ms) v = 0.0;
+  p->stage_frames = 0;
+  return cuda_status(e);
+}
+
+int sqn_stage_times(sqn_plan *p, double *out, int32_t n) {
+  if (!p) return SQN_ERR_PLAN_NOTVALID;
+  if (!out || n < 1) return SQN_ERR_INVALID_ARGUMENT;
+  if (!p->timing) return SQN_ERR_NOT_SUPPORTED;
+  DeviceGuard guard(p->device);
+  if (cudaStreamSynchronize(p->stream) != cudaSuccess) return SQN_ERR_CUDA;
+  harvest_timing(p);
+  double v[5] = {p->stage_ms[0], p->stage_ms[1], p->stage_ms[2], p->stage_ms[3], (double)p->stage_frames};
+  for (int i = 0; i < n && i < 5; ++i) out[i] = v[i];
+  return SQN_OK;
+}
+
+int64_t sqn_launch_count(const sqn_plan *p) { return p ? p->launches : -1; }
+
+int sqn_plan_destroy(sqn_plan *p) {
+  if (!p) return SQN_ERR_PLAN_NOTVALID;
+  free_plan(p);
+  return SQN_OK;
+}
+
+}  // extern "C"

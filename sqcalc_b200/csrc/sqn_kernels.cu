@@ -1,0 +1,640 @@
+// Device kernels of the static S(q) hot path (sm_100a).
+//
+// Per frame:
+//   k_prep     wrap each atom into the cell, find the first cell of its ES
+//              kernel support on the fine grid and its home (tile, transform)
+//              bin; count the bin                               [HBM: positions]
+//   k_scan     exclusive scan of the bin counts (one CTA) and reset the counts
+//   k_scatter  write each atom's 16-byte point record into its bin slot
+//   k_spread   gather spreading: one CTA owns one fine-grid tile of one
+//              transform, stages the points of the bins that can reach it,
+//              evaluates the separable ES kernel rows in shared memory and
+//              accumulates every cell in registers; each cell is written once,
+//              coalesced, so the grid needs no zeroing and no atomics
+//                                                              [HBM: grid write]
+//   (cuFFT R2C / D2Z, out of place)
+//   k_bin      deconvolve the half-space modes, form the weighted total and the
+//              pair products Re(rho_a rho_b*) and add them, in FP64, to
+//              per-CTA shared-memory shell histograms flushed once per CTA
+//                                                  [HBM: kept modes read once]
+//
+// The reference does the same math as cuFINUFFT spread + cuFFT + deconvolve
+// (external/finufft/src/cuda/3d/spreadinterp3d.cuh:276-383,
+//  external/finufft/src/cuda/deconvolve_wrapper.cu:76-118) followed by the host
+// loops of src/sqc_structure_factor.f90:457-643.
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "sqn_internal.h"
+
+namespace sqn {
+
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+// ---------------------------------------------------------------------------
+// Atom -> fine grid
+// ---------------------------------------------------------------------------
+
+struct AtomCell {
+  int ix0[3];     // first support cell, wrapped into [0, nf)
+  double off[3];  // (X - ix0) - (w/2 - 1/2), in (-1/2, 1/2]
+};
+
+// s = A^-1 (r - origin), s -= floor(s)  (cell_fractional, src/sqc_cell.f90:143-152,
+// and the wrap of src/sqc_gpu.f90:230-236); X = nf * s is the fine-grid coordinate.
+__device__ __forceinline__ void atom_cell(const double *__restrict__ pos, int64_t i,
+                                          const FrameGeom &g, AtomCell &c) {
+  const double d0 = __dsub_rn(pos[3 * i + 0], g.origin[0]);
+  const double d1 = __dsub_rn(pos[3 * i + 1], g.origin[1]);
+  const double d2 = __dsub_rn(pos[3 * i + 2], g.origin[2]);
+  const double halfw = 0.5 * (double)g.w;
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    double s = __dadd_rn(__dadd_rn(__dmul_rn(g.inv[r], d0), __dmul_rn(g.inv[3 + r], d1)),
+                         __dmul_rn(g.inv[6 + r], d2));
+    s = __dsub_rn(s, floor(s));
+    // A non-finite coordinate must not index outside the grid: park it at 0.
+    if (!(s >= 0.0 && s <= 1.0)) s = 0.0;
+    const double X = __dmul_rn((double)g.nf[r], s);
+    const double start = ceil(__dsub_rn(X, halfw));
+    c.off[r] = __dsub_rn(__dsub_rn(X, start), halfw - 0.5);
+    int ix0 = (int)start;
+    if (ix0 < 0) ix0 += g.nf[r];
+    if (ix0 >= g.nf[r]) ix0 -= g.nf[r];
+    c.ix0[r] = ix0;
+  }
+}
+
+__device__ __forceinline__ uint32_t home_key(const AtomCell &c, int sp, const FrameGeom &g,
+                                             int &l0, int &l1, int &l2) {
+  const int t0 = c.ix0[0] / g.tile[0], t1 = c.ix0[1] / g.tile[1], t2 = c.ix0[2] / g.tile[2];
+  l0 = c.ix0[0] - t0 * g.tile[0];
+  l1 = c.ix0[1] - t1 * g.tile[1];
+  l2 = c.ix0[2] - t2 * g.tile[2];
+  const int tr = g.ntr > 1 ? sp : 0;
+  return (uint32_t)tr * (uint32_t)g.ntiles + (uint32_t)((t2 * g.ntile[1] + t1) * g.ntile[0] + t0);
+}
+
+__global__ void k_prep(const double *__restrict__ pos, const uint8_t *__restrict__ species,
+                       FrameGeom g, int *__restrict__ counts, uint32_t *__restrict__ key,
+                       uint32_t *__restrict__ slot) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < g.natoms;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    AtomCell c;
+    atom_cell(pos, i, g, c);
+    int l0, l1, l2;
+    const uint32_t k = home_key(c, species[i], g, l0, l1, l2);
+    key[i] = k;
+    slot[i] = (uint32_t)atomicAdd(&counts[k], 1);
+  }
+}
+
+// Exclusive scan of counts[0..n) into starts[0..n], then zero counts for the
+// next frame.  One CTA of 1024 threads, each owning a contiguous run.
+__global__ void __launch_bounds__(1024) k_scan(int *__restrict__ counts, int *__restrict__ starts,
+                                               int n) {
+  __shared__ int wsum[32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int per = (n + 1023) / 1024;
+  const int lo = min(n, tid * per), hi = min(n, lo + per);
+  int s = 0;
+  for (int i = lo; i < hi; ++i) s += counts[i];
+  int v = s;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int t = __shfl_up_sync(FULL, v, o);
+    if (lane >= o) v += t;
+  }
+  if (lane == 31) wsum[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    int x = wsum[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int t = __shfl_up_sync(FULL, x, o);
+      if (lane >= o) x += t;
+    }
+    wsum[lane] = x;
+  }
+  __syncthreads();
+  int run = v - s + (warp > 0 ? wsum[warp - 1] : 0);
+  for (int i = lo; i < hi; ++i) {
+    const int c = counts[i];
+    starts[i] = run;
+    run += c;
+    counts[i] = 0;
+  }
+  if (tid == 1023) starts[n] = run;
+}
+
+template <typename R>
+__global__ void k_scatter(const double *__restrict__ pos, const uint8_t *__restrict__ species,
+                          FrameGeom g, const uint32_t *__restrict__ key,
+                          const uint32_t *__restrict__ slot, const int *__restrict__ starts,
+                          PointRec<R> *__restrict__ recs) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < g.natoms;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    AtomCell c;
+    atom_cell(pos, i, g, c);
+    const int sp = species[i];
+    int l0, l1, l2;
+    (void)home_key(c, sp, g, l0, l1, l2);
+    PointRec<R> r;
+    r.f[0] = (R)c.off[0];
+    r.f[1] = (R)c.off[1];
+    r.f[2] = (R)c.off[2];
+    r.packed = (uint32_t)l0 | ((uint32_t)l1 << 8) | ((uint32_t)l2 << 16) | ((uint32_t)sp << 24);
+    if constexpr (sizeof(R) == 8) r.pad = 0;
+    recs[(int64_t)starts[key[i]] + slot[i]] = r;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// ES kernel: phi(t) = exp(beta (sqrt(1 - (2t/w)^2) - 1)) on |t| < w/2, else 0
+// (external/finufft/include/cufinufft/spreadinterp.h:84-98).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float es_phi(float t, float c2, float beta) {
+  const float z2 = c2 * t * t;
+  return z2 < 1.0f ? expf(beta * (sqrtf(1.0f - z2) - 1.0f)) : 0.0f;
+}
+__device__ __forceinline__ double es_phi(double t, double c2, double beta) {
+  const double z2 = c2 * t * t;
+  return z2 < 1.0 ? exp(beta * (sqrt(1.0 - z2) - 1.0)) : 0.0;
+}
+
+// ---------------------------------------------------------------------------
+// Gather spreading, one CTA per (tile, transform).
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void __launch_bounds__(SPREAD_THREADS)
+    k_spread(const PointRec<R> *__restrict__ recs, const int *__restrict__ starts, FrameGeom g,
+             const R *__restrict__ strength, R *__restrict__ grid) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R *s_rows = reinterpret_cast<R *>(smem_raw);                      // [CHUNK][ROW]
+  int4 *s_meta = reinterpret_cast<int4 *>(s_rows + CHUNK * ROW);    // [CHUNK] rx, ry, rz, sp
+  R *s_off = reinterpret_cast<R *>(s_meta + CHUNK);                 // [CHUNK][3]
+  __shared__ int s_bstart[MAX_NB];
+  __shared__ int s_bpref[MAX_NB + 1];
+  __shared__ int s_borg[MAX_NB][3];
+  __shared__ int s_wcount[SPREAD_THREADS / 32];
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int tile = blockIdx.x, tr = blockIdx.y;
+  const int t0 = tile % g.ntile[0];
+  const int t1 = (tile / g.ntile[0]) % g.ntile[1];
+  const int t2 = tile / (g.ntile[0] * g.ntile[1]);
+  const int X0 = t0 * g.tile[0], Y0 = t1 * g.tile[1], Z0 = t2 * g.tile[2];
+  const int tx = min(g.tile[0], g.nf[0] - X0);
+  const int ty = min(g.tile[1], g.nf[1] - Y0);
+  const int tz = min(g.tile[2], g.nf[2] - Z0);
+  const int nb = g.nbk[0] * g.nbk[1] * g.nbk[2];
+
+  if (tid < nb) {
+    const int kx = tid % g.nbk[0], ky = (tid / g.nbk[0]) % g.nbk[1],
+              kz = tid / (g.nbk[0] * g.nbk[1]);
+    int bx = t0 - kx, by = t1 - ky, bz = t2 - kz;
+    if (bx < 0) bx += g.ntile[0];
+    if (by < 0) by += g.ntile[1];
+    if (bz < 0) bz += g.ntile[2];
+    const int key = tr * g.ntiles + (bz * g.ntile[1] + by) * g.ntile[0] + bx;
+    const int st = starts[key];
+    s_bstart[tid] = st;
+    s_bpref[tid + 1] = starts[key + 1] - st;
+    s_borg[tid][0] = bx * g.tile[0];
+    s_borg[tid][1] = by * g.tile[1];
+    s_borg[tid][2] = bz * g.tile[2];
+  }
+  __syncthreads();
+  if (tid == 0) {
+    s_bpref[0] = 0;
+    for (int b = 0; b < nb; ++b) s_bpref[b + 1] += s_bpref[b];
+  }
+  __syncthreads();
+  const int total = s_bpref[nb];
+
+  R acc[TILE_Z];
+#pragma unroll
+  for (int z = 0; z < TILE_Z; ++z) acc[z] = R(0);
+  const R halfw = R(0.5) * (R)g.w - R(0.5);
+  const R c2 = R(4) / ((R)g.w * (R)g.w);
+  const R beta = (R)g.beta;
+
+  for (int base = 0; base < total; base += CHUNK) {
+    const int i = base + tid;
+    bool keep = false;
+    int4 meta = make_int4(0, 0, 0, 0);
+    R o0 = 0, o1 = 0, o2 = 0;
+    if (i < total) {
+      int b = 0;
+      while (i >= s_bpref[b + 1]) ++b;
+      const PointRec<R> rec = recs[s_bstart[b] + (i - s_bpref[b])];
+      const int lx0 = rec.packed & 255, ly0 = (rec.packed >> 8) & 255,
+                lz0 = (rec.packed >> 16) & 255;
+      int rx = s_borg[b][0] + lx0 - X0;
+      int ry = s_borg[b][1] + ly0 - Y0;
+      int rz = s_borg[b][2] + lz0 - Z0;
+      if (rx < 0) rx += g.nf[0];
+      if (ry < 0) ry += g.nf[1];
+      if (rz < 0) rz += g.nf[2];
+      keep = (rx < tx || rx + g.w > g.nf[0]) && (ry < ty || ry + g.w > g.nf[1]) &&
+             (rz < tz || rz + g.w > g.nf[2]);
+      meta = make_int4(rx, ry, rz, (int)(rec.packed >> 24));
+      o0 = rec.f[0];
+      o1 = rec.f[1];
+      o2 = rec.f[2];
+    }
+    const unsigned bal = __ballot_sync(FULL, keep);
+    if (lane == 0) s_wcount[warp] = __popc(bal);
+    __syncthreads();
+    int wbase = 0, npts = 0;
+#pragma unroll
+    for (int k = 0; k < SPREAD_THREADS / 32; ++k) {
+      const int cnt = s_wcount[k];
+      wbase += k < warp ? cnt : 0;
+      npts += cnt;
+    }
+    if (keep) {
+      const int p = wbase + __popc(bal & ((1u << lane) - 1u));
+      s_meta[p] = meta;
+      s_off[3 * p + 0] = o0;
+      s_off[3 * p + 1] = o1;
+      s_off[3 * p + 2] = o2;
+    }
+    __syncthreads();
+
+    // Kernel rows of every staged point, shifted into tile coordinates.
+    for (int e = tid; e < npts * ROW; e += SPREAD_THREADS) {
+      const int p = e / ROW, c = e - p * ROW;
+      const int4 m = s_meta[p];
+      int d, cell, te, r, n;
+      if (c < TILE_X) {
+        d = 0; cell = c; te = tx; r = m.x; n = g.nf[0];
+      } else if (c < TILE_X + TILE_Y) {
+        d = 1; cell = c - TILE_X; te = ty; r = m.y; n = g.nf[1];
+      } else {
+        d = 2; cell = c - TILE_X - TILE_Y; te = tz; r = m.z; n = g.nf[2];
+      }
+      R v = R(0);
+      if (cell < te) {
+        int k = cell - r;
+        if (k < 0) k += n;
+        if (k < g.w) {
+          const R t = ((R)k - halfw) - s_off[3 * p + d];
+          v = es_phi(t, c2, beta);
+          if (d == 2) v *= strength[m.w];
+        }
+      }
+      s_rows[e] = v;
+    }
+    __syncthreads();
+
+    for (int p = 0; p < npts; ++p) {
+      const R *row = s_rows + p * ROW;
+      const R kyv = row[TILE_X + warp];
+      if (kyv != R(0)) {
+        const R a = row[lane] * kyv;
+#pragma unroll
+        for (int z = 0; z < TILE_Z; ++z) acc[z] = fma(a, row[TILE_X + TILE_Y + z], acc[z]);
+      }
+    }
+    __syncthreads();
+  }
+
+  if (lane < tx && warp < ty) {
+    R *out = grid + (int64_t)tr * g.vol_real +
+             ((int64_t)Z0 * g.nf[1] + (Y0 + warp)) * g.pitch + X0 + lane;
+    const int64_t zs = (int64_t)g.nf[1] * g.pitch;
+#pragma unroll
+    for (int z = 0; z < TILE_Z; ++z)
+      if (z < tz) out[z * zs] = acc[z];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Mode bookkeeping shared by the bin and norm kernels.
+// ---------------------------------------------------------------------------
+
+// |q| of mode h in the reference's operation order, without contraction
+// (src/sqc_structure_factor.f90:366-368), so that shells match bit for bit.
+__device__ __forceinline__ double qlen_exact(const BinGeom &b, int h1, int h2, int h3) {
+  double q[3];
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+    q[r] = __dadd_rn(__dadd_rn(__dmul_rn(b.recip[r], (double)h1), __dmul_rn(b.recip[3 + r], (double)h2)),
+                     __dmul_rn(b.recip[6 + r], (double)h3));
+  return __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(q[0], q[0]), __dmul_rn(q[1], q[1])),
+                              __dmul_rn(q[2], q[2])));
+}
+
+// shell = int((|q| - qmin)/dq) clamped to [0, nq)   (:396-399, zero based)
+__device__ __forceinline__ int shell_of(const BinGeom &b, double ql) {
+  int s = (int)__ddiv_rn(__dsub_rn(ql, b.qmin), b.dq);
+  return min(max(s, 0), b.nq - 1);
+}
+
+// IT92 form factor f(q) = sum_i a_i exp(-b_i (q/4pi)^2) + c (src/sqc_elements.f90:226-239).
+__device__ __forceinline__ double xray_f(const double *__restrict__ c, double q) {
+  double st = q / (4.0 * 3.14159265358979323846);
+  st = st * st;
+  double f = c[8];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) f = f + c[i] * exp(-c[4 + i] * st);
+  return f;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+  return v;
+}
+
+// Add v to hist[s]: one atomic per warp when every active lane has the same shell.
+__device__ __forceinline__ void hist_add(double *hist, int s, double v, bool keep, bool uni,
+                                         int s0, int lane) {
+  if (uni) {
+    v = warp_sum(keep ? v : 0.0);
+    if (lane == 0) atomicAdd(&hist[s0], v);
+  } else if (keep) {
+    atomicAdd(&hist[s], v);
+  }
+}
+
+template <typename R> struct Cplx;
+template <> struct Cplx<float> { using T = float2; };
+template <> struct Cplx<double> { using T = double2; };
+
+// ---------------------------------------------------------------------------
+// Fused deconvolve + weighted total + pair products + FP64 shell binning.
+// NT > 0: exactly NT transforms (unrolled).  NT == 0: any ntr <= MAX_FAST_T.
+// Rows (h2, h3) are dealt to warps; lanes walk h1 >= 0 (32 consecutive complex
+// values per warp and transform, one coalesced read).
+// ---------------------------------------------------------------------------
+template <typename R, int NT, bool SMEM>
+__global__ void __launch_bounds__(256)
+    k_bin(const int4 *__restrict__ rows, int nrows, const typename Cplx<R>::T *__restrict__ G,
+          BinGeom b, const R *__restrict__ inv1, const R *__restrict__ inv2,
+          const R *__restrict__ inv3, const double *__restrict__ amp,
+          const double *__restrict__ xcoef, double *__restrict__ acc, double *__restrict__ gnum) {
+  extern __shared__ double s_hist[];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nwarps = blockDim.x >> 5;
+  const int nhist = b.nquant * b.nq;
+  double *hist = SMEM ? s_hist : acc;
+  if (SMEM) {
+    for (int i = tid; i < nhist; i += blockDim.x) s_hist[i] = 0.0;
+    __syncthreads();
+  }
+  const int ntr = NT > 0 ? NT : b.ntr;
+  constexpr int TM = NT > 0 ? NT : MAX_FAST_T;
+
+  for (int r = blockIdx.x * nwarps + warp; r < nrows; r += gridDim.x * nwarps) {
+    const int4 row = rows[r];
+    const int h2 = row.x, h3 = row.y, lo = row.z, hi = row.w;
+    const int64_t ky = h2 >= 0 ? h2 : b.nf[1] + h2;
+    const int64_t kz = h3 >= 0 ? h3 : b.nf[2] + h3;
+    const int64_t rowbase = (kz * b.nf[1] + ky) * b.c1;
+    const R dyz = inv2[abs(h2)] * inv3[abs(h3)];
+    const int64_t gbase =
+        ((int64_t)(h3 + b.hm[2]) * b.m2 + (int64_t)(h2 + b.hm[1])) * (int64_t)(b.hm[0] + 1);
+    for (int h1b = lo; h1b <= hi; h1b += 32) {
+      const int h1 = h1b + lane;
+      bool keep = h1 <= hi;
+      double ql = 0.0;
+      int s = 0;
+      if (keep) {
+        ql = qlen_exact(b, h1, h2, h3);
+        keep = !(h1 == 0 && h2 == 0 && h3 == 0) && ql >= b.qmin && ql <= b.qmax;
+        s = shell_of(b, ql);
+      }
+      const unsigned act = __ballot_sync(FULL, keep);
+      if (act == 0u) continue;
+      double re[TM], im[TM];
+      double tre = 0.0, tim = 0.0;
+      const double mult = h1 > 0 ? 2.0 : 1.0;
+#pragma unroll
+      for (int t = 0; t < TM; ++t) {
+        re[t] = 0.0;
+        im[t] = 0.0;
+      }
+      if (keep) {
+        const R dec = inv1[h1] * dyz;
+#pragma unroll
+        for (int t = 0; t < TM; ++t) {
+          if (t < ntr) {
+            const typename Cplx<R>::T v = G[(int64_t)t * b.vol_cplx + rowbase + h1];
+            re[t] = (double)(v.x * dec);
+            im[t] = (double)(v.y * dec);
+            const double a = b.xray ? xray_f(xcoef + 9 * t, ql) : amp[t];
+            tre += a * re[t];
+            tim += a * im[t];
+          }
+        }
+      }
+      const double I = tre * tre + tim * tim;
+      if (b.want_grid && keep) gnum[gbase + h1] += I;
+      const int s0 = __shfl_sync(FULL, s, __ffs(act) - 1);
+      const bool uni = __all_sync(FULL, !keep || s == s0);
+      hist_add(hist, s, mult * I, keep, uni, s0, lane);
+      if (b.partials) {
+        int p = 1;
+#pragma unroll
+        for (int a = 0; a < TM; ++a) {
+#pragma unroll
+          for (int c = a; c < TM; ++c) {
+            if (c < ntr) {
+              hist_add(hist + p * b.nq, s, mult * (re[a] * re[c] + im[a] * im[c]), keep, uni,
+                       s0, lane);
+              ++p;
+            }
+          }
+        }
+      }
+    }
+  }
+  if (SMEM) {
+    __syncthreads();
+    for (int i = tid; i < nhist; i += blockDim.x) {
+      const double v = s_hist[i];
+      if (v != 0.0) atomicAdd(&acc[i], v);
+    }
+  }
+}
+
+// den(shell) and shell_count(shell) over all kept modes (both halves),
+// mode_denominator of src/sqc_structure_factor.f90:425-451.
+__global__ void __launch_bounds__(256)
+    k_norms(const int4 *__restrict__ rows, int nrows, BinGeom b, const double *__restrict__ amp,
+            const double *__restrict__ xcoef, const double *__restrict__ counts_t,
+            double *__restrict__ den, double *__restrict__ cnt) {
+  extern __shared__ double s_n[];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nwarps = blockDim.x >> 5;
+  for (int i = tid; i < 2 * b.nq; i += blockDim.x) s_n[i] = 0.0;
+  __syncthreads();
+  for (int r = blockIdx.x * nwarps + warp; r < nrows; r += gridDim.x * nwarps) {
+    const int4 row = rows[r];
+    const int h2 = row.x, h3 = row.y, lo = row.z, hi = row.w;
+    for (int h1b = lo; h1b <= hi; h1b += 32) {
+      const int h1 = h1b + lane;
+      bool keep = h1 <= hi;
+      double ql = 0.0;
+      int s = 0;
+      if (keep) {
+        ql = qlen_exact(b, h1, h2, h3);
+        keep = !(h1 == 0 && h2 == 0 && h3 == 0) && ql >= b.qmin && ql <= b.qmax;
+        s = shell_of(b, ql);
+      }
+      if (!keep) continue;
+      const double mult = h1 > 0 ? 2.0 : 1.0;
+      double d;
+      if (b.norm == 3) {
+        d = (double)b.natoms;
+      } else {
+        double sw = 0.0, sw2 = 0.0;
+        for (int t = 0; t < b.ntr; ++t) {
+          const double w = b.xray ? xray_f(xcoef + 9 * t, ql) : amp[t];
+          sw = sw + counts_t[t] * w;
+          sw2 = sw2 + counts_t[t] * w * w;
+        }
+        d = b.norm == 1 ? sw * sw / (double)b.natoms : sw2;
+      }
+      atomicAdd(&s_n[s], mult * d);
+      atomicAdd(&s_n[b.nq + s], mult);
+    }
+  }
+  __syncthreads();
+  for (int i = tid; i < b.nq; i += blockDim.x) {
+    if (s_n[i] != 0.0) atomicAdd(&den[i], s_n[i]);
+    if (s_n[b.nq + i] != 0.0) atomicAdd(&cnt[i], s_n[b.nq + i]);
+  }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Launch wrappers
+// ---------------------------------------------------------------------------
+
+static int grid_for(int64_t n, int threads) {
+  int64_t b = (n + threads - 1) / threads;
+  if (b > 148 * 32) b = 148 * 32;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+template <typename R>
+cudaError_t launch_prep(const double *pos, const uint8_t *species, const FrameGeom &g,
+                        int *counts, uint32_t *key, uint32_t *slot, cudaStream_t s) {
+  k_prep<<<grid_for(g.natoms, 256), 256, 0, s>>>(pos, species, g, counts, key, slot);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scan(int *counts, int *starts, int n, cudaStream_t s) {
+  k_scan<<<1, 1024, 0, s>>>(counts, starts, n);
+  return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_scatter(const double *pos, const uint8_t *species, const FrameGeom &g,
+                           const uint32_t *key, const uint32_t *slot, const int *starts,
+                           PointRec<R> *recs, cudaStream_t s) {
+  k_scatter<R><<<grid_for(g.natoms, 256), 256, 0, s>>>(pos, species, g, key, slot, starts, recs);
+  return cudaGetLastError();
+}
+
+size_t spread_smem_bytes(bool fp64) {
+  const size_t r = fp64 ? 8 : 4;
+  return (size_t)CHUNK * ROW * r + (size_t)CHUNK * sizeof(int4) + (size_t)CHUNK * 3 * r;
+}
+
+cudaError_t spread_set_attributes() {
+  cudaError_t e = cudaFuncSetAttribute(k_spread<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)spread_smem_bytes(false));
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_spread<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)spread_smem_bytes(true));
+}
+
+template <typename R>
+cudaError_t launch_spread(const PointRec<R> *recs, const int *starts, const FrameGeom &g,
+                          const R *strength, R *grid, cudaStream_t s) {
+  dim3 grd((unsigned)g.ntiles, (unsigned)g.ntr);
+  k_spread<R><<<grd, SPREAD_THREADS, spread_smem_bytes(sizeof(R) == 8), s>>>(recs, starts, g,
+                                                                             strength, grid);
+  return cudaGetLastError();
+}
+
+template <typename R, int NT>
+static cudaError_t bin_dispatch_smem(const int4 *rows, int nrows, const void *G, const BinGeom &b,
+                                     const R *i1, const R *i2, const R *i3, const double *amp,
+                                     const double *xc, double *acc, double *gnum, int nsm,
+                                     cudaStream_t s) {
+  using C = typename Cplx<R>::T;
+  const size_t hist = (size_t)b.nquant * b.nq * sizeof(double);
+  const int blocks = nsm * 4;
+  if (hist <= 160 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(k_bin<R, NT, true>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hist);
+    if (e != cudaSuccess) return e;
+    k_bin<R, NT, true><<<blocks, 256, hist, s>>>(rows, nrows, (const C *)G, b, i1, i2, i3, amp,
+                                                 xc, acc, gnum);
+  } else {
+    k_bin<R, NT, false><<<blocks, 256, 0, s>>>(rows, nrows, (const C *)G, b, i1, i2, i3, amp, xc,
+                                               acc, gnum);
+  }
+  return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_bin(const int4 *rows, int nrows, const void *G, const BinGeom &b,
+                       const R *inv1, const R *inv2, const R *inv3, const double *amp,
+                       const double *xcoef, double *acc, double *gnum, int nsm, cudaStream_t s) {
+  switch (b.ntr) {
+    case 1: return bin_dispatch_smem<R, 1>(rows, nrows, G, b, inv1, inv2, inv3, amp, xcoef, acc, gnum, nsm, s);
+    case 2: return bin_dispatch_smem<R, 2>(rows, nrows, G, b, inv1, inv2, inv3, amp, xcoef, acc, gnum, nsm, s);
+    case 3: return bin_dispatch_smem<R, 3>(rows, nrows, G, b, inv1, inv2, inv3, amp, xcoef, acc, gnum, nsm, s);
+    case 4: return bin_dispatch_smem<R, 4>(rows, nrows, G, b, inv1, inv2, inv3, amp, xcoef, acc, gnum, nsm, s);
+    default:
+      if (b.ntr > MAX_FAST_T) return cudaErrorInvalidValue;
+      return bin_dispatch_smem<R, 0>(rows, nrows, G, b, inv1, inv2, inv3, amp, xcoef, acc, gnum, nsm, s);
+  }
+}
+
+cudaError_t launch_norms(const int4 *rows, int nrows, const BinGeom &b, const double *amp,
+                         const double *xcoef, const double *counts_t, double *den, double *cnt,
+                         int nsm, cudaStream_t s) {
+  const size_t sh = 2 * (size_t)b.nq * sizeof(double);
+  cudaError_t e = cudaFuncSetAttribute(k_norms, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)sh);
+  if (e != cudaSuccess) return e;
+  k_norms<<<nsm * 4, 256, sh, s>>>(rows, nrows, b, amp, xcoef, counts_t, den, cnt);
+  return cudaGetLastError();
+}
+
+template cudaError_t launch_prep<float>(const double *, const uint8_t *, const FrameGeom &, int *,
+                                        uint32_t *, uint32_t *, cudaStream_t);
+template cudaError_t launch_prep<double>(const double *, const uint8_t *, const FrameGeom &, int *,
+                                         uint32_t *, uint32_t *, cudaStream_t);
+template cudaError_t launch_scatter<float>(const double *, const uint8_t *, const FrameGeom &,
+                                           const uint32_t *, const uint32_t *, const int *,
+                                           PointRec<float> *, cudaStream_t);
+template cudaError_t launch_scatter<double>(const double *, const uint8_t *, const FrameGeom &,
+                                            const uint32_t *, const uint32_t *, const int *,
+                                            PointRec<double> *, cudaStream_t);
+template cudaError_t launch_spread<float>(const PointRec<float> *, const int *, const FrameGeom &,
+                                          const float *, float *, cudaStream_t);
+template cudaError_t launch_spread<double>(const PointRec<double> *, const int *,
+                                           const FrameGeom &, const double *, double *,
+                                           cudaStream_t);
+template cudaError_t launch_bin<float>(const int4 *, int, const void *, const BinGeom &,
+                                       const float *, const float *, const float *,
+                                       const double *, const double *, double *, double *, int,
+                                       cudaStream_t);
+template cudaError_t launch_bin<double>(const int4 *, int, const void *, const BinGeom &,
+                                        const double *, const double *, const double *,
+                                        const double *, const double *, double *, double *, int,
+                                        cudaStream_t);
+
+}  // namespace sqn
