@@ -34,6 +34,8 @@ METRIC = "S(q) frames/s at N=1M (FP32 spread/FFT + FP64 accumulation, partials)"
 UNIT = "frames/s"
 N_ATOMS = 1_000_000
 BOX = 220.0
+# --scale s shrinks the box by s at fixed density (profiling runs only)
+SCALE = 1.0
 FRACTIONS = (0.5, 0.3, 0.2)
 B_NEUTRON = (4.149, 5.803, 9.45)
 QMAX, NQ, EPS = 6.0, 500, 1e-6
@@ -223,8 +225,10 @@ def run_ours(args, rank, world, local_rank):
     types, frames = make_frames(K + W, SEED + 7919 * rank)
     prec = _lib.PREC_SINGLE if args.precision == "single" else _lib.PREC_DOUBLE
     eps = EPS
-    stream = torch.cuda.current_stream()
-    # The plans run on torch's current stream, so torch CUDA events bracket them.
+    # A dedicated (non-default) stream: the plans run on it, so torch CUDA
+    # events recorded on it bracket exactly the library's work.
+    stream = torch.cuda.Stream(device=local_rank)
+    torch.cuda.set_stream(stream)
     mk = lambda timing: _lib.Plan(np.eye(3).reshape(9) * BOX, np.zeros(3), types,  # noqa: E731
                                   weight=_lib.WEIGHT_NEUTRON, amp_const=np.array(B_NEUTRON),
                                   qmin=0.0, qmax=QMAX, nq=NQ, norm=_lib.NORM_MEAN,
@@ -373,7 +377,13 @@ def main():
     ap.add_argument("--precision", default="single", choices=["single", "double"])
     ap.add_argument("--upsampfac", type=float, default=0.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--scale", type=float, default=1.0,
+                    help="shrink the box by this factor at fixed density (profiling only)")
     args = ap.parse_args()
+    if args.scale != 1.0:
+        global N_ATOMS, BOX
+        BOX = BOX * args.scale
+        N_ATOMS = int(round(N_ATOMS * args.scale ** 3))
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

@@ -405,10 +405,7 @@ int setup_plan(sqn_plan *p, const sqn_plan_desc *d) {
     g.nf[i] = (int)p->nf[i];
     g.tile[i] = (int)std::min<int64_t>(tmax[i], p->nf[i]);
     g.ntile[i] = (int)((p->nf[i] + g.tile[i] - 1) / g.tile[i]);
-    const int need = (w - 1 + g.tile[i] - 1) / g.tile[i] + 1 + (p->nf[i] % g.tile[i] ? 1 : 0);
-    g.nbk[i] = std::min(g.ntile[i], need);
   }
-  if (g.nbk[0] * g.nbk[1] * g.nbk[2] > MAX_NB) return SQN_ERR_NOT_SUPPORTED;
   std::memcpy(g.inv, p->inv, sizeof(g.inv));
   std::memcpy(g.origin, p->origin, sizeof(g.origin));
   g.w = w;

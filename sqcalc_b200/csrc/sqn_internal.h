@@ -17,7 +17,8 @@ constexpr int SPREAD_THREADS = TILE_X * TILE_Y;  // 256
 constexpr int ROW = TILE_X + TILE_Y + TILE_Z;    // kernel row entries per staged point
 constexpr int CHUNK = SPREAD_THREADS;            // candidate points per pass
 constexpr int MAX_W = 16;
-constexpr int MAX_NB = 27;                       // neighbour bins of a tile (3 per dim at most)
+constexpr int MAX_BINS_DIM = 4;                  // bins per dim a tile may need (w <= 16)
+constexpr int MAX_NB = 64;                       // neighbour bins of a tile
 constexpr int MAX_FAST_T = 8;                    // species held in registers by the bin kernel
 
 // Point record written by the bin sort and read by the spread kernel.
@@ -43,7 +44,6 @@ struct FrameGeom {
   int nf[3];          // fine grid
   int tile[3];        // tile extent per dim
   int ntile[3];       // tiles per dim
-  int nbk[3];         // bins per dim a tile reads (its own and the ones before it)
   int w;              // ES kernel width
   double beta;        // ES shape
   int ntr;            // fine grids per frame

@@ -179,6 +179,8 @@ __global__ void __launch_bounds__(SPREAD_THREADS)
   __shared__ int s_bpref[MAX_NB + 1];
   __shared__ int s_borg[MAX_NB][3];
   __shared__ int s_wcount[SPREAD_THREADS / 32];
+  __shared__ int s_bl[3][MAX_BINS_DIM];
+  __shared__ int s_nbl[3];
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int tile = blockIdx.x, tr = blockIdx.y;
@@ -189,15 +191,35 @@ __global__ void __launch_bounds__(SPREAD_THREADS)
   const int tx = min(g.tile[0], g.nf[0] - X0);
   const int ty = min(g.tile[1], g.nf[1] - Y0);
   const int tz = min(g.tile[2], g.nf[2] - Z0);
-  const int nb = g.nbk[0] * g.nbk[1] * g.nbk[2];
 
+  // Bins whose points can reach this tile, per dimension: a support starting
+  // at cell c covers c .. c+w-1, so the start cells that matter are
+  // X0-(w-1) .. X0+t-1, taken cyclically.
+  if (tid < 3) {
+    const int d = tid;
+    const int T = g.tile[d], nt = g.ntile[d], n = g.nf[d];
+    const int t = d == 0 ? t0 : (d == 1 ? t1 : t2);
+    const int Xd = t * T, td = min(T, n - Xd);
+    int cnt = 0;
+    if (g.w - 1 + td >= n) {
+      for (int b = 0; b < nt && cnt < MAX_BINS_DIM; ++b) s_bl[d][cnt++] = b;
+    } else {
+      const int ws = Xd - (g.w - 1);
+      if (ws >= 0) {
+        for (int b = ws / T; b <= t && cnt < MAX_BINS_DIM; ++b) s_bl[d][cnt++] = b;
+      } else {
+        for (int b = (n + ws) / T; b < nt && cnt < MAX_BINS_DIM; ++b) s_bl[d][cnt++] = b;
+        for (int b = 0; b <= t && cnt < MAX_BINS_DIM; ++b) s_bl[d][cnt++] = b;
+      }
+    }
+    s_nbl[d] = cnt;
+  }
+  __syncthreads();
+  const int nb0 = s_nbl[0], nb1 = s_nbl[1];
+  const int nb = nb0 * nb1 * s_nbl[2];
   if (tid < nb) {
-    const int kx = tid % g.nbk[0], ky = (tid / g.nbk[0]) % g.nbk[1],
-              kz = tid / (g.nbk[0] * g.nbk[1]);
-    int bx = t0 - kx, by = t1 - ky, bz = t2 - kz;
-    if (bx < 0) bx += g.ntile[0];
-    if (by < 0) by += g.ntile[1];
-    if (bz < 0) bz += g.ntile[2];
+    const int bx = s_bl[0][tid % nb0], by = s_bl[1][(tid / nb0) % nb1],
+              bz = s_bl[2][tid / (nb0 * nb1)];
     const int key = tr * g.ntiles + (bz * g.ntile[1] + by) * g.ntile[0] + bx;
     const int st = starts[key];
     s_bstart[tid] = st;
