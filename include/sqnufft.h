@@ -51,7 +51,8 @@ enum {
   SQN_ERR_TYPE_ID = 45,             /* a type id outside 1..ntypes */
   SQN_ERR_CUFFT = 46,               /* cuFFT plan or execution failure */
   SQN_ERR_TIMEOUT = 47,             /* a bounded device wait gave up */
-  SQN_ERR_NOT_SUPPORTED = 48
+  SQN_ERR_NOT_SUPPORTED = 48,
+  SQN_ERR_SCRATCH_LIMIT = 49        /* request does not fit the fixed no-alloc scratch */
 };
 
 enum { SQN_WEIGHT_UNIT = 0, SQN_WEIGHT_NEUTRON = 1, SQN_WEIGHT_XRAY = 2 };
@@ -174,6 +175,35 @@ int sqn_stage_times(sqn_plan *plan, double *out, int32_t n);
 
 /* Number of this library's own kernel launches so far (cuFFT's not counted). */
 int64_t sqn_launch_count(const sqn_plan *plan);
+
+/* Size of the fixed device scratch array of sqn_spread_frame_noalloc (per GPU). */
+#define SQN_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
+
+/* Wrap, bin-sort and spread one frame onto caller-provided fine grids WITHOUT
+ * allocating any device memory.  No counterpart in the reference: it is for
+ * callers that cannot call cudaMalloc -- a host framework that owns all device
+ * memory through its own pool, a caller in the middle of recording a CUDA graph
+ * (allocation is illegal during a global-mode stream capture), a service that
+ * must not grow its footprint per request.
+ *   pos       [natoms][3] FP64 Cartesian positions, device memory
+ *   species   [natoms] grid index of each atom (0..ntr-1), host memory
+ *   strength  [ntr] FP32 strength of the atoms of each grid, host memory
+ *   cell, origin, nf[3], kernel_width, beta: as sqn_plan_info reports them
+ *   grid      [ntr][nf3][nf2][nf1] FP32 output, device memory, x fastest;
+ *             every cell is written (no zeroing needed)
+ *   stream    cudaStream_t or NULL
+ * Its scratch (bin counts and starts, per-atom keys, sorted point records)
+ * lives in one file-scope device array of SQN_NOALLOC_SCRATCH_BYTES that every
+ * GPU loading the library holds until exit; requests that do not fit return
+ * SQN_ERR_SCRATCH_LIMIT.  The first call on a device resolves the array's
+ * address with that device current; make it before any stream capture.  Calls
+ * share the array (it keeps the last call's contents; counts are cleared each
+ * call), so calls that overlap on the GPU race and must be serialised.
+ * FP32 only; returns once the work is queued on `stream`. */
+int sqn_spread_frame_noalloc(const double *pos, int64_t natoms, const uint8_t *species,
+                             int32_t ntr, const float *strength, const double *cell,
+                             const double *origin, const int64_t *nf, int32_t kernel_width,
+                             double beta, float *grid, void *stream);
 
 /* Release the plan and its device memory.  Replaces cufinufft_destroy plus the
  * cudaFree calls of gpu_finalize (src/sqc_gpu.f90:365-404). */

@@ -28,8 +28,10 @@ EXPORTS = (
     "sqn_abi_version", "sqn_error_string", "sqn_default_desc", "sqn_plan_create",
     "sqn_plan_info_get", "sqn_accumulate_frames", "sqn_sync", "sqn_get_accumulators",
     "sqn_peek_num_async", "sqn_finalize", "sqn_reset", "sqn_stage_times", "sqn_launch_count",
-    "sqn_plan_destroy",
+    "sqn_plan_destroy", "sqn_spread_frame_noalloc",
 )
+ERR_SCRATCH_LIMIT = 49
+NOALLOC_SCRATCH_BYTES = 32 * 1024 * 1024
 
 
 class SqnDesc(ctypes.Structure):
@@ -114,6 +116,8 @@ def load():
     L.sqn_launch_count.argtypes = [vp]
     L.sqn_launch_count.restype = i64
     L.sqn_plan_destroy.argtypes = [vp]
+    L.sqn_spread_frame_noalloc.argtypes = [vp, i64, vp, ctypes.c_int32, vp, vp, vp, vp,
+                                           ctypes.c_int32, ctypes.c_double, vp, vp]
     if L.sqn_abi_version() != ABI_VERSION:
         raise ImportError("libsqnufft.so ABI %d, binding expects %d"
                           % (L.sqn_abi_version(), ABI_VERSION))
