@@ -89,6 +89,67 @@ double es_beta(int w, double sigma) {
   return bw * w;
 }
 
+// Relative cost of one cell of a 3D real-to-complex FFT of size n on B200:
+// measured cuFFT throughput is ~6 ps per cell for powers of two >= 256 and
+// ~9-13 ps for other 2,3,5-smooth sizes.
+double fft_cell_cost(int64_t n) {
+  const bool pow2 = (n & (n - 1)) == 0;
+  return (pow2 && n >= 256) ? 0.65 : 1.0;
+}
+
+// Fine grid and ES width.  With sigma given, nf = next235even(max(sigma m, 2w))
+// per dimension (the reference's rule, external/finufft/src/cuda/common.cu:166-177).
+// Otherwise each dimension takes the cheapest FFT size n >= 1.2 m whose
+// upsampling n/m reaches eps with a width <= wcap; the width is then the one the
+// smallest upsampling needs.  Returns false when eps needs a width above MAX_W.
+bool choose_fine_grid(const int *modes, double eps, double sigma_req, int w_req, int wcap,
+                      int64_t *nf, int *w_out, double *sigma_out) {
+  bool ok = true;
+  if (sigma_req > 0.0) {
+    int w = w_req > 0 ? w_req : es_width(eps, sigma_req);
+    if (w > MAX_W) {
+      w = MAX_W;
+      ok = false;
+    }
+    for (int i = 0; i < 3; ++i)
+      nf[i] = next235even(std::max<int64_t>((int64_t)std::ceil(sigma_req * modes[i]), 2 * w));
+    *w_out = w;
+    *sigma_out = sigma_req;
+    return ok;
+  }
+  double smin = 1e30;
+  for (int i = 0; i < 3; ++i) {
+    const int m = modes[i];
+    int64_t best = 0;
+    double best_cost = 1e300;
+    int64_t n = next235even((int64_t)std::ceil(1.2 * m));
+    for (int k = 0; k < 64 && n <= (int64_t)std::ceil(2.5 * m) + 64; ++k) {
+      const double s = (double)n / m;
+      const int w = std::max(w_req > 0 ? w_req : es_width(eps, s), 2);
+      if (w <= wcap && n >= 2 * w) {
+        const double cost = (double)n * fft_cell_cost(n);
+        if (cost < best_cost) {
+          best_cost = cost;
+          best = n;
+        }
+      }
+      n = next235even(n + 2);
+    }
+    if (best == 0) best = next235even(std::max<int64_t>(2 * m, 2 * MAX_W));
+    nf[i] = best;
+    smin = std::min(smin, (double)best / m);
+  }
+  int w = w_req > 0 ? w_req : es_width(eps, smin);
+  if (w > MAX_W) {
+    w = MAX_W;
+    ok = false;
+  }
+  for (int i = 0; i < 3; ++i) nf[i] = std::max<int64_t>(nf[i], next235even(2 * w));
+  *w_out = w;
+  *sigma_out = smin;
+  return ok;
+}
+
 double es_phi_host(double t, int w, double beta) {
   const double z = 2.0 * t / w;
   const double zz = z * z;
@@ -377,26 +438,17 @@ int setup_plan(sqn_plan *p, const sqn_plan_desc *d) {
     warn = SQN_WARN_EPS_TOO_SMALL;
   }
   p->eps_used = eps;
-  double sigma = d->upsampfac;
-  if (sigma == 0.0) {
-    // Low upsampling keeps the fine grid (and so the FFT, the dominant HBM
-    // traffic) 4x smaller than sigma = 2 whenever a width <= 16 reaches eps.
-    sigma = es_width(eps, 1.25) <= MAX_W ? 1.25 : 2.0;
-  }
-  if (sigma <= 1.0) return SQN_ERR_UPSAMPFAC_TOO_SMALL;
-  int w = d->kernel_width > 0 ? d->kernel_width : es_width(eps, sigma);
-  if (w > MAX_W) {
+  if (d->upsampfac != 0.0 && d->upsampfac <= 1.0) return SQN_ERR_UPSAMPFAC_TOO_SMALL;
+  int w = 0;
+  double sigma = 0.0;
+  if (!choose_fine_grid(p->modes, eps, d->upsampfac, d->kernel_width, p->fp64 ? MAX_W : 12,
+                        p->nf, &w, &sigma)) {
     w = MAX_W;
     warn = SQN_WARN_EPS_TOO_SMALL;
   }
   p->w = w;
   p->sigma = sigma;
   p->beta = es_beta(w, sigma);
-  for (int i = 0; i < 3; ++i) {
-    int64_t n = (int64_t)std::ceil(sigma * p->modes[i]);
-    n = std::max<int64_t>(n, 2 * w);
-    p->nf[i] = next235even(n);
-  }
 
   // --- tiles ---------------------------------------------------------------
   FrameGeom &g = p->fg;
@@ -415,14 +467,18 @@ int setup_plan(sqn_plan *p, const sqn_plan_desc *d) {
   g.pitch = p->nf[0];
   g.vol_real = p->nf[0] * p->nf[1] * p->nf[2];
   g.natoms = d->natoms;
+  g.rec_stride = rec_stride(w, p->fp64);
   if ((int64_t)g.ntiles * p->ntr >= INT32_MAX) return SQN_ERR_NOT_SUPPORTED;
-  p->nkeys = g.ntiles * p->ntr;
+  p->nkeys = g.ntiles;  // one bin per tile; records carry their species
 
   BinGeom &b = p->bg;
   std::memcpy(b.recip, p->recip, sizeof(b.recip));
   b.qmin = d->qmin;
   b.qmax = d->qmax;
   b.dq = (d->qmax - d->qmin) / (double)d->nq;
+  b.qminf = (float)d->qmin;
+  b.qmaxf = (float)d->qmax;
+  b.invdqf = (float)(1.0 / b.dq);
   b.nq = d->nq;
   for (int i = 0; i < 3; ++i) {
     b.hm[i] = p->hm[i];
@@ -453,7 +509,7 @@ int setup_plan(sqn_plan *p, const sqn_plan_desc *d) {
   if ((st = dalloc(p, &p->d_starts, (size_t)p->nkeys + 1))) return st;
   {
     char *v;
-    if ((st = dalloc(p, &v, (size_t)N * (p->fp64 ? sizeof(PointRec<double>) : sizeof(PointRec<float>)))))
+    if ((st = dalloc(p, &v, (size_t)N * g.rec_stride * rsz)))
       return st;
     p->d_recs = v;
     if ((st = dalloc(p, &v, (size_t)p->ntr * g.vol_real * rsz))) return st;
@@ -594,11 +650,11 @@ template <typename R> int run_frame(sqn_plan *p, const double *dpos, int slot) {
   if (e == cudaSuccess) e = launch_scan(p->d_counts, p->d_starts, p->nkeys, s);
   if (e == cudaSuccess)
     e = launch_scatter<R>(dpos, p->d_species, g, p->d_key, p->d_slot, p->d_starts,
-                          (PointRec<R> *)p->d_recs, s);
+                          (R *)p->d_recs, s);
   if (e != cudaSuccess) return SQN_ERR_CUDA;
   if (slot >= 0) cudaEventRecord(p->ev_free[slot], s);
   if (p->timing) cudaEventRecord(ev[1], s);
-  e = launch_spread<R>((const PointRec<R> *)p->d_recs, p->d_starts, g, (const R *)p->d_strength,
+  e = launch_spread<R>((const R *)p->d_recs, p->d_starts, g, (const R *)p->d_strength,
                        (R *)p->d_grid, s);
   if (e != cudaSuccess) return SQN_ERR_CUDA;
   if (p->timing) cudaEventRecord(ev[2], s);

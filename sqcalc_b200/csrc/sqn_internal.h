@@ -1,5 +1,5 @@
-// Internal types shared by the host side (sqn_api.cu) and the kernels
-// (sqn_kernels.cu) of libsqnufft.so.
+// Internal types shared by the host side (sqn_api.cu, sqn_noalloc.cu) and the
+// kernels (sqn_kernels.cu) of libsqnufft.so.
 #pragma once
 
 #include <cstdint>
@@ -7,35 +7,35 @@
 
 namespace sqn {
 
-// Spread tile in fine-grid cells: 32 x-cells (one per lane, so every row store
-// is a 128-byte coalesced write), 8 y-rows (one per warp), 8 z-cells held in
-// registers by each thread.
+// Spread tile in fine-grid cells (x fastest).  A CTA of 16 warps owns one
+// 32 x 16 x 8 tile; warp k owns the 8 x 4 (x, y) patch ((k % 4) * 8, (k / 4) * 4)
+// of it and each lane keeps the 8 z-cells of its (x, y) column in registers.
 constexpr int TILE_X = 32;
-constexpr int TILE_Y = 8;
+constexpr int TILE_Y = 16;
 constexpr int TILE_Z = 8;
-constexpr int SPREAD_THREADS = TILE_X * TILE_Y;  // 256
-constexpr int ROW = TILE_X + TILE_Y + TILE_Z;    // kernel row entries per staged point
-constexpr int CHUNK = SPREAD_THREADS;            // candidate points per pass
+constexpr int PATCH_X = 8;
+constexpr int PATCH_Y = 4;
+constexpr int SPREAD_WARPS = (TILE_X / PATCH_X) * (TILE_Y / PATCH_Y);  // 16
+constexpr int SPREAD_THREADS = 32 * SPREAD_WARPS;                       // 512
+constexpr int ROW = TILE_X + TILE_Y + TILE_Z;  // shifted kernel-row entries per staged point
+constexpr int CHUNK = 256;                     // candidate points staged per pass
 constexpr int MAX_W = 16;
-constexpr int MAX_BINS_DIM = 4;                  // bins per dim a tile may need (w <= 16)
-constexpr int MAX_NB = 64;                       // neighbour bins of a tile
-constexpr int MAX_FAST_T = 8;                    // species held in registers by the bin kernel
+constexpr int MAX_BINS_DIM = 4;                // bins per dim a tile may need (w <= 16)
+constexpr int MAX_NB = 64;                     // neighbour bins of a tile
+constexpr int MAX_FAST_T = 8;                  // species held in registers
 
-// Point record written by the bin sort and read by the spread kernel.
-// packed: bits 0-7 / 8-15 / 16-23 start cell of the kernel support relative to
-// the origin of the home tile in x / y / z; bits 24-31 species index.
-// f[d]: (X_d - ix0_d) - (w/2 - 1/2) in (-1/2, 1/2], X_d the fine-grid coordinate
-// and ix0_d = ceil(X_d - w/2) the first cell of the support.
-template <typename R> struct alignas(16) PointRec;
-template <> struct alignas(16) PointRec<float> {
-  float f[3];
-  uint32_t packed;
-};
-template <> struct alignas(16) PointRec<double> {
-  double f[3];
-  uint32_t packed;
-  uint32_t pad;
-};
+// Point records written by the bin sort and read by the spread kernel: one
+// record of rec_stride R-sized slots per atom, 16-byte aligned:
+//   slot 0            packed word: bits 0-7 / 8-15 / 16-23 first support cell
+//                     relative to the home tile origin in x / y / z, bits 24-31
+//                     species index (stored in the slot's low 32 bits)
+//   slots 1 .. 3w     ES kernel values phi(k - (X_d - ix0_d)), k = 0..w-1, for
+//                     x, then y, then z
+inline int rec_stride(int w, bool fp64) {
+  const int n = 3 * w + 1;
+  const int q = fp64 ? 2 : 4;
+  return (n + q - 1) / q * q;
+}
 
 // Geometry and kernel parameters, passed by value to the per-frame kernels.
 struct FrameGeom {
@@ -48,6 +48,7 @@ struct FrameGeom {
   double beta;        // ES shape
   int ntr;            // fine grids per frame
   int ntiles;         // ntile[0]*ntile[1]*ntile[2]
+  int rec_stride;     // R-sized slots per point record
   int64_t pitch;      // real row pitch of the spread grid (elements)
   int64_t vol_real;   // real elements per fine grid
   int64_t natoms;
@@ -57,6 +58,7 @@ struct FrameGeom {
 struct BinGeom {
   double recip[9];    // b_j = recip[3*j + r]
   double qmin, qmax, dq;
+  float qminf, qmaxf, invdqf;  // FP32 copies for the fast shell estimate
   int nq;
   int hm[3];          // (modes - 1) / 2
   int nf[3];
@@ -80,9 +82,9 @@ cudaError_t launch_scan(int *counts, int *starts, int n, cudaStream_t s);
 template <typename R>
 cudaError_t launch_scatter(const double *pos, const uint8_t *species, const FrameGeom &g,
                            const uint32_t *key, const uint32_t *slot, const int *starts,
-                           PointRec<R> *recs, cudaStream_t s);
+                           R *recs, cudaStream_t s);
 template <typename R>
-cudaError_t launch_spread(const PointRec<R> *recs, const int *starts, const FrameGeom &g,
+cudaError_t launch_spread(const R *recs, const int *starts, const FrameGeom &g,
                           const R *strength, R *grid, cudaStream_t s);
 template <typename R>
 cudaError_t launch_bin(const int4 *rows, int nrows, const void *G, const BinGeom &b,

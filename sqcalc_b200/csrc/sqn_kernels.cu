@@ -73,8 +73,8 @@ __device__ __forceinline__ uint32_t home_key(const AtomCell &c, int sp, const Fr
   l0 = c.ix0[0] - t0 * g.tile[0];
   l1 = c.ix0[1] - t1 * g.tile[1];
   l2 = c.ix0[2] - t2 * g.tile[2];
-  const int tr = g.ntr > 1 ? sp : 0;
-  return (uint32_t)tr * (uint32_t)g.ntiles + (uint32_t)((t2 * g.ntile[1] + t1) * g.ntile[0] + t0);
+  (void)sp;  // one bin per tile holds the points of every transform
+  return (uint32_t)((t2 * g.ntile[1] + t1) * g.ntile[0] + t0);
 }
 
 __global__ void k_prep(const double *__restrict__ pos, const uint8_t *__restrict__ species,
@@ -129,28 +129,6 @@ __global__ void __launch_bounds__(1024) k_scan(int *__restrict__ counts, int *__
   if (tid == 1023) starts[n] = run;
 }
 
-template <typename R>
-__global__ void k_scatter(const double *__restrict__ pos, const uint8_t *__restrict__ species,
-                          FrameGeom g, const uint32_t *__restrict__ key,
-                          const uint32_t *__restrict__ slot, const int *__restrict__ starts,
-                          PointRec<R> *__restrict__ recs) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < g.natoms;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    AtomCell c;
-    atom_cell(pos, i, g, c);
-    const int sp = species[i];
-    int l0, l1, l2;
-    (void)home_key(c, sp, g, l0, l1, l2);
-    PointRec<R> r;
-    r.f[0] = (R)c.off[0];
-    r.f[1] = (R)c.off[1];
-    r.f[2] = (R)c.off[2];
-    r.packed = (uint32_t)l0 | ((uint32_t)l1 << 8) | ((uint32_t)l2 << 16) | ((uint32_t)sp << 24);
-    if constexpr (sizeof(R) == 8) r.pad = 0;
-    recs[(int64_t)starts[key[i]] + slot[i]] = r;
-  }
-}
-
 // ---------------------------------------------------------------------------
 // ES kernel: phi(t) = exp(beta (sqrt(1 - (2t/w)^2) - 1)) on |t| < w/2, else 0
 // (external/finufft/include/cufinufft/spreadinterp.h:84-98).
@@ -164,26 +142,72 @@ __device__ __forceinline__ double es_phi(double t, double c2, double beta) {
   return z2 < 1.0 ? exp(beta * (sqrt(1.0 - z2) - 1.0)) : 0.0;
 }
 
-// ---------------------------------------------------------------------------
-// Gather spreading, one CTA per (tile, transform).
-// ---------------------------------------------------------------------------
 template <typename R>
-__global__ void __launch_bounds__(SPREAD_THREADS)
-    k_spread(const PointRec<R> *__restrict__ recs, const int *__restrict__ starts, FrameGeom g,
+__global__ void k_scatter(const double *__restrict__ pos, const uint8_t *__restrict__ species,
+                          FrameGeom g, const uint32_t *__restrict__ key,
+                          const uint32_t *__restrict__ slot, const int *__restrict__ starts,
+                          R *__restrict__ recs) {
+  const R halfw = R(0.5) * (R)g.w - R(0.5);
+  const R c2 = R(4) / ((R)g.w * (R)g.w);
+  const R beta = (R)g.beta;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < g.natoms;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    AtomCell c;
+    atom_cell(pos, i, g, c);
+    const int sp = species[i];
+    int l0, l1, l2;
+    (void)home_key(c, sp, g, l0, l1, l2);
+    R *r = recs + ((int64_t)starts[key[i]] + slot[i]) * g.rec_stride;
+    const uint32_t packed =
+        (uint32_t)l0 | ((uint32_t)l1 << 8) | ((uint32_t)l2 << 16) | ((uint32_t)sp << 24);
+    if constexpr (sizeof(R) == 4)
+      r[0] = __uint_as_float(packed);
+    else
+      r[0] = __longlong_as_double((long long)packed);
+    // The separable kernel values of the w support cells along each axis,
+    // evaluated once per atom (the spread reuses them for every tile).
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const R off = (R)c.off[d];
+      for (int k = 0; k < g.w; ++k) r[1 + d * g.w + k] = es_phi(((R)k - halfw) - off, c2, beta);
+    }
+  }
+}
+
+template <typename R> __device__ __forceinline__ uint32_t rec_packed(const R *r);
+template <> __device__ __forceinline__ uint32_t rec_packed<float>(const float *r) {
+  return __float_as_uint(r[0]);
+}
+template <> __device__ __forceinline__ uint32_t rec_packed<double>(const double *r) {
+  return (uint32_t)__double_as_longlong(r[0]);
+}
+
+// ---------------------------------------------------------------------------
+// Gather spreading, one CTA per 32 x 16 x 8 tile for all transforms.
+// NT > 0: exactly NT transforms; NT == 0: any ntr <= MAX_FAST_T.
+// ---------------------------------------------------------------------------
+template <typename R, int NT>
+__global__ void __launch_bounds__(SPREAD_THREADS, (sizeof(R) == 4 || NT == 1) ? 2 : 1)
+    k_spread(const R *__restrict__ recs, const int *__restrict__ starts, FrameGeom g,
              const R *__restrict__ strength, R *__restrict__ grid) {
+  constexpr int TM = NT > 0 ? NT : MAX_FAST_T;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R *s_rows = reinterpret_cast<R *>(smem_raw);                      // [CHUNK][ROW]
   int4 *s_meta = reinterpret_cast<int4 *>(s_rows + CHUNK * ROW);    // [CHUNK] rx, ry, rz, sp
-  R *s_off = reinterpret_cast<R *>(s_meta + CHUNK);                 // [CHUNK][3]
+  int *s_rec = reinterpret_cast<int *>(s_meta + CHUNK);             // [CHUNK] record index
+  unsigned *s_mask = reinterpret_cast<unsigned *>(s_rec + CHUNK);   // [CHUNK] patch masks
   __shared__ int s_bstart[MAX_NB];
   __shared__ int s_bpref[MAX_NB + 1];
   __shared__ int s_borg[MAX_NB][3];
-  __shared__ int s_wcount[SPREAD_THREADS / 32];
+  __shared__ int s_wcount[SPREAD_WARPS];
   __shared__ int s_bl[3][MAX_BINS_DIM];
   __shared__ int s_nbl[3];
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int tile = blockIdx.x, tr = blockIdx.y;
+  const int cx = (warp & 3) * PATCH_X + (lane & 7);   // this lane's x cell in the tile
+  const int cy = (warp >> 2) * PATCH_Y + (lane >> 3);  // and its y cell
+  const int tile = blockIdx.x;
+  const int ntr = NT > 0 ? NT : g.ntr;
   const int t0 = tile % g.ntile[0];
   const int t1 = (tile / g.ntile[0]) % g.ntile[1];
   const int t2 = tile / (g.ntile[0] * g.ntile[1]);
@@ -220,7 +244,7 @@ __global__ void __launch_bounds__(SPREAD_THREADS)
   if (tid < nb) {
     const int bx = s_bl[0][tid % nb0], by = s_bl[1][(tid / nb0) % nb1],
               bz = s_bl[2][tid / (nb0 * nb1)];
-    const int key = tr * g.ntiles + (bz * g.ntile[1] + by) * g.ntile[0] + bx;
+    const int key = (bz * g.ntile[1] + by) * g.ntile[0] + bx;
     const int st = starts[key];
     s_bstart[tid] = st;
     s_bpref[tid + 1] = starts[key + 1] - st;
@@ -236,43 +260,40 @@ __global__ void __launch_bounds__(SPREAD_THREADS)
   __syncthreads();
   const int total = s_bpref[nb];
 
-  R acc[TILE_Z];
+  R acc[TM][TILE_Z];
 #pragma unroll
-  for (int z = 0; z < TILE_Z; ++z) acc[z] = R(0);
-  const R halfw = R(0.5) * (R)g.w - R(0.5);
-  const R c2 = R(4) / ((R)g.w * (R)g.w);
-  const R beta = (R)g.beta;
+  for (int t = 0; t < TM; ++t)
+#pragma unroll
+    for (int z = 0; z < TILE_Z; ++z) acc[t][z] = R(0);
+  const unsigned xbit = 1u << (warp & 3), ybit = 1u << (4 + (warp >> 2));
 
   for (int base = 0; base < total; base += CHUNK) {
+    // Stage the candidates that overlap the tile (compacted, order kept).
     const int i = base + tid;
     bool keep = false;
     int4 meta = make_int4(0, 0, 0, 0);
-    R o0 = 0, o1 = 0, o2 = 0;
-    if (i < total) {
+    int ridx = 0;
+    if (tid < CHUNK && i < total) {
       int b = 0;
       while (i >= s_bpref[b + 1]) ++b;
-      const PointRec<R> rec = recs[s_bstart[b] + (i - s_bpref[b])];
-      const int lx0 = rec.packed & 255, ly0 = (rec.packed >> 8) & 255,
-                lz0 = (rec.packed >> 16) & 255;
-      int rx = s_borg[b][0] + lx0 - X0;
-      int ry = s_borg[b][1] + ly0 - Y0;
-      int rz = s_borg[b][2] + lz0 - Z0;
+      ridx = s_bstart[b] + (i - s_bpref[b]);
+      const uint32_t packed = rec_packed<R>(recs + (int64_t)ridx * g.rec_stride);
+      int rx = s_borg[b][0] + (int)(packed & 255u) - X0;
+      int ry = s_borg[b][1] + (int)((packed >> 8) & 255u) - Y0;
+      int rz = s_borg[b][2] + (int)((packed >> 16) & 255u) - Z0;
       if (rx < 0) rx += g.nf[0];
       if (ry < 0) ry += g.nf[1];
       if (rz < 0) rz += g.nf[2];
       keep = (rx < tx || rx + g.w > g.nf[0]) && (ry < ty || ry + g.w > g.nf[1]) &&
              (rz < tz || rz + g.w > g.nf[2]);
-      meta = make_int4(rx, ry, rz, (int)(rec.packed >> 24));
-      o0 = rec.f[0];
-      o1 = rec.f[1];
-      o2 = rec.f[2];
+      meta = make_int4(rx, ry, rz, (int)(packed >> 24));
     }
     const unsigned bal = __ballot_sync(FULL, keep);
     if (lane == 0) s_wcount[warp] = __popc(bal);
     __syncthreads();
     int wbase = 0, npts = 0;
 #pragma unroll
-    for (int k = 0; k < SPREAD_THREADS / 32; ++k) {
+    for (int k = 0; k < SPREAD_WARPS; ++k) {
       const int cnt = s_wcount[k];
       wbase += k < warp ? cnt : 0;
       npts += cnt;
@@ -280,13 +301,14 @@ __global__ void __launch_bounds__(SPREAD_THREADS)
     if (keep) {
       const int p = wbase + __popc(bal & ((1u << lane) - 1u));
       s_meta[p] = meta;
-      s_off[3 * p + 0] = o0;
-      s_off[3 * p + 1] = o1;
-      s_off[3 * p + 2] = o2;
+      s_rec[p] = ridx;
+      s_mask[p] = 0u;
     }
     __syncthreads();
 
-    // Kernel rows of every staged point, shifted into tile coordinates.
+    // Kernel rows of every staged point shifted into tile coordinates (taken
+    // from the record), the strength folded into the z row, and the mask of
+    // the x / y patches each point reaches.
     for (int e = tid; e < npts * ROW; e += SPREAD_THREADS) {
       const int p = e / ROW, c = e - p * ROW;
       const int4 m = s_meta[p];
@@ -303,34 +325,55 @@ __global__ void __launch_bounds__(SPREAD_THREADS)
         int k = cell - r;
         if (k < 0) k += n;
         if (k < g.w) {
-          const R t = ((R)k - halfw) - s_off[3 * p + d];
-          v = es_phi(t, c2, beta);
+          v = recs[(int64_t)s_rec[p] * g.rec_stride + 1 + d * g.w + k];
           if (d == 2) v *= strength[m.w];
         }
       }
       s_rows[e] = v;
+      if (v != R(0) && d < 2)
+        atomicOr(&s_mask[p], d == 0 ? (1u << (cell >> 3)) : (1u << (4 + (cell >> 2))));
     }
     __syncthreads();
 
-    for (int p = 0; p < npts; ++p) {
-      const R *row = s_rows + p * ROW;
-      const R kyv = row[TILE_X + warp];
-      if (kyv != R(0)) {
-        const R a = row[lane] * kyv;
+    // Each warp walks only the points that reach its patch.
+    for (int pb = 0; pb < npts; pb += 32) {
+      const int p = pb + lane;
+      bool act = false;
+      if (p < npts) {
+        const unsigned m = s_mask[p];
+        act = (m & xbit) && (m & ybit);
+      }
+      unsigned am = __ballot_sync(FULL, act);
+      while (am) {
+        const int q = pb + __ffs(am) - 1;
+        am &= am - 1u;
+        const R *row = s_rows + q * ROW;
+        const R a = row[cx] * row[TILE_X + cy];
+        const int tr = ntr > 1 ? s_meta[q].w : 0;  // the same for the whole warp
 #pragma unroll
-        for (int z = 0; z < TILE_Z; ++z) acc[z] = fma(a, row[TILE_X + TILE_Y + z], acc[z]);
+        for (int t = 0; t < TM; ++t) {
+          if (t == tr) {
+#pragma unroll
+            for (int z = 0; z < TILE_Z; ++z)
+              acc[t][z] = fma(a, row[TILE_X + TILE_Y + z], acc[t][z]);
+          }
+        }
       }
     }
     __syncthreads();
   }
 
-  if (lane < tx && warp < ty) {
-    R *out = grid + (int64_t)tr * g.vol_real +
-             ((int64_t)Z0 * g.nf[1] + (Y0 + warp)) * g.pitch + X0 + lane;
+  if (cx < tx && cy < ty) {
     const int64_t zs = (int64_t)g.nf[1] * g.pitch;
+    R *out = grid + ((int64_t)Z0 * g.nf[1] + (Y0 + cy)) * g.pitch + X0 + cx;
 #pragma unroll
-    for (int z = 0; z < TILE_Z; ++z)
-      if (z < tz) out[z * zs] = acc[z];
+    for (int t = 0; t < TM; ++t) {
+      if (t < ntr) {
+#pragma unroll
+        for (int z = 0; z < TILE_Z; ++z)
+          if (z < tz) out[(int64_t)t * g.vol_real + z * zs] = acc[t][z];
+      }
+    }
   }
 }
 
@@ -354,6 +397,36 @@ __device__ __forceinline__ double qlen_exact(const BinGeom &b, int h1, int h2, i
 __device__ __forceinline__ int shell_of(const BinGeom &b, double ql) {
   int s = (int)__ddiv_rn(__dsub_rn(ql, b.qmin), b.dq);
   return min(max(s, 0), b.nq - 1);
+}
+
+// Kept test and zero-based shell of mode h, identical to the reference's FP64
+// evaluation (:366-399).  A fast estimate (q from the row constant, |q| in
+// FP32) decides whenever |q| is clear of qmin, qmax and every shell edge by a
+// margin well above its error; otherwise the exact FP64 path runs.  ql returns
+// |q| (FP64, for the x-ray form factors).
+__device__ __forceinline__ bool classify_mode(const BinGeom &b, const double *crow, int h1,
+                                              int h2, int h3, int &s, double &ql) {
+  if (h1 == 0 && h2 == 0 && h3 == 0) return false;
+  const double q0 = fma((double)h1, b.recip[0], crow[0]);
+  const double q1 = fma((double)h1, b.recip[1], crow[1]);
+  const double q2 = fma((double)h1, b.recip[2], crow[2]);
+  const double ql2 = fma(q0, q0, fma(q1, q1, q2 * q2));
+  const float qf = sqrtf((float)ql2);
+  const float tol_q = 4e-7f * qf + 1e-30f;
+  const float t = (qf - b.qminf) * b.invdqf;
+  const float tol_t = 4e-7f * (qf * b.invdqf + 1.0f) + 1e-6f;
+  const bool near = fabsf(qf - b.qmaxf) <= tol_q || fabsf(qf - b.qminf) <= tol_q ||
+                    fabsf(t - rintf(t)) <= tol_t;
+  if (b.xray) ql = sqrt(ql2);
+  if (!near) {
+    if (qf > b.qmaxf || qf < b.qminf) return false;
+    s = min(max((int)t, 0), b.nq - 1);
+    return true;
+  }
+  ql = qlen_exact(b, h1, h2, h3);
+  if (ql > b.qmax || ql < b.qmin) return false;
+  s = shell_of(b, ql);
+  return true;
 }
 
 // IT92 form factor f(q) = sum_i a_i exp(-b_i (q/4pi)^2) + c (src/sqc_elements.f90:226-239).
@@ -393,8 +466,8 @@ template <> struct Cplx<double> { using T = double2; };
 // Rows (h2, h3) are dealt to warps; lanes walk h1 >= 0 (32 consecutive complex
 // values per warp and transform, one coalesced read).
 // ---------------------------------------------------------------------------
-template <typename R, int NT, bool SMEM>
-__global__ void __launch_bounds__(256)
+template <typename R, int NT, bool SMEM, bool XR>
+__global__ void __launch_bounds__(256, 2)
     k_bin(const int4 *__restrict__ rows, int nrows, const typename Cplx<R>::T *__restrict__ G,
           BinGeom b, const R *__restrict__ inv1, const R *__restrict__ inv2,
           const R *__restrict__ inv3, const double *__restrict__ amp,
@@ -420,16 +493,21 @@ __global__ void __launch_bounds__(256)
     const R dyz = inv2[abs(h2)] * inv3[abs(h3)];
     const int64_t gbase =
         ((int64_t)(h3 + b.hm[2]) * b.m2 + (int64_t)(h2 + b.hm[1])) * (int64_t)(b.hm[0] + 1);
+    double crow[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+      crow[k] = fma((double)h2, b.recip[3 + k], (double)h3 * b.recip[6 + k]);
     for (int h1b = lo; h1b <= hi; h1b += 32) {
       const int h1 = h1b + lane;
-      bool keep = h1 <= hi;
+      const bool inrow = h1 <= hi;
+      // Issue the loads first: they do not depend on the classification.
+      typename Cplx<R>::T v[TM];
+#pragma unroll
+      for (int t = 0; t < TM; ++t)
+        if (t < ntr && inrow) v[t] = G[(int64_t)t * b.vol_cplx + rowbase + h1];
       double ql = 0.0;
       int s = 0;
-      if (keep) {
-        ql = qlen_exact(b, h1, h2, h3);
-        keep = !(h1 == 0 && h2 == 0 && h3 == 0) && ql >= b.qmin && ql <= b.qmax;
-        s = shell_of(b, ql);
-      }
+      const bool keep = inrow && classify_mode(b, crow, h1, h2, h3, s, ql);
       const unsigned act = __ballot_sync(FULL, keep);
       if (act == 0u) continue;
       double re[TM], im[TM];
@@ -445,10 +523,9 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
         for (int t = 0; t < TM; ++t) {
           if (t < ntr) {
-            const typename Cplx<R>::T v = G[(int64_t)t * b.vol_cplx + rowbase + h1];
-            re[t] = (double)(v.x * dec);
-            im[t] = (double)(v.y * dec);
-            const double a = b.xray ? xray_f(xcoef + 9 * t, ql) : amp[t];
+            re[t] = (double)(v[t].x * dec);
+            im[t] = (double)(v[t].y * dec);
+            const double a = XR ? xray_f(xcoef + 9 * t, ql) : amp[t];
             tre += a * re[t];
             tim += a * im[t];
           }
@@ -561,30 +638,68 @@ cudaError_t launch_scan(int *counts, int *starts, int n, cudaStream_t s) {
 template <typename R>
 cudaError_t launch_scatter(const double *pos, const uint8_t *species, const FrameGeom &g,
                            const uint32_t *key, const uint32_t *slot, const int *starts,
-                           PointRec<R> *recs, cudaStream_t s) {
+                           R *recs, cudaStream_t s) {
   k_scatter<R><<<grid_for(g.natoms, 256), 256, 0, s>>>(pos, species, g, key, slot, starts, recs);
   return cudaGetLastError();
 }
 
 size_t spread_smem_bytes(bool fp64) {
   const size_t r = fp64 ? 8 : 4;
-  return (size_t)CHUNK * ROW * r + (size_t)CHUNK * sizeof(int4) + (size_t)CHUNK * 3 * r;
+  return (size_t)CHUNK * ROW * r + (size_t)CHUNK * (sizeof(int4) + 2 * sizeof(int));
+}
+
+template <typename R> static cudaError_t spread_attr(bool fp64) {
+  const int b = (int)spread_smem_bytes(fp64);
+  cudaError_t e = cudaSuccess;
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_spread<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_spread<R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_spread<R, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_spread<R, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_spread<R, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+  return e;
 }
 
 cudaError_t spread_set_attributes() {
-  cudaError_t e = cudaFuncSetAttribute(k_spread<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)spread_smem_bytes(false));
+  cudaError_t e = spread_attr<float>(false);
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_spread<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)spread_smem_bytes(true));
+  return spread_attr<double>(true);
 }
 
 template <typename R>
-cudaError_t launch_spread(const PointRec<R> *recs, const int *starts, const FrameGeom &g,
+cudaError_t launch_spread(const R *recs, const int *starts, const FrameGeom &g,
                           const R *strength, R *grid, cudaStream_t s) {
-  dim3 grd((unsigned)g.ntiles, (unsigned)g.ntr);
-  k_spread<R><<<grd, SPREAD_THREADS, spread_smem_bytes(sizeof(R) == 8), s>>>(recs, starts, g,
-                                                                             strength, grid);
+  const dim3 grd((unsigned)g.ntiles);
+  const size_t sm = spread_smem_bytes(sizeof(R) == 8);
+  switch (g.ntr) {
+    case 1: k_spread<R, 1><<<grd, SPREAD_THREADS, sm, s>>>(recs, starts, g, strength, grid); break;
+    case 2: k_spread<R, 2><<<grd, SPREAD_THREADS, sm, s>>>(recs, starts, g, strength, grid); break;
+    case 3: k_spread<R, 3><<<grd, SPREAD_THREADS, sm, s>>>(recs, starts, g, strength, grid); break;
+    case 4: k_spread<R, 4><<<grd, SPREAD_THREADS, sm, s>>>(recs, starts, g, strength, grid); break;
+    default:
+      if (g.ntr > MAX_FAST_T) return cudaErrorInvalidValue;
+      k_spread<R, 0><<<grd, SPREAD_THREADS, sm, s>>>(recs, starts, g, strength, grid);
+  }
+  return cudaGetLastError();
+}
+
+template <typename R, int NT, bool XR>
+static cudaError_t bin_dispatch_xr(const int4 *rows, int nrows, const void *G, const BinGeom &b,
+                                   const R *i1, const R *i2, const R *i3, const double *amp,
+                                   const double *xc, double *acc, double *gnum, int nsm,
+                                   cudaStream_t s) {
+  using C = typename Cplx<R>::T;
+  const size_t hist = (size_t)b.nquant * b.nq * sizeof(double);
+  const int blocks = nsm * 4;
+  if (hist <= 160 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(k_bin<R, NT, true, XR>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hist);
+    if (e != cudaSuccess) return e;
+    k_bin<R, NT, true, XR><<<blocks, 256, hist, s>>>(rows, nrows, (const C *)G, b, i1, i2, i3,
+                                                     amp, xc, acc, gnum);
+  } else {
+    k_bin<R, NT, false, XR><<<blocks, 256, 0, s>>>(rows, nrows, (const C *)G, b, i1, i2, i3, amp,
+                                                   xc, acc, gnum);
+  }
   return cudaGetLastError();
 }
 
@@ -593,20 +708,8 @@ static cudaError_t bin_dispatch_smem(const int4 *rows, int nrows, const void *G,
                                      const R *i1, const R *i2, const R *i3, const double *amp,
                                      const double *xc, double *acc, double *gnum, int nsm,
                                      cudaStream_t s) {
-  using C = typename Cplx<R>::T;
-  const size_t hist = (size_t)b.nquant * b.nq * sizeof(double);
-  const int blocks = nsm * 4;
-  if (hist <= 160 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(k_bin<R, NT, true>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hist);
-    if (e != cudaSuccess) return e;
-    k_bin<R, NT, true><<<blocks, 256, hist, s>>>(rows, nrows, (const C *)G, b, i1, i2, i3, amp,
-                                                 xc, acc, gnum);
-  } else {
-    k_bin<R, NT, false><<<blocks, 256, 0, s>>>(rows, nrows, (const C *)G, b, i1, i2, i3, amp, xc,
-                                               acc, gnum);
-  }
-  return cudaGetLastError();
+  if (b.xray) return bin_dispatch_xr<R, NT, true>(rows, nrows, G, b, i1, i2, i3, amp, xc, acc, gnum, nsm, s);
+  return bin_dispatch_xr<R, NT, false>(rows, nrows, G, b, i1, i2, i3, amp, xc, acc, gnum, nsm, s);
 }
 
 template <typename R>
@@ -641,15 +744,14 @@ template cudaError_t launch_prep<double>(const double *, const uint8_t *, const 
                                          uint32_t *, uint32_t *, cudaStream_t);
 template cudaError_t launch_scatter<float>(const double *, const uint8_t *, const FrameGeom &,
                                            const uint32_t *, const uint32_t *, const int *,
-                                           PointRec<float> *, cudaStream_t);
+                                           float *, cudaStream_t);
 template cudaError_t launch_scatter<double>(const double *, const uint8_t *, const FrameGeom &,
                                             const uint32_t *, const uint32_t *, const int *,
-                                            PointRec<double> *, cudaStream_t);
-template cudaError_t launch_spread<float>(const PointRec<float> *, const int *, const FrameGeom &,
+                                            double *, cudaStream_t);
+template cudaError_t launch_spread<float>(const float *, const int *, const FrameGeom &,
                                           const float *, float *, cudaStream_t);
-template cudaError_t launch_spread<double>(const PointRec<double> *, const int *,
-                                           const FrameGeom &, const double *, double *,
-                                           cudaStream_t);
+template cudaError_t launch_spread<double>(const double *, const int *, const FrameGeom &,
+                                           const double *, double *, cudaStream_t);
 template cudaError_t launch_bin<float>(const int4 *, int, const void *, const BinGeom &,
                                        const float *, const float *, const float *,
                                        const double *, const double *, double *, double *, int,

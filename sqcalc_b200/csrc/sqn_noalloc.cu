@@ -125,7 +125,8 @@ extern "C" int sqn_spread_frame_noalloc(const double *pos, int64_t natoms,
   g.pitch = nf[0];
   g.vol_real = nf[0] * nf[1] * nf[2];
   g.natoms = natoms;
-  const int64_t nkeys = (int64_t)g.ntiles * ntr;
+  g.rec_stride = rec_stride(w, false);
+  const int64_t nkeys = (int64_t)g.ntiles;  // one bin per tile
   if (nkeys >= INT32_MAX) return SQN_ERR_SCRATCH_LIMIT;
 
   // Scratch layout inside the static array, each section 256-byte aligned.
@@ -134,7 +135,7 @@ extern "C" int sqn_spread_frame_noalloc(const double *pos, int64_t natoms,
   const size_t o_key = o_starts + align256(sizeof(int) * (size_t)(nkeys + 1));
   const size_t o_slot = o_key + align256(sizeof(uint32_t) * (size_t)natoms);
   const size_t o_recs = o_slot + align256(sizeof(uint32_t) * (size_t)natoms);
-  const size_t o_species = o_recs + align256(sizeof(PointRec<float>) * (size_t)natoms);
+  const size_t o_species = o_recs + align256(sizeof(float) * (size_t)g.rec_stride * (size_t)natoms);
   const size_t o_strength = o_species + align256((size_t)natoms);
   const size_t total = o_strength + align256(sizeof(float) * (size_t)ntr);
   if (total > (size_t)SQN_NOALLOC_SCRATCH_BYTES) return SQN_ERR_SCRATCH_LIMIT;
@@ -146,7 +147,7 @@ extern "C" int sqn_spread_frame_noalloc(const double *pos, int64_t natoms,
   int *starts = reinterpret_cast<int *>(base + o_starts);
   uint32_t *key = reinterpret_cast<uint32_t *>(base + o_key);
   uint32_t *slot = reinterpret_cast<uint32_t *>(base + o_slot);
-  PointRec<float> *recs = reinterpret_cast<PointRec<float> *>(base + o_recs);
+  float *recs = reinterpret_cast<float *>(base + o_recs);
   uint8_t *d_species = base + o_species;
   float *d_strength = reinterpret_cast<float *>(base + o_strength);
 
