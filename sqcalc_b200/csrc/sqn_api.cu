@@ -468,6 +468,7 @@ int setup_plan(sqn_plan *p, const sqn_plan_desc *d) {
   g.vol_real = p->nf[0] * p->nf[1] * p->nf[2];
   g.natoms = d->natoms;
   g.rec_stride = rec_stride(w, p->fp64);
+  g.chunk = spread_chunk(g.rec_stride, p->fp64);
   if ((int64_t)g.ntiles * p->ntr >= INT32_MAX) return SQN_ERR_NOT_SUPPORTED;
   p->nkeys = g.ntiles;  // one bin per tile; records carry their species
 

@@ -17,23 +17,22 @@ constexpr int PATCH_X = 8;
 constexpr int PATCH_Y = 4;
 constexpr int SPREAD_WARPS = (TILE_X / PATCH_X) * (TILE_Y / PATCH_Y);  // 16
 constexpr int SPREAD_THREADS = 32 * SPREAD_WARPS;                       // 512
-constexpr int ROW = TILE_X + TILE_Y + TILE_Z;  // shifted kernel-row entries per staged point
-constexpr int CHUNK = 256;                     // candidate points staged per pass
 constexpr int MAX_W = 16;
 constexpr int MAX_BINS_DIM = 4;                // bins per dim a tile may need (w <= 16)
 constexpr int MAX_NB = 64;                     // neighbour bins of a tile
 constexpr int MAX_FAST_T = 8;                  // species held in registers
 
 // Point records written by the bin sort and read by the spread kernel: one
-// record of rec_stride R-sized slots per atom, 16-byte aligned:
+// record of rec_stride R-sized slots per atom:
 //   slot 0            packed word: bits 0-7 / 8-15 / 16-23 first support cell
 //                     relative to the home tile origin in x / y / z, bits 24-31
 //                     species index (stored in the slot's low 32 bits)
 //   slots 1 .. 3w     ES kernel values phi(k - (X_d - ix0_d)), k = 0..w-1, for
 //                     x, then y, then z
+// The stride is a multiple of 32 bytes (one DRAM sector).
 inline int rec_stride(int w, bool fp64) {
   const int n = 3 * w + 1;
-  const int q = fp64 ? 2 : 4;
+  const int q = fp64 ? 4 : 8;
   return (n + q - 1) / q * q;
 }
 
@@ -49,7 +48,8 @@ struct FrameGeom {
   int ntr;            // fine grids per frame
   int ntiles;         // ntile[0]*ntile[1]*ntile[2]
   int rec_stride;     // R-sized slots per point record
-  int64_t pitch;      // real row pitch of the spread grid (elements)
+  int chunk;          // points the spread stages in shared memory per pass
+  int64_t pitch;     // real row pitch of the spread grid (elements)
   int64_t vol_real;   // real elements per fine grid
   int64_t natoms;
 };
@@ -94,7 +94,8 @@ cudaError_t launch_bin(const int4 *rows, int nrows, const void *G, const BinGeom
 cudaError_t launch_norms(const int4 *rows, int nrows, const BinGeom &b, const double *amp,
                          const double *xcoef, const double *counts_t, double *den,
                          double *cnt, int nsm, cudaStream_t s);
-size_t spread_smem_bytes(bool fp64);
+size_t spread_smem_bytes(int chunk, int stride, bool fp64);
+int spread_chunk(int stride, bool fp64);
 cudaError_t spread_set_attributes();
 
 }  // namespace sqn

@@ -2,15 +2,17 @@
 //
 // Per frame:
 //   k_prep     wrap each atom into the cell, find the first cell of its ES
-//              kernel support on the fine grid and its home (tile, transform)
-//              bin; count the bin                               [HBM: positions]
+//              kernel support on the fine grid and its home tile; count the
+//              tile's bin                                        [HBM: positions]
 //   k_scan     exclusive scan of the bin counts (one CTA) and reset the counts
-//   k_scatter  write each atom's 16-byte point record into its bin slot
-//   k_spread   gather spreading: one CTA owns one fine-grid tile of one
-//              transform, stages the points of the bins that can reach it,
-//              evaluates the separable ES kernel rows in shared memory and
-//              accumulates every cell in registers; each cell is written once,
-//              coalesced, so the grid needs no zeroing and no atomics
+//   k_scatter  write each atom's record into its bin slot: packed start cell +
+//              species and the 3w separable kernel values, evaluated once
+//   k_spread   gather spreading: one CTA owns one 32 x 16 x 8 fine-grid tile
+//              for every transform, stages the records of the bins that can
+//              reach it in shared memory, and each warp accumulates its 8 x 4
+//              patch (8 z-cells per lane, per transform) in registers from the
+//              points that reach the patch; every cell is written exactly
+//              once, so the grid needs no zeroing and no atomics
 //                                                              [HBM: grid write]
 //   (cuFFT R2C / D2Z, out of place)
 //   k_bin      deconvolve the half-space modes, form the weighted total and the
@@ -67,25 +69,25 @@ __device__ __forceinline__ void atom_cell(const double *__restrict__ pos, int64_
   }
 }
 
-__device__ __forceinline__ uint32_t home_key(const AtomCell &c, int sp, const FrameGeom &g,
-                                             int &l0, int &l1, int &l2) {
+// Home tile of the support start (one bin per tile holds every transform) and
+// the start cell relative to the tile origin.
+__device__ __forceinline__ uint32_t home_key(const AtomCell &c, const FrameGeom &g, int &l0,
+                                             int &l1, int &l2) {
   const int t0 = c.ix0[0] / g.tile[0], t1 = c.ix0[1] / g.tile[1], t2 = c.ix0[2] / g.tile[2];
   l0 = c.ix0[0] - t0 * g.tile[0];
   l1 = c.ix0[1] - t1 * g.tile[1];
   l2 = c.ix0[2] - t2 * g.tile[2];
-  (void)sp;  // one bin per tile holds the points of every transform
   return (uint32_t)((t2 * g.ntile[1] + t1) * g.ntile[0] + t0);
 }
 
-__global__ void k_prep(const double *__restrict__ pos, const uint8_t *__restrict__ species,
-                       FrameGeom g, int *__restrict__ counts, uint32_t *__restrict__ key,
-                       uint32_t *__restrict__ slot) {
+__global__ void k_prep(const double *__restrict__ pos, FrameGeom g, int *__restrict__ counts,
+                       uint32_t *__restrict__ key, uint32_t *__restrict__ slot) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < g.natoms;
        i += (int64_t)gridDim.x * blockDim.x) {
     AtomCell c;
     atom_cell(pos, i, g, c);
     int l0, l1, l2;
-    const uint32_t k = home_key(c, species[i], g, l0, l1, l2);
+    const uint32_t k = home_key(c, g, l0, l1, l2);
     key[i] = k;
     slot[i] = (uint32_t)atomicAdd(&counts[k], 1);
   }
@@ -142,6 +144,21 @@ __device__ __forceinline__ double es_phi(double t, double c2, double beta) {
   return z2 < 1.0 ? exp(beta * (sqrt(1.0 - z2) - 1.0)) : 0.0;
 }
 
+template <typename R> __device__ __forceinline__ R pack_word(uint32_t w);
+template <> __device__ __forceinline__ float pack_word<float>(uint32_t w) {
+  return __uint_as_float(w);
+}
+template <> __device__ __forceinline__ double pack_word<double>(uint32_t w) {
+  return __longlong_as_double((long long)w);
+}
+template <typename R> __device__ __forceinline__ uint32_t unpack_word(R v);
+template <> __device__ __forceinline__ uint32_t unpack_word<float>(float v) {
+  return __float_as_uint(v);
+}
+template <> __device__ __forceinline__ uint32_t unpack_word<double>(double v) {
+  return (uint32_t)__double_as_longlong(v);
+}
+
 template <typename R>
 __global__ void k_scatter(const double *__restrict__ pos, const uint8_t *__restrict__ species,
                           FrameGeom g, const uint32_t *__restrict__ key,
@@ -156,14 +173,10 @@ __global__ void k_scatter(const double *__restrict__ pos, const uint8_t *__restr
     atom_cell(pos, i, g, c);
     const int sp = species[i];
     int l0, l1, l2;
-    (void)home_key(c, sp, g, l0, l1, l2);
+    (void)home_key(c, g, l0, l1, l2);
     R *r = recs + ((int64_t)starts[key[i]] + slot[i]) * g.rec_stride;
-    const uint32_t packed =
-        (uint32_t)l0 | ((uint32_t)l1 << 8) | ((uint32_t)l2 << 16) | ((uint32_t)sp << 24);
-    if constexpr (sizeof(R) == 4)
-      r[0] = __uint_as_float(packed);
-    else
-      r[0] = __longlong_as_double((long long)packed);
+    r[0] = pack_word<R>((uint32_t)l0 | ((uint32_t)l1 << 8) | ((uint32_t)l2 << 16) |
+                        ((uint32_t)sp << 24));
     // The separable kernel values of the w support cells along each axis,
     // evaluated once per atom (the spread reuses them for every tile).
 #pragma unroll
@@ -174,32 +187,39 @@ __global__ void k_scatter(const double *__restrict__ pos, const uint8_t *__restr
   }
 }
 
-template <typename R> __device__ __forceinline__ uint32_t rec_packed(const R *r);
-template <> __device__ __forceinline__ uint32_t rec_packed<float>(const float *r) {
-  return __float_as_uint(r[0]);
-}
-template <> __device__ __forceinline__ uint32_t rec_packed<double>(const double *r) {
-  return (uint32_t)__double_as_longlong(r[0]);
+// Does the cyclic support [r, r+w) (mod n) meet the cells [b, b+len)?
+__device__ __forceinline__ bool cyc_meet(int r, int w, int b, int len, int n) {
+  if (len <= 0) return false;
+  int d1 = b - r;
+  if (d1 < 0) d1 += n;
+  int d2 = r - b;
+  if (d2 < 0) d2 += n;
+  return d1 < w || d2 < len;
 }
 
 // ---------------------------------------------------------------------------
 // Gather spreading, one CTA per 32 x 16 x 8 tile for all transforms.
 // NT > 0: exactly NT transforms; NT == 0: any ntr <= MAX_FAST_T.
+// Shared memory per staged point: its record (kernel values), its shifted z
+// row (strength folded in), (rx, ry, rz, species) relative to the tile, the
+// mask of the 8 x 4 patches it reaches, and its record index.
 // ---------------------------------------------------------------------------
 template <typename R, int NT>
 __global__ void __launch_bounds__(SPREAD_THREADS, (sizeof(R) == 4 || NT == 1) ? 2 : 1)
     k_spread(const R *__restrict__ recs, const int *__restrict__ starts, FrameGeom g,
              const R *__restrict__ strength, R *__restrict__ grid) {
   constexpr int TM = NT > 0 ? NT : MAX_FAST_T;
+  const int chunk = g.chunk, stride = g.rec_stride;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  R *s_rows = reinterpret_cast<R *>(smem_raw);                      // [CHUNK][ROW]
-  int4 *s_meta = reinterpret_cast<int4 *>(s_rows + CHUNK * ROW);    // [CHUNK] rx, ry, rz, sp
-  int *s_rec = reinterpret_cast<int *>(s_meta + CHUNK);             // [CHUNK] record index
-  unsigned *s_mask = reinterpret_cast<unsigned *>(s_rec + CHUNK);   // [CHUNK] patch masks
+  R *s_vals = reinterpret_cast<R *>(smem_raw);                        // [chunk][stride]
+  R *s_zrow = s_vals + (size_t)chunk * stride;                        // [chunk][TILE_Z]
+  int4 *s_meta = reinterpret_cast<int4 *>(s_zrow + (size_t)chunk * TILE_Z);  // [chunk]
+  int *s_rec = reinterpret_cast<int *>(s_meta + chunk);               // [chunk]
+  unsigned *s_mask = reinterpret_cast<unsigned *>(s_rec + chunk);     // [chunk]
   __shared__ int s_bstart[MAX_NB];
   __shared__ int s_bpref[MAX_NB + 1];
   __shared__ int s_borg[MAX_NB][3];
-  __shared__ int s_wcount[SPREAD_WARPS];
+  __shared__ int s_wcount[MAX_FAST_T * SPREAD_WARPS];
   __shared__ int s_bl[3][MAX_BINS_DIM];
   __shared__ int s_nbl[3];
 
@@ -215,6 +235,7 @@ __global__ void __launch_bounds__(SPREAD_THREADS, (sizeof(R) == 4 || NT == 1) ? 
   const int tx = min(g.tile[0], g.nf[0] - X0);
   const int ty = min(g.tile[1], g.nf[1] - Y0);
   const int tz = min(g.tile[2], g.nf[2] - Z0);
+  const int w = g.w;
 
   // Bins whose points can reach this tile, per dimension: a support starting
   // at cell c covers c .. c+w-1, so the start cells that matter are
@@ -225,10 +246,10 @@ __global__ void __launch_bounds__(SPREAD_THREADS, (sizeof(R) == 4 || NT == 1) ? 
     const int t = d == 0 ? t0 : (d == 1 ? t1 : t2);
     const int Xd = t * T, td = min(T, n - Xd);
     int cnt = 0;
-    if (g.w - 1 + td >= n) {
+    if (w - 1 + td >= n) {
       for (int b = 0; b < nt && cnt < MAX_BINS_DIM; ++b) s_bl[d][cnt++] = b;
     } else {
-      const int ws = Xd - (g.w - 1);
+      const int ws = Xd - (w - 1);
       if (ws >= 0) {
         for (int b = ws / T; b <= t && cnt < MAX_BINS_DIM; ++b) s_bl[d][cnt++] = b;
       } else {
@@ -266,97 +287,126 @@ __global__ void __launch_bounds__(SPREAD_THREADS, (sizeof(R) == 4 || NT == 1) ? 
 #pragma unroll
     for (int z = 0; z < TILE_Z; ++z) acc[t][z] = R(0);
   const unsigned xbit = 1u << (warp & 3), ybit = 1u << (4 + (warp >> 2));
+  const int units = stride * (int)sizeof(R) / 16;  // 16-byte units per record
 
-  for (int base = 0; base < total; base += CHUNK) {
-    // Stage the candidates that overlap the tile (compacted, order kept).
+  for (int base = 0; base < total; base += chunk) {
+    // 1. candidates that overlap the tile, compacted (order kept)
     const int i = base + tid;
     bool keep = false;
     int4 meta = make_int4(0, 0, 0, 0);
     int ridx = 0;
-    if (tid < CHUNK && i < total) {
+    if (tid < chunk && i < total) {
       int b = 0;
       while (i >= s_bpref[b + 1]) ++b;
       ridx = s_bstart[b] + (i - s_bpref[b]);
-      const uint32_t packed = rec_packed<R>(recs + (int64_t)ridx * g.rec_stride);
+      const uint32_t packed = unpack_word<R>(recs[(int64_t)ridx * stride]);
       int rx = s_borg[b][0] + (int)(packed & 255u) - X0;
       int ry = s_borg[b][1] + (int)((packed >> 8) & 255u) - Y0;
       int rz = s_borg[b][2] + (int)((packed >> 16) & 255u) - Z0;
       if (rx < 0) rx += g.nf[0];
       if (ry < 0) ry += g.nf[1];
       if (rz < 0) rz += g.nf[2];
-      keep = (rx < tx || rx + g.w > g.nf[0]) && (ry < ty || ry + g.w > g.nf[1]) &&
-             (rz < tz || rz + g.w > g.nf[2]);
+      keep = (rx < tx || rx + w > g.nf[0]) && (ry < ty || ry + w > g.nf[1]) &&
+             (rz < tz || rz + w > g.nf[2]);
       meta = make_int4(rx, ry, rz, (int)(packed >> 24));
     }
-    const unsigned bal = __ballot_sync(FULL, keep);
-    if (lane == 0) s_wcount[warp] = __popc(bal);
-    __syncthreads();
-    int wbase = 0, npts = 0;
+    // Counting sort of the kept points by transform (order kept within one),
+    // so that each transform's points form one contiguous range.
+    const int my_t = ntr > 1 ? meta.w : 0;
+    unsigned my_bal = 0u;
 #pragma unroll
-    for (int k = 0; k < SPREAD_WARPS; ++k) {
-      const int cnt = s_wcount[k];
-      wbase += k < warp ? cnt : 0;
-      npts += cnt;
+    for (int t = 0; t < TM; ++t) {
+      if (t < ntr) {
+        const unsigned bt = __ballot_sync(FULL, keep && my_t == t);
+        if (lane == 0) s_wcount[t * SPREAD_WARPS + warp] = __popc(bt);
+        if (t == my_t) my_bal = bt;
+      }
     }
+    __syncthreads();
+    int tstart[TM + 1];
+    tstart[0] = 0;
+#pragma unroll
+    for (int t = 0; t < TM; ++t) {
+      int tot = 0;
+      if (t < ntr)
+#pragma unroll
+        for (int k = 0; k < SPREAD_WARPS; ++k) tot += s_wcount[t * SPREAD_WARPS + k];
+      tstart[t + 1] = tstart[t] + tot;
+    }
+    const int npts = tstart[TM];
     if (keep) {
-      const int p = wbase + __popc(bal & ((1u << lane) - 1u));
+      int p = __popc(my_bal & ((1u << lane) - 1u));
+#pragma unroll
+      for (int t = 0; t < TM; ++t)
+        if (t == my_t) p += tstart[t];
+      for (int k = 0; k < warp; ++k) p += s_wcount[my_t * SPREAD_WARPS + k];
       s_meta[p] = meta;
       s_rec[p] = ridx;
-      s_mask[p] = 0u;
     }
     __syncthreads();
 
-    // Kernel rows of every staged point shifted into tile coordinates (taken
-    // from the record), the strength folded into the z row, and the mask of
-    // the x / y patches each point reaches.
-    for (int e = tid; e < npts * ROW; e += SPREAD_THREADS) {
-      const int p = e / ROW, c = e - p * ROW;
+    // 2. copy the kept records into shared memory (16-byte vector loads)
+    {
+      const float4 *src = reinterpret_cast<const float4 *>(recs);
+      float4 *dst = reinterpret_cast<float4 *>(s_vals);
+      for (int e = tid; e < npts * units; e += SPREAD_THREADS) {
+        const int p = e / units, u = e - p * units;
+        dst[e] = src[(int64_t)s_rec[p] * units + u];
+      }
+    }
+    __syncthreads();
+
+    // 3. per point: the patches it reaches and its z row shifted into the tile
+    for (int p = tid; p < npts; p += SPREAD_THREADS) {
       const int4 m = s_meta[p];
-      int d, cell, te, r, n;
-      if (c < TILE_X) {
-        d = 0; cell = c; te = tx; r = m.x; n = g.nf[0];
-      } else if (c < TILE_X + TILE_Y) {
-        d = 1; cell = c - TILE_X; te = ty; r = m.y; n = g.nf[1];
-      } else {
-        d = 2; cell = c - TILE_X - TILE_Y; te = tz; r = m.z; n = g.nf[2];
+      unsigned mask = 0u;
+#pragma unroll
+      for (int k = 0; k < TILE_X / PATCH_X; ++k)
+        if (cyc_meet(m.x, w, k * PATCH_X, min(PATCH_X, tx - k * PATCH_X), g.nf[0]))
+          mask |= 1u << k;
+#pragma unroll
+      for (int k = 0; k < TILE_Y / PATCH_Y; ++k)
+        if (cyc_meet(m.y, w, k * PATCH_Y, min(PATCH_Y, ty - k * PATCH_Y), g.nf[1]))
+          mask |= 1u << (4 + k);
+      s_mask[p] = mask;
+      const R *v = s_vals + (size_t)p * stride + 1 + 2 * w;
+      const R sw = strength[m.w];
+#pragma unroll
+      for (int z = 0; z < TILE_Z; ++z) {
+        int k = z - m.z;
+        if (k < 0) k += g.nf[2];
+        s_zrow[p * TILE_Z + z] = (z < tz && k < w) ? v[k] * sw : R(0);
       }
-      R v = R(0);
-      if (cell < te) {
-        int k = cell - r;
-        if (k < 0) k += n;
-        if (k < g.w) {
-          v = recs[(int64_t)s_rec[p] * g.rec_stride + 1 + d * g.w + k];
-          if (d == 2) v *= strength[m.w];
-        }
-      }
-      s_rows[e] = v;
-      if (v != R(0) && d < 2)
-        atomicOr(&s_mask[p], d == 0 ? (1u << (cell >> 3)) : (1u << (4 + (cell >> 2))));
     }
     __syncthreads();
 
-    // Each warp walks only the points that reach its patch.
-    for (int pb = 0; pb < npts; pb += 32) {
-      const int p = pb + lane;
-      bool act = false;
-      if (p < npts) {
-        const unsigned m = s_mask[p];
-        act = (m & xbit) && (m & ybit);
-      }
-      unsigned am = __ballot_sync(FULL, act);
-      while (am) {
-        const int q = pb + __ffs(am) - 1;
-        am &= am - 1u;
-        const R *row = s_rows + q * ROW;
-        const R a = row[cx] * row[TILE_X + cy];
-        const int tr = ntr > 1 ? s_meta[q].w : 0;  // the same for the whole warp
+    // 4. each warp walks only the points that reach its patch, transform by
+    //    transform (static accumulator indices)
 #pragma unroll
-        for (int t = 0; t < TM; ++t) {
-          if (t == tr) {
+    for (int t = 0; t < TM; ++t) {
+      if (t >= ntr) break;
+      const int tend = tstart[t + 1];
+      for (int pb = tstart[t]; pb < tend; pb += 32) {
+        const int p = pb + lane;
+        bool act = false;
+        if (p < tend) {
+          const unsigned m = s_mask[p];
+          act = (m & xbit) && (m & ybit);
+        }
+        unsigned am = __ballot_sync(FULL, act);
+        while (am) {
+          const int q = pb + __ffs(am) - 1;
+          am &= am - 1u;
+          const int4 m = s_meta[q];
+          const R *v = s_vals + (size_t)q * stride + 1;
+          int kx = cx - m.x;
+          if (kx < 0) kx += g.nf[0];
+          int ky = cy - m.y;
+          if (ky < 0) ky += g.nf[1];
+          const R a = (kx < w ? v[kx] : R(0)) * (ky < w ? v[w + ky] : R(0));
+          const R *zr = s_zrow + q * TILE_Z;
 #pragma unroll
-            for (int z = 0; z < TILE_Z; ++z)
-              acc[t][z] = fma(a, row[TILE_X + TILE_Y + z], acc[t][z]);
-          }
+          for (int z = 0; z < TILE_Z; ++z) acc[t][z] = fma(a, zr[z], acc[t][z]);
         }
       }
     }
@@ -626,7 +676,8 @@ static int grid_for(int64_t n, int threads) {
 template <typename R>
 cudaError_t launch_prep(const double *pos, const uint8_t *species, const FrameGeom &g,
                         int *counts, uint32_t *key, uint32_t *slot, cudaStream_t s) {
-  k_prep<<<grid_for(g.natoms, 256), 256, 0, s>>>(pos, species, g, counts, key, slot);
+  (void)species;
+  k_prep<<<grid_for(g.natoms, 256), 256, 0, s>>>(pos, g, counts, key, slot);
   return cudaGetLastError();
 }
 
@@ -643,33 +694,58 @@ cudaError_t launch_scatter(const double *pos, const uint8_t *species, const Fram
   return cudaGetLastError();
 }
 
-size_t spread_smem_bytes(bool fp64) {
+size_t spread_point_bytes(int stride, bool fp64) {
   const size_t r = fp64 ? 8 : 4;
-  return (size_t)CHUNK * ROW * r + (size_t)CHUNK * (sizeof(int4) + 2 * sizeof(int));
+  return (size_t)stride * r + (size_t)TILE_Z * r + sizeof(int4) + 2 * sizeof(int);
 }
 
-template <typename R> static cudaError_t spread_attr(bool fp64) {
-  const int b = (int)spread_smem_bytes(fp64);
-  cudaError_t e = cudaSuccess;
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_spread<R, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_spread<R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_spread<R, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_spread<R, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_spread<R, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+size_t spread_smem_bytes(int chunk, int stride, bool fp64) {
+  return (size_t)chunk * spread_point_bytes(stride, fp64);
+}
+
+int spread_chunk(int stride, bool fp64) {
+  // Two CTAs per SM when the staging fits in ~110 KB, else one (<= 220 KB).
+  const size_t per = spread_point_bytes(stride, fp64);
+  int c = (int)((110 * 1024) / per);
+  if (c < 128) c = (int)((220 * 1024) / per);
+  c = c > SPREAD_THREADS ? SPREAD_THREADS : c;
+  return c / 32 * 32;
+}
+
+// Allow each spread instantiation the device's opt-in shared memory minus its
+// static shared memory.
+template <typename K> static cudaError_t smem_optin(K kernel, int optin) {
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, kernel);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              optin - (int)fa.sharedSizeBytes);
+}
+
+template <typename R> static cudaError_t spread_attr(int optin) {
+  cudaError_t e = smem_optin(k_spread<R, 1>, optin);
+  if (e == cudaSuccess) e = smem_optin(k_spread<R, 2>, optin);
+  if (e == cudaSuccess) e = smem_optin(k_spread<R, 3>, optin);
+  if (e == cudaSuccess) e = smem_optin(k_spread<R, 4>, optin);
+  if (e == cudaSuccess) e = smem_optin(k_spread<R, 0>, optin);
   return e;
 }
 
 cudaError_t spread_set_attributes() {
-  cudaError_t e = spread_attr<float>(false);
-  if (e != cudaSuccess) return e;
-  return spread_attr<double>(true);
+  int dev = 0, optin = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess)
+    e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (e == cudaSuccess) e = spread_attr<float>(optin);
+  if (e == cudaSuccess) e = spread_attr<double>(optin);
+  return e;
 }
 
 template <typename R>
 cudaError_t launch_spread(const R *recs, const int *starts, const FrameGeom &g,
                           const R *strength, R *grid, cudaStream_t s) {
   const dim3 grd((unsigned)g.ntiles);
-  const size_t sm = spread_smem_bytes(sizeof(R) == 8);
+  const size_t sm = spread_smem_bytes(g.chunk, g.rec_stride, sizeof(R) == 8);
   switch (g.ntr) {
     case 1: k_spread<R, 1><<<grd, SPREAD_THREADS, sm, s>>>(recs, starts, g, strength, grid); break;
     case 2: k_spread<R, 2><<<grd, SPREAD_THREADS, sm, s>>>(recs, starts, g, strength, grid); break;
