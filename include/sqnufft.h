@@ -65,7 +65,8 @@ enum { SQN_PREC_DOUBLE = 0, SQN_PREC_SINGLE = 1 };
 enum { SQN_HOST = 0, SQN_DEVICE = 1 };
 /* sqn_plan_desc.flags */
 enum {
-  SQN_FLAG_TIMING = 1 /* record per-stage CUDA events (sqn_stage_times) */
+  SQN_FLAG_TIMING = 1, /* record per-stage CUDA events (sqn_stage_times) */
+  SQN_FLAG_GRAD = 2    /* allocate the adjoint buffers of sqn_sq_grad */
 };
 
 /* Everything sqcalc's configure + gpu_setup know after the first frame
@@ -172,6 +173,19 @@ int sqn_reset(sqn_plan *plan);
  * out[0] wrap+bin sort, out[1] spread, out[2] FFT, out[3] deconvolve+bin,
  * out[4] frames timed.  Needs SQN_FLAG_TIMING. */
 int sqn_stage_times(sqn_plan *plan, double *out, int32_t n);
+
+/* One frame, outside the accumulators: S_frame(q) = sum_{h in shell} |T(h)|^2 / den
+ * and, when dLdS is given, the gradient of L = sum_s dLdS[s] * S_frame(s) with
+ * respect to the Cartesian positions (q-independent weights; the plan needs
+ * SQN_FLAG_GRAD).  pos [natoms][3] and grad [natoms][3] live in host (SQN_HOST)
+ * or device (SQN_DEVICE) memory; dLdS [nq] and S [nq] in host memory; S may be
+ * NULL.  The forward transform is recomputed (nothing is kept from earlier
+ * calls); the adjoint is three type-2 NUFFTs (amplify, C2R FFT, ES
+ * interpolation).  No counterpart in the reference, which has no gradient;
+ * it differentiates the direct sum of src/sqc_structure_factor.f90:1440-1456.
+ * Synchronous. */
+int sqn_sq_grad(sqn_plan *plan, const double *pos, int32_t where, const double *dLdS, double *S,
+                double *grad);
 
 /* Number of this library's own kernel launches so far (cuFFT's not counted). */
 int64_t sqn_launch_count(const sqn_plan *plan);

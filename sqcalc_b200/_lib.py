@@ -22,13 +22,14 @@ NORM_MEAN, NORM_SELF, NORM_NATOM = 1, 2, 3
 PREC_DOUBLE, PREC_SINGLE = 0, 1
 HOST, DEVICE = 0, 1
 FLAG_TIMING = 1
+FLAG_GRAD = 2
 
 # Every symbol include/sqnufft.h declares.
 EXPORTS = (
     "sqn_abi_version", "sqn_error_string", "sqn_default_desc", "sqn_plan_create",
     "sqn_plan_info_get", "sqn_accumulate_frames", "sqn_sync", "sqn_get_accumulators",
     "sqn_peek_num_async", "sqn_finalize", "sqn_reset", "sqn_stage_times", "sqn_launch_count",
-    "sqn_plan_destroy", "sqn_spread_frame_noalloc",
+    "sqn_plan_destroy", "sqn_spread_frame_noalloc", "sqn_sq_grad",
 )
 ERR_SCRATCH_LIMIT = 49
 NOALLOC_SCRATCH_BYTES = 32 * 1024 * 1024
@@ -116,6 +117,7 @@ def load():
     L.sqn_launch_count.argtypes = [vp]
     L.sqn_launch_count.restype = i64
     L.sqn_plan_destroy.argtypes = [vp]
+    L.sqn_sq_grad.argtypes = [vp, vp, ctypes.c_int32, vp, vp, vp]
     L.sqn_spread_frame_noalloc.argtypes = [vp, i64, vp, ctypes.c_int32, vp, vp, vp, vp,
                                            ctypes.c_int32, ctypes.c_double, vp, vp]
     if L.sqn_abi_version() != ABI_VERSION:
@@ -148,7 +150,8 @@ class Plan:
     def __init__(self, cell, origin, type_id, ntypes=None, weight=WEIGHT_UNIT, amp_const=None,
                  xray_coef=None, qmin=0.0, qmax=20.0, nq=500, norm=NORM_MEAN, partials=True,
                  want_grid=False, precision=PREC_DOUBLE, eps=1e-9, upsampfac=0.0,
-                 kernel_width=0, device=0, max_grid_modes=0, timing=False, stream=None):
+                 kernel_width=0, device=0, max_grid_modes=0, timing=False, stream=None,
+                 grad=False):
         L = load()
         self._L = L
         self.type_id = np.ascontiguousarray(type_id, dtype=np.int32)
@@ -180,7 +183,7 @@ class Plan:
         d.partials = int(bool(partials))
         d.want_grid = int(bool(want_grid))
         d.precision = int(precision)
-        d.flags = FLAG_TIMING if timing else 0
+        d.flags = (FLAG_TIMING if timing else 0) | (FLAG_GRAD if grad else 0)
         d.eps = float(eps)
         d.upsampfac = float(upsampfac)
         d.kernel_width = int(kernel_width)
@@ -242,6 +245,29 @@ class Plan:
                                    ctypes.cast(ctypes.byref(nf), ctypes.c_void_p)),
               "sqn_finalize")
         return s, sp.reshape(nq, T, T).transpose(2, 1, 0), sg, int(nf.value)
+
+    def sq_grad(self, pos, dLdS=None):
+        """One frame: S(q) of that frame and, with dLdS, dL/dr for L = sum dLdS * S.
+
+        pos: (natoms, 3) float64 numpy array (host) or a torch CUDA tensor
+        (device; the gradient is then a torch CUDA tensor too)."""
+        nq = self.nq
+        S = np.zeros(nq)
+        g = None if dLdS is None else np.ascontiguousarray(dLdS, dtype=np.float64)
+        if hasattr(pos, "data_ptr"):  # torch tensor on the device
+            import torch
+            pos = pos.contiguous()
+            grad = torch.empty_like(pos) if g is not None else None
+            torch.cuda.current_stream().synchronize()
+            check(self._L.sqn_sq_grad(self._h, ctypes.c_void_p(pos.data_ptr()), DEVICE, _ptr(g),
+                                      _ptr(S), ctypes.c_void_p(grad.data_ptr()) if grad is not None
+                                      else None), "sqn_sq_grad")
+            return S, grad
+        a = np.ascontiguousarray(pos, dtype=np.float64)
+        grad = np.zeros((self.natoms, 3)) if g is not None else None
+        check(self._L.sqn_sq_grad(self._h, _ptr(a), HOST, _ptr(g), _ptr(S), _ptr(grad)),
+              "sqn_sq_grad")
+        return S, grad
 
     def peek_num_async(self, host_buf_ptr):
         check(self._L.sqn_peek_num_async(self._h, ctypes.c_void_p(host_buf_ptr)), "sqn_peek")

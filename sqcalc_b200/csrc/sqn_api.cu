@@ -256,6 +256,13 @@ struct sqn_plan_s {
   double *d_acc = nullptr, *d_gnum = nullptr, *d_den = nullptr, *d_cnt = nullptr;
   cufftHandle fft = 0;
   bool fft_ok = false;
+  // adjoint (SQN_FLAG_GRAD)
+  bool grad_ok = false;
+  int32_t *d_orig = nullptr;
+  void *d_F = nullptr, *d_U = nullptr, *d_wstrength = nullptr;
+  double *d_grad = nullptr, *d_gsh = nullptr, *d_num1 = nullptr;
+  cufftHandle fft_fwd1 = 0, fft_inv3 = 0;
+  bool fft_fwd1_ok = false, fft_inv3_ok = false;
   int64_t gnum_half = 0;
 
   int64_t nframes = 0;
@@ -297,6 +304,8 @@ void free_plan(sqn_plan *p) {
   if (p->stream) cudaStreamSynchronize(p->stream);
   if (p->copy_stream) cudaStreamSynchronize(p->copy_stream);
   if (p->fft_ok) cufftDestroy(p->fft);
+  if (p->fft_fwd1_ok) cufftDestroy(p->fft_fwd1);
+  if (p->fft_inv3_ok) cufftDestroy(p->fft_inv3);
   for (void *v : p->allocs) cudaFree(v);
   for (int i = 0; i < 2; ++i) {
     if (p->ev_copied[i]) cudaEventDestroy(p->ev_copied[i]);
@@ -629,8 +638,98 @@ int setup_plan(sqn_plan *p, const sqn_plan_desc *d) {
     p->device_bytes += (int64_t)ws;
     if (cufftSetStream(p->fft, s) != CUFFT_SUCCESS) return SQN_ERR_CUFFT;
   }
+
+  // --- adjoint buffers (dS/dr) -----------------------------------------------
+  if (d->flags & SQN_FLAG_GRAD) {
+    if (xray) return SQN_ERR_NOT_SUPPORTED;
+    char *v;
+    if ((st = dalloc(p, &p->d_orig, (size_t)N))) return st;
+    if ((st = dalloc(p, &v, (size_t)3 * b.vol_cplx * 2 * rsz))) return st;
+    p->d_F = v;
+    if ((st = dalloc(p, &v, (size_t)3 * g.vol_real * rsz))) return st;
+    p->d_U = v;
+    if ((st = dalloc(p, &v, (size_t)p->nspecies * rsz))) return st;
+    p->d_wstrength = v;
+    if ((st = dalloc(p, &p->d_grad, (size_t)3 * N))) return st;
+    if ((st = dalloc(p, &p->d_gsh, (size_t)d->nq))) return st;
+    if ((st = dalloc(p, &p->d_num1, (size_t)d->nq))) return st;
+    cudaError_t ce;
+    if (p->fp64) {
+      ce = cudaMemcpy(p->d_wstrength, p->amp_sp.data(), p->amp_sp.size() * 8, cudaMemcpyHostToDevice);
+    } else {
+      std::vector<float> f = to_r<float>(p->amp_sp);
+      ce = cudaMemcpy(p->d_wstrength, f.data(), f.size() * 4, cudaMemcpyHostToDevice);
+    }
+    if (ce != cudaSuccess) return SQN_ERR_CUDA;
+    long long n[3] = {p->nf[2], p->nf[1], p->nf[0]};
+    long long rembed[3] = {p->nf[2], p->nf[1], g.pitch};
+    long long cembed[3] = {p->nf[2], p->nf[1], b.c1};
+    size_t ws = 0;
+    if (cufftCreate(&p->fft_fwd1) != CUFFT_SUCCESS) return SQN_ERR_CUFFT;
+    p->fft_fwd1_ok = true;
+    if (cufftMakePlanMany64(p->fft_fwd1, 3, n, rembed, 1, g.vol_real, cembed, 1, b.vol_cplx,
+                            p->fp64 ? CUFFT_D2Z : CUFFT_R2C, 1, &ws) != CUFFT_SUCCESS)
+      return SQN_ERR_CUFFT;
+    p->device_bytes += (int64_t)ws;
+    if (cufftCreate(&p->fft_inv3) != CUFFT_SUCCESS) return SQN_ERR_CUFFT;
+    p->fft_inv3_ok = true;
+    if (cufftMakePlanMany64(p->fft_inv3, 3, n, cembed, 1, b.vol_cplx, rembed, 1, g.vol_real,
+                            p->fp64 ? CUFFT_Z2D : CUFFT_C2R, 3, &ws) != CUFFT_SUCCESS)
+      return SQN_ERR_CUFFT;
+    p->device_bytes += (int64_t)ws;
+    if (cufftSetStream(p->fft_fwd1, s) != CUFFT_SUCCESS ||
+        cufftSetStream(p->fft_inv3, s) != CUFFT_SUCCESS)
+      return SQN_ERR_CUFFT;
+    p->grad_ok = true;
+  }
   if (cudaStreamSynchronize(s) != cudaSuccess) return SQN_ERR_CUDA;
   return warn;
+}
+
+// One frame through the weighted forward transform and, with gsh, its adjoint.
+template <typename R> int grad_frame(sqn_plan *p, const double *dpos, bool want_grad) {
+  cudaStream_t s = p->stream;
+  FrameGeom g = p->fg;
+  g.ntr = 1;  // the total T(h) = sum_j c_j exp(i q.r_j): one weighted transform
+  BinGeom b = p->bg;
+  b.ntr = 1;
+  b.partials = 0;
+  b.want_grid = 0;
+  b.nquant = 1;
+  cudaError_t e = launch_prep<R>(dpos, p->d_species, g, p->d_counts, p->d_key, p->d_slot, s);
+  if (e == cudaSuccess) e = launch_scan(p->d_counts, p->d_starts, p->nkeys, s);
+  if (e == cudaSuccess)
+    e = launch_scatter<R>(dpos, p->d_species, g, p->d_key, p->d_slot, p->d_starts,
+                          (R *)p->d_recs, p->d_orig, s);
+  if (e == cudaSuccess)
+    e = launch_spread<R>((const R *)p->d_recs, p->d_starts, g, (const R *)p->d_wstrength,
+                         (R *)p->d_grid, s);
+  if (e != cudaSuccess) return SQN_ERR_CUDA;
+  cufftResult fr = p->fp64 ? cufftExecD2Z(p->fft_fwd1, (cufftDoubleReal *)p->d_grid,
+                                          (cufftDoubleComplex *)p->d_G)
+                           : cufftExecR2C(p->fft_fwd1, (cufftReal *)p->d_grid, (cufftComplex *)p->d_G);
+  if (fr != CUFFT_SUCCESS) return SQN_ERR_CUFFT;
+  if (cudaMemsetAsync(p->d_num1, 0, sizeof(double) * (size_t)b.nq, s) != cudaSuccess)
+    return SQN_ERR_CUDA;
+  if (want_grad &&
+      cudaMemsetAsync(p->d_F, 0, (size_t)3 * b.vol_cplx * 2 * sizeof(R), s) != cudaSuccess)
+    return SQN_ERR_CUDA;
+  e = launch_adj_coef<R>(p->d_rows, p->nrows, p->d_G, b, (const R *)p->d_inv[0],
+                         (const R *)p->d_inv[1], (const R *)p->d_inv[2], p->d_gsh, p->d_num1,
+                         want_grad ? p->d_F : nullptr, p->nsm, s);
+  if (e != cudaSuccess) return SQN_ERR_CUDA;
+  p->launches += 5;
+  if (!want_grad) return SQN_OK;
+  fr = p->fp64 ? cufftExecZ2D(p->fft_inv3, (cufftDoubleComplex *)p->d_F, (cufftDoubleReal *)p->d_U)
+               : cufftExecC2R(p->fft_inv3, (cufftComplex *)p->d_F, (cufftReal *)p->d_U);
+  if (fr != CUFFT_SUCCESS) return SQN_ERR_CUFFT;
+  Recip rb;
+  std::memcpy(rb.b, p->recip, sizeof(rb.b));
+  e = launch_interp<R>((const R *)p->d_recs, p->d_orig, dpos, p->fg, (const R *)p->d_U, rb,
+                       p->d_amp_sp, p->d_grad, s);
+  if (e != cudaSuccess) return SQN_ERR_CUDA;
+  p->launches += 1;
+  return SQN_OK;
 }
 
 template <typename R> int run_frame(sqn_plan *p, const double *dpos, int slot) {
@@ -651,7 +750,7 @@ template <typename R> int run_frame(sqn_plan *p, const double *dpos, int slot) {
   if (e == cudaSuccess) e = launch_scan(p->d_counts, p->d_starts, p->nkeys, s);
   if (e == cudaSuccess)
     e = launch_scatter<R>(dpos, p->d_species, g, p->d_key, p->d_slot, p->d_starts,
-                          (R *)p->d_recs, s);
+                          (R *)p->d_recs, nullptr, s);
   if (e != cudaSuccess) return SQN_ERR_CUDA;
   if (slot >= 0) cudaEventRecord(p->ev_free[slot], s);
   if (p->timing) cudaEventRecord(ev[1], s);
@@ -978,6 +1077,47 @@ int sqn_stage_times(sqn_plan *p, double *out, int32_t n) {
   harvest_timing(p);
   double v[5] = {p->stage_ms[0], p->stage_ms[1], p->stage_ms[2], p->stage_ms[3], (double)p->stage_frames};
   for (int i = 0; i < n && i < 5; ++i) out[i] = v[i];
+  return SQN_OK;
+}
+
+int sqn_sq_grad(sqn_plan *p, const double *pos, int32_t where, const double *dLdS, double *S,
+                double *grad) {
+  if (!p) return SQN_ERR_PLAN_NOTVALID;
+  if (!p->grad_ok) return SQN_ERR_NOT_SUPPORTED;
+  if (!pos || (where != SQN_HOST && where != SQN_DEVICE) || (dLdS && !grad))
+    return SQN_ERR_INVALID_ARGUMENT;
+  DeviceGuard guard(p->device);
+  cudaStream_t s = p->stream;
+  const int64_t N = p->desc.natoms;
+  const int nq = p->desc.nq;
+  const double *dpos = pos;
+  if (where == SQN_HOST) {
+    // the copy stream may still be filling this slot for an earlier call
+    if (cudaStreamSynchronize(p->copy_stream) != cudaSuccess ||
+        cudaMemcpyAsync(p->d_pos[0], pos, sizeof(double) * 3 * (size_t)N, cudaMemcpyHostToDevice,
+                        s) != cudaSuccess)
+      return SQN_ERR_CUDA;
+    dpos = p->d_pos[0];
+  }
+  std::vector<double> gsh(nq, 0.0);
+  if (dLdS)
+    for (int k = 0; k < nq; ++k) gsh[k] = p->den[k] > 0.0 ? dLdS[k] / p->den[k] : 0.0;
+  if (cudaMemcpyAsync(p->d_gsh, gsh.data(), sizeof(double) * nq, cudaMemcpyHostToDevice, s) !=
+      cudaSuccess)
+    return SQN_ERR_CUDA;
+  const int st = p->fp64 ? grad_frame<double>(p, dpos, dLdS != nullptr)
+                         : grad_frame<float>(p, dpos, dLdS != nullptr);
+  if (st != SQN_OK) return st;
+  std::vector<double> num(nq);
+  cudaError_t e = cudaMemcpyAsync(num.data(), p->d_num1, sizeof(double) * nq,
+                                  cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess && dLdS)
+    e = cudaMemcpyAsync(grad, p->d_grad, sizeof(double) * 3 * (size_t)N,
+                        where == SQN_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return SQN_ERR_CUDA;
+  if (S)
+    for (int k = 0; k < nq; ++k) S[k] = p->den[k] > 0.0 ? num[k] / p->den[k] : 0.0;
   return SQN_OK;
 }
 

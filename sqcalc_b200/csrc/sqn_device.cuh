@@ -1,0 +1,178 @@
+// Device helpers shared by the per-frame kernels (sqn_kernels.cu) and the
+// adjoint kernels (sqn_adjoint.cu).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "sqn_internal.h"
+
+namespace sqn {
+namespace dev {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+// ---------------------------------------------------------------------------
+// Atom -> fine grid
+// ---------------------------------------------------------------------------
+
+struct AtomCell {
+  int ix0[3];     // first support cell, wrapped into [0, nf)
+  double off[3];  // (X - ix0) - (w/2 - 1/2), in (-1/2, 1/2]
+};
+
+// s = A^-1 (r - origin), s -= floor(s)  (cell_fractional, src/sqc_cell.f90:143-152,
+// and the wrap of src/sqc_gpu.f90:230-236); X = nf * s is the fine-grid coordinate.
+__device__ __forceinline__ void atom_cell(const double *__restrict__ pos, int64_t i,
+                                          const FrameGeom &g, AtomCell &c) {
+  const double d0 = __dsub_rn(pos[3 * i + 0], g.origin[0]);
+  const double d1 = __dsub_rn(pos[3 * i + 1], g.origin[1]);
+  const double d2 = __dsub_rn(pos[3 * i + 2], g.origin[2]);
+  const double halfw = 0.5 * (double)g.w;
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    double s = __dadd_rn(__dadd_rn(__dmul_rn(g.inv[r], d0), __dmul_rn(g.inv[3 + r], d1)),
+                         __dmul_rn(g.inv[6 + r], d2));
+    s = __dsub_rn(s, floor(s));
+    // A non-finite coordinate must not index outside the grid: park it at 0.
+    if (!(s >= 0.0 && s <= 1.0)) s = 0.0;
+    const double X = __dmul_rn((double)g.nf[r], s);
+    const double start = ceil(__dsub_rn(X, halfw));
+    c.off[r] = __dsub_rn(__dsub_rn(X, start), halfw - 0.5);
+    int ix0 = (int)start;
+    if (ix0 < 0) ix0 += g.nf[r];
+    if (ix0 >= g.nf[r]) ix0 -= g.nf[r];
+    c.ix0[r] = ix0;
+  }
+}
+
+// Home tile of the support start (one bin per tile holds every transform) and
+// the start cell relative to the tile origin.
+__device__ __forceinline__ uint32_t home_key(const AtomCell &c, const FrameGeom &g, int &l0,
+                                             int &l1, int &l2) {
+  const int t0 = c.ix0[0] / g.tile[0], t1 = c.ix0[1] / g.tile[1], t2 = c.ix0[2] / g.tile[2];
+  l0 = c.ix0[0] - t0 * g.tile[0];
+  l1 = c.ix0[1] - t1 * g.tile[1];
+  l2 = c.ix0[2] - t2 * g.tile[2];
+  return (uint32_t)((t2 * g.ntile[1] + t1) * g.ntile[0] + t0);
+}
+
+// ES kernel: phi(t) = exp(beta (sqrt(1 - (2t/w)^2) - 1)) on |t| < w/2, else 0
+// (external/finufft/include/cufinufft/spreadinterp.h:84-98).
+__device__ __forceinline__ float es_phi(float t, float c2, float beta) {
+  const float z2 = c2 * t * t;
+  return z2 < 1.0f ? expf(beta * (sqrtf(1.0f - z2) - 1.0f)) : 0.0f;
+}
+__device__ __forceinline__ double es_phi(double t, double c2, double beta) {
+  const double z2 = c2 * t * t;
+  return z2 < 1.0 ? exp(beta * (sqrt(1.0 - z2) - 1.0)) : 0.0;
+}
+
+// ---------------------------------------------------------------------------
+// Modes
+// ---------------------------------------------------------------------------
+
+// |q| of mode h in the reference's operation order, without contraction
+// (src/sqc_structure_factor.f90:366-368), so that shells match bit for bit.
+__device__ __forceinline__ double qlen_exact(const BinGeom &b, int h1, int h2, int h3) {
+  double q[3];
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+    q[r] = __dadd_rn(__dadd_rn(__dmul_rn(b.recip[r], (double)h1), __dmul_rn(b.recip[3 + r], (double)h2)),
+                     __dmul_rn(b.recip[6 + r], (double)h3));
+  return __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(q[0], q[0]), __dmul_rn(q[1], q[1])),
+                              __dmul_rn(q[2], q[2])));
+}
+
+// shell = int((|q| - qmin)/dq) clamped to [0, nq)   (:396-399, zero based)
+__device__ __forceinline__ int shell_of(const BinGeom &b, double ql) {
+  int s = (int)__ddiv_rn(__dsub_rn(ql, b.qmin), b.dq);
+  return min(max(s, 0), b.nq - 1);
+}
+
+// Kept test and zero-based shell of mode h, identical to the reference's FP64
+// evaluation (:366-399).  A fast estimate (q from the row constant, |q| in
+// FP32) decides whenever |q| is clear of qmin, qmax and every shell edge by a
+// margin well above its error; otherwise the exact FP64 path runs.  ql returns
+// |q| (FP64, for the x-ray form factors).
+__device__ __forceinline__ bool classify_mode(const BinGeom &b, const double *crow, int h1,
+                                              int h2, int h3, int &s, double &ql) {
+  if (h1 == 0 && h2 == 0 && h3 == 0) return false;
+  const double q0 = fma((double)h1, b.recip[0], crow[0]);
+  const double q1 = fma((double)h1, b.recip[1], crow[1]);
+  const double q2 = fma((double)h1, b.recip[2], crow[2]);
+  const double ql2 = fma(q0, q0, fma(q1, q1, q2 * q2));
+  const float qf = sqrtf((float)ql2);
+  const float tol_q = 4e-7f * qf + 1e-30f;
+  const float t = (qf - b.qminf) * b.invdqf;
+  const float tol_t = 4e-7f * (qf * b.invdqf + 1.0f) + 1e-6f;
+  const bool near = fabsf(qf - b.qmaxf) <= tol_q || fabsf(qf - b.qminf) <= tol_q ||
+                    fabsf(t - rintf(t)) <= tol_t;
+  if (b.xray) ql = sqrt(ql2);
+  if (!near) {
+    if (qf > b.qmaxf || qf < b.qminf) return false;
+    s = min(max((int)t, 0), b.nq - 1);
+    return true;
+  }
+  ql = qlen_exact(b, h1, h2, h3);
+  if (ql > b.qmax || ql < b.qmin) return false;
+  s = shell_of(b, ql);
+  return true;
+}
+
+// Row constant h2 b2 + h3 b3 of the fast |q| estimate.
+__device__ __forceinline__ void row_const(const BinGeom &b, int h2, int h3, double *crow) {
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+    crow[k] = fma((double)h2, b.recip[3 + k], (double)h3 * b.recip[6 + k]);
+}
+
+// IT92 form factor f(q) = sum_i a_i exp(-b_i (q/4pi)^2) + c (src/sqc_elements.f90:226-239).
+__device__ __forceinline__ double xray_f(const double *__restrict__ c, double q) {
+  double st = q / (4.0 * 3.14159265358979323846);
+  st = st * st;
+  double f = c[8];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) f = f + c[i] * exp(-c[4 + i] * st);
+  return f;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+  return v;
+}
+
+// Add v to hist[s]: one atomic per warp when every active lane has the same shell.
+__device__ __forceinline__ void hist_add(double *hist, int s, double v, bool keep, bool uni,
+                                         int s0, int lane) {
+  if (uni) {
+    v = warp_sum(keep ? v : 0.0);
+    if (lane == 0) atomicAdd(&hist[s0], v);
+  } else if (keep) {
+    atomicAdd(&hist[s], v);
+  }
+}
+
+template <typename R> struct Cplx;
+template <> struct Cplx<float> { using T = float2; };
+template <> struct Cplx<double> { using T = double2; };
+
+// The packed word of a point record lives in the low 32 bits of slot 0.
+template <typename R> __device__ __forceinline__ R pack_rec(uint32_t w);
+template <> __device__ __forceinline__ float pack_rec<float>(uint32_t w) {
+  return __uint_as_float(w);
+}
+template <> __device__ __forceinline__ double pack_rec<double>(uint32_t w) {
+  return __longlong_as_double((long long)w);
+}
+template <typename R> __device__ __forceinline__ uint32_t unpack_rec(R v);
+template <> __device__ __forceinline__ uint32_t unpack_rec<float>(float v) {
+  return __float_as_uint(v);
+}
+template <> __device__ __forceinline__ uint32_t unpack_rec<double>(double v) {
+  return (uint32_t)__double_as_longlong(v);
+}
+
+}  // namespace dev
+}  // namespace sqn

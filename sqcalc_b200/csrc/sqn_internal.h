@@ -82,7 +82,7 @@ cudaError_t launch_scan(int *counts, int *starts, int n, cudaStream_t s);
 template <typename R>
 cudaError_t launch_scatter(const double *pos, const uint8_t *species, const FrameGeom &g,
                            const uint32_t *key, const uint32_t *slot, const int *starts,
-                           R *recs, cudaStream_t s);
+                           R *recs, int32_t *orig, cudaStream_t s);
 template <typename R>
 cudaError_t launch_spread(const R *recs, const int *starts, const FrameGeom &g,
                           const R *strength, R *grid, cudaStream_t s);
@@ -97,5 +97,18 @@ cudaError_t launch_norms(const int4 *rows, int nrows, const BinGeom &b, const do
 size_t spread_smem_bytes(int chunk, int stride, bool fp64);
 int spread_chunk(int stride, bool fp64);
 cudaError_t spread_set_attributes();
+
+// Adjoint (sqn_adjoint.cu).
+struct Recip {
+  double b[9];  // b_j = b[3*j + r]
+};
+template <typename R>
+cudaError_t launch_adj_coef(const int4 *rows, int nrows, const void *G, const BinGeom &b,
+                            const R *inv1, const R *inv2, const R *inv3, const double *gsh,
+                            double *num, void *F, int nsm, cudaStream_t s);
+template <typename R>
+cudaError_t launch_interp(const R *recs, const int32_t *orig, const double *pos,
+                          const FrameGeom &g, const R *U, const Recip &rb, const double *camp,
+                          double *grad, cudaStream_t s);
 
 }  // namespace sqn

@@ -27,58 +27,14 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "sqn_device.cuh"
 #include "sqn_internal.h"
 
 namespace sqn {
 
 namespace {
 
-constexpr unsigned FULL = 0xffffffffu;
-
-// ---------------------------------------------------------------------------
-// Atom -> fine grid
-// ---------------------------------------------------------------------------
-
-struct AtomCell {
-  int ix0[3];     // first support cell, wrapped into [0, nf)
-  double off[3];  // (X - ix0) - (w/2 - 1/2), in (-1/2, 1/2]
-};
-
-// s = A^-1 (r - origin), s -= floor(s)  (cell_fractional, src/sqc_cell.f90:143-152,
-// and the wrap of src/sqc_gpu.f90:230-236); X = nf * s is the fine-grid coordinate.
-__device__ __forceinline__ void atom_cell(const double *__restrict__ pos, int64_t i,
-                                          const FrameGeom &g, AtomCell &c) {
-  const double d0 = __dsub_rn(pos[3 * i + 0], g.origin[0]);
-  const double d1 = __dsub_rn(pos[3 * i + 1], g.origin[1]);
-  const double d2 = __dsub_rn(pos[3 * i + 2], g.origin[2]);
-  const double halfw = 0.5 * (double)g.w;
-#pragma unroll
-  for (int r = 0; r < 3; ++r) {
-    double s = __dadd_rn(__dadd_rn(__dmul_rn(g.inv[r], d0), __dmul_rn(g.inv[3 + r], d1)),
-                         __dmul_rn(g.inv[6 + r], d2));
-    s = __dsub_rn(s, floor(s));
-    // A non-finite coordinate must not index outside the grid: park it at 0.
-    if (!(s >= 0.0 && s <= 1.0)) s = 0.0;
-    const double X = __dmul_rn((double)g.nf[r], s);
-    const double start = ceil(__dsub_rn(X, halfw));
-    c.off[r] = __dsub_rn(__dsub_rn(X, start), halfw - 0.5);
-    int ix0 = (int)start;
-    if (ix0 < 0) ix0 += g.nf[r];
-    if (ix0 >= g.nf[r]) ix0 -= g.nf[r];
-    c.ix0[r] = ix0;
-  }
-}
-
-// Home tile of the support start (one bin per tile holds every transform) and
-// the start cell relative to the tile origin.
-__device__ __forceinline__ uint32_t home_key(const AtomCell &c, const FrameGeom &g, int &l0,
-                                             int &l1, int &l2) {
-  const int t0 = c.ix0[0] / g.tile[0], t1 = c.ix0[1] / g.tile[1], t2 = c.ix0[2] / g.tile[2];
-  l0 = c.ix0[0] - t0 * g.tile[0];
-  l1 = c.ix0[1] - t1 * g.tile[1];
-  l2 = c.ix0[2] - t2 * g.tile[2];
-  return (uint32_t)((t2 * g.ntile[1] + t1) * g.ntile[0] + t0);
-}
+using namespace dev;
 
 __global__ void k_prep(const double *__restrict__ pos, FrameGeom g, int *__restrict__ counts,
                        uint32_t *__restrict__ key, uint32_t *__restrict__ slot) {
@@ -131,39 +87,11 @@ __global__ void __launch_bounds__(1024) k_scan(int *__restrict__ counts, int *__
   if (tid == 1023) starts[n] = run;
 }
 
-// ---------------------------------------------------------------------------
-// ES kernel: phi(t) = exp(beta (sqrt(1 - (2t/w)^2) - 1)) on |t| < w/2, else 0
-// (external/finufft/include/cufinufft/spreadinterp.h:84-98).
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ float es_phi(float t, float c2, float beta) {
-  const float z2 = c2 * t * t;
-  return z2 < 1.0f ? expf(beta * (sqrtf(1.0f - z2) - 1.0f)) : 0.0f;
-}
-__device__ __forceinline__ double es_phi(double t, double c2, double beta) {
-  const double z2 = c2 * t * t;
-  return z2 < 1.0 ? exp(beta * (sqrt(1.0 - z2) - 1.0)) : 0.0;
-}
-
-template <typename R> __device__ __forceinline__ R pack_word(uint32_t w);
-template <> __device__ __forceinline__ float pack_word<float>(uint32_t w) {
-  return __uint_as_float(w);
-}
-template <> __device__ __forceinline__ double pack_word<double>(uint32_t w) {
-  return __longlong_as_double((long long)w);
-}
-template <typename R> __device__ __forceinline__ uint32_t unpack_word(R v);
-template <> __device__ __forceinline__ uint32_t unpack_word<float>(float v) {
-  return __float_as_uint(v);
-}
-template <> __device__ __forceinline__ uint32_t unpack_word<double>(double v) {
-  return (uint32_t)__double_as_longlong(v);
-}
-
 template <typename R>
 __global__ void k_scatter(const double *__restrict__ pos, const uint8_t *__restrict__ species,
                           FrameGeom g, const uint32_t *__restrict__ key,
                           const uint32_t *__restrict__ slot, const int *__restrict__ starts,
-                          R *__restrict__ recs) {
+                          R *__restrict__ recs, int32_t *__restrict__ orig) {
   const R halfw = R(0.5) * (R)g.w - R(0.5);
   const R c2 = R(4) / ((R)g.w * (R)g.w);
   const R beta = (R)g.beta;
@@ -174,8 +102,10 @@ __global__ void k_scatter(const double *__restrict__ pos, const uint8_t *__restr
     const int sp = species[i];
     int l0, l1, l2;
     (void)home_key(c, g, l0, l1, l2);
-    R *r = recs + ((int64_t)starts[key[i]] + slot[i]) * g.rec_stride;
-    r[0] = pack_word<R>((uint32_t)l0 | ((uint32_t)l1 << 8) | ((uint32_t)l2 << 16) |
+    const int64_t dst = (int64_t)starts[key[i]] + slot[i];
+    if (orig) orig[dst] = (int32_t)i;
+    R *r = recs + dst * g.rec_stride;
+    r[0] = pack_rec<R>((uint32_t)l0 | ((uint32_t)l1 << 8) | ((uint32_t)l2 << 16) |
                         ((uint32_t)sp << 24));
     // The separable kernel values of the w support cells along each axis,
     // evaluated once per atom (the spread reuses them for every tile).
@@ -299,7 +229,7 @@ __global__ void __launch_bounds__(SPREAD_THREADS, (sizeof(R) == 4 || NT == 1) ? 
       int b = 0;
       while (i >= s_bpref[b + 1]) ++b;
       ridx = s_bstart[b] + (i - s_bpref[b]);
-      const uint32_t packed = unpack_word<R>(recs[(int64_t)ridx * stride]);
+      const uint32_t packed = unpack_rec<R>(recs[(int64_t)ridx * stride]);
       int rx = s_borg[b][0] + (int)(packed & 255u) - X0;
       int ry = s_borg[b][1] + (int)((packed >> 8) & 255u) - Y0;
       int rz = s_borg[b][2] + (int)((packed >> 16) & 255u) - Z0;
@@ -426,89 +356,6 @@ __global__ void __launch_bounds__(SPREAD_THREADS, (sizeof(R) == 4 || NT == 1) ? 
     }
   }
 }
-
-// ---------------------------------------------------------------------------
-// Mode bookkeeping shared by the bin and norm kernels.
-// ---------------------------------------------------------------------------
-
-// |q| of mode h in the reference's operation order, without contraction
-// (src/sqc_structure_factor.f90:366-368), so that shells match bit for bit.
-__device__ __forceinline__ double qlen_exact(const BinGeom &b, int h1, int h2, int h3) {
-  double q[3];
-#pragma unroll
-  for (int r = 0; r < 3; ++r)
-    q[r] = __dadd_rn(__dadd_rn(__dmul_rn(b.recip[r], (double)h1), __dmul_rn(b.recip[3 + r], (double)h2)),
-                     __dmul_rn(b.recip[6 + r], (double)h3));
-  return __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(q[0], q[0]), __dmul_rn(q[1], q[1])),
-                              __dmul_rn(q[2], q[2])));
-}
-
-// shell = int((|q| - qmin)/dq) clamped to [0, nq)   (:396-399, zero based)
-__device__ __forceinline__ int shell_of(const BinGeom &b, double ql) {
-  int s = (int)__ddiv_rn(__dsub_rn(ql, b.qmin), b.dq);
-  return min(max(s, 0), b.nq - 1);
-}
-
-// Kept test and zero-based shell of mode h, identical to the reference's FP64
-// evaluation (:366-399).  A fast estimate (q from the row constant, |q| in
-// FP32) decides whenever |q| is clear of qmin, qmax and every shell edge by a
-// margin well above its error; otherwise the exact FP64 path runs.  ql returns
-// |q| (FP64, for the x-ray form factors).
-__device__ __forceinline__ bool classify_mode(const BinGeom &b, const double *crow, int h1,
-                                              int h2, int h3, int &s, double &ql) {
-  if (h1 == 0 && h2 == 0 && h3 == 0) return false;
-  const double q0 = fma((double)h1, b.recip[0], crow[0]);
-  const double q1 = fma((double)h1, b.recip[1], crow[1]);
-  const double q2 = fma((double)h1, b.recip[2], crow[2]);
-  const double ql2 = fma(q0, q0, fma(q1, q1, q2 * q2));
-  const float qf = sqrtf((float)ql2);
-  const float tol_q = 4e-7f * qf + 1e-30f;
-  const float t = (qf - b.qminf) * b.invdqf;
-  const float tol_t = 4e-7f * (qf * b.invdqf + 1.0f) + 1e-6f;
-  const bool near = fabsf(qf - b.qmaxf) <= tol_q || fabsf(qf - b.qminf) <= tol_q ||
-                    fabsf(t - rintf(t)) <= tol_t;
-  if (b.xray) ql = sqrt(ql2);
-  if (!near) {
-    if (qf > b.qmaxf || qf < b.qminf) return false;
-    s = min(max((int)t, 0), b.nq - 1);
-    return true;
-  }
-  ql = qlen_exact(b, h1, h2, h3);
-  if (ql > b.qmax || ql < b.qmin) return false;
-  s = shell_of(b, ql);
-  return true;
-}
-
-// IT92 form factor f(q) = sum_i a_i exp(-b_i (q/4pi)^2) + c (src/sqc_elements.f90:226-239).
-__device__ __forceinline__ double xray_f(const double *__restrict__ c, double q) {
-  double st = q / (4.0 * 3.14159265358979323846);
-  st = st * st;
-  double f = c[8];
-#pragma unroll
-  for (int i = 0; i < 4; ++i) f = f + c[i] * exp(-c[4 + i] * st);
-  return f;
-}
-
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
-  return v;
-}
-
-// Add v to hist[s]: one atomic per warp when every active lane has the same shell.
-__device__ __forceinline__ void hist_add(double *hist, int s, double v, bool keep, bool uni,
-                                         int s0, int lane) {
-  if (uni) {
-    v = warp_sum(keep ? v : 0.0);
-    if (lane == 0) atomicAdd(&hist[s0], v);
-  } else if (keep) {
-    atomicAdd(&hist[s], v);
-  }
-}
-
-template <typename R> struct Cplx;
-template <> struct Cplx<float> { using T = float2; };
-template <> struct Cplx<double> { using T = double2; };
 
 // ---------------------------------------------------------------------------
 // Fused deconvolve + weighted total + pair products + FP64 shell binning.
@@ -689,8 +536,9 @@ cudaError_t launch_scan(int *counts, int *starts, int n, cudaStream_t s) {
 template <typename R>
 cudaError_t launch_scatter(const double *pos, const uint8_t *species, const FrameGeom &g,
                            const uint32_t *key, const uint32_t *slot, const int *starts,
-                           R *recs, cudaStream_t s) {
-  k_scatter<R><<<grid_for(g.natoms, 256), 256, 0, s>>>(pos, species, g, key, slot, starts, recs);
+                           R *recs, int32_t *orig, cudaStream_t s) {
+  k_scatter<R><<<grid_for(g.natoms, 256), 256, 0, s>>>(pos, species, g, key, slot, starts, recs,
+                                                       orig);
   return cudaGetLastError();
 }
 
@@ -820,10 +668,10 @@ template cudaError_t launch_prep<double>(const double *, const uint8_t *, const 
                                          uint32_t *, uint32_t *, cudaStream_t);
 template cudaError_t launch_scatter<float>(const double *, const uint8_t *, const FrameGeom &,
                                            const uint32_t *, const uint32_t *, const int *,
-                                           float *, cudaStream_t);
+                                           float *, int32_t *, cudaStream_t);
 template cudaError_t launch_scatter<double>(const double *, const uint8_t *, const FrameGeom &,
                                             const uint32_t *, const uint32_t *, const int *,
-                                            double *, cudaStream_t);
+                                            double *, int32_t *, cudaStream_t);
 template cudaError_t launch_spread<float>(const float *, const int *, const FrameGeom &,
                                           const float *, float *, cudaStream_t);
 template cudaError_t launch_spread<double>(const double *, const int *, const FrameGeom &,

@@ -162,7 +162,7 @@ extern "C" int sqn_spread_frame_noalloc(const double *pos, int64_t natoms,
     e = cudaMemcpyAsync(d_strength, strength, sizeof(float) * (size_t)ntr, cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) e = launch_prep<float>(pos, d_species, g, counts, key, slot, s);
   if (e == cudaSuccess) e = launch_scan(counts, starts, (int)nkeys, s);
-  if (e == cudaSuccess) e = launch_scatter<float>(pos, d_species, g, key, slot, starts, recs, s);
+  if (e == cudaSuccess) e = launch_scatter<float>(pos, d_species, g, key, slot, starts, recs, nullptr, s);
   if (e == cudaSuccess) e = launch_spread<float>(recs, starts, g, d_strength, grid, s);
   if (e != cudaSuccess) {
     cudaGetLastError();
