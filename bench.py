@@ -211,6 +211,111 @@ def cpu_baseline_sample():
                       "%d threads, %.1f s" % (cores, dt)}
 
 
+def _max_over_ranks(x, dist, local_rank):
+    if not dist:
+        return x
+    import torch
+    import torch.distributed as td
+    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local_rank}")
+    td.all_reduce(t, op=td.ReduceOp.MAX)
+    return float(t.item())
+
+
+def precision_leg(types, dev, base, fbytes, W, K, stream, dist, world, local_rank):
+    """The plain FP64 path (same tolerance) on the same device-resident frames,
+    and max |dS| of the FP32 path against FP64 at eps 1e-12 on two frames."""
+    import torch
+    from sqcalc_b200 import _lib
+
+    def plan(prec, eps):
+        return _lib.Plan(np.eye(3).reshape(9) * BOX, np.zeros(3), types,
+                         weight=_lib.WEIGHT_NEUTRON, amp_const=np.array(B_NEUTRON), qmin=0.0,
+                         qmax=QMAX, nq=NQ, norm=_lib.NORM_MEAN, partials=True, precision=prec,
+                         eps=eps, device=local_rank, stream=stream.cuda_stream)
+
+    k = min(K, 10)
+    p = plan(_lib.PREC_DOUBLE, EPS)
+    for f in range(W):
+        p.accumulate((base + f * fbytes, 1), where=_lib.DEVICE)
+    p.sync()
+    if dist:
+        import torch.distributed as td
+        td.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for f in range(W, W + k):
+        p.accumulate((base + f * fbytes, 1), where=_lib.DEVICE)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    t = _max_over_ranks(ev0.elapsed_time(ev1) * 1e-3, dist, local_rank)
+    fp64 = {"value": k * world / t, "unit": UNIT, "steps": k, "ms_per_step": 1e3 * t / k,
+            "eps": EPS, "upsampfac": p.info.upsampfac, "kernel_width": p.info.kernel_width,
+            "fine_grid": list(p.info.nf)}
+    p.close()
+    res = {}
+    for name, prec, eps in (("fp32", _lib.PREC_SINGLE, EPS), ("fp64_ref", _lib.PREC_DOUBLE, 1e-12)):
+        q = plan(prec, eps)
+        for f in range(2):
+            q.accumulate((base + f * fbytes, 1), where=_lib.DEVICE)
+        s, sp, _, _ = q.finalize()
+        res[name] = (s, sp)
+        q.close()
+    fp64["max_abs_dS_fp32"] = float(np.max(np.abs(res["fp32"][0] - res["fp64_ref"][0])))
+    fp64["max_abs_dS_partials_fp32"] = float(np.max(np.abs(res["fp32"][1] - res["fp64_ref"][1])))
+    fp64["dS_reference"] = "FP64 NUFFT at eps 1e-12 on the same 2 frames"
+    return fp64
+
+
+GRAD_N, GRAD_BOX, GRAD_QMIN, GRAD_QMAX, GRAD_NQ = 100_000, 100.0, 0.5, 8.0, 375
+
+
+def grad_leg(W, K, stream, dist, local_rank):
+    """dS/dr evaluations/s on the differentiation form: cubic L = 100 A,
+    N = 1e5, 2 types 1:2, loss sum_shells (S - S_target)^2 over q in [0.5, 8],
+    S_target from a copy displaced by N(0, 0.2^2).  One evaluation = one
+    sqn_sq_grad call with dL/dS: the weighted forward transform recomputed,
+    three type-2 interpolations, S and the FP64 gradient returned."""
+    import torch
+    from sqcalc_b200 import _lib
+
+    rng = np.random.default_rng(SEED + 4)
+    types = np.repeat([1, 2], [GRAD_N // 3, GRAD_N - GRAD_N // 3]).astype(np.int32)
+    rng.shuffle(types)
+    pos = rng.random((GRAD_N, 3)) * GRAD_BOX
+    target_pos = pos + rng.normal(0.0, 0.2, pos.shape)
+    d = torch.from_numpy(pos).to(f"cuda:{local_rank}")
+    out = {"metric": "dS/dr evals/s", "unit": "evals/s",
+           "config": {"workload": "differentiation form: cubic L=100 A, N=1e5, 2 types 1:2, "
+                                  "uniform, loss over q in [0.5,8], S_target from a copy "
+                                  "displaced by N(0,0.2^2)", "nq": GRAD_NQ}}
+    k = min(K, 20)
+    for name, prec, eps in (("f32+f64acc", _lib.PREC_SINGLE, 1e-6), ("f64", _lib.PREC_DOUBLE, 1e-10)):
+        with _lib.Plan(np.eye(3).reshape(9) * GRAD_BOX, np.zeros(3), types, qmin=GRAD_QMIN,
+                       qmax=GRAD_QMAX, nq=GRAD_NQ, partials=False, precision=prec, eps=eps,
+                       device=local_rank, stream=stream.cuda_stream, grad=True) as p:
+            S_t, _ = p.sq_grad(target_pos)
+            S, _ = p.sq_grad(d)
+            dLdS = 2.0 * (S - S_t)
+            for _ in range(W):
+                p.sq_grad(d, dLdS)
+            torch.cuda.synchronize()
+            l0 = p.launch_count()
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record(stream)
+            for _ in range(k):
+                p.sq_grad(d, dLdS)
+            ev1.record(stream)
+            torch.cuda.synchronize()
+            t = _max_over_ranks(ev0.elapsed_time(ev1) * 1e-3, dist, local_rank)
+            out[name] = {"value": k / t, "ms_per_eval": 1e3 * t / k, "eps": eps, "steps": k,
+                         "modes": list(p.modes), "fine_grid": list(p.info.nf),
+                         "kernel_width": p.info.kernel_width,
+                         "gpu_launches_per_eval": (p.launch_count() - l0) / k}
+    out["value"] = out["f32+f64acc"]["value"]
+    return out
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     from sqcalc_b200 import _lib, build
@@ -309,6 +414,12 @@ def run_ours(args, rank, world, local_rank):
     e2e_value = K * world / e2e_t
     e2e_plan.close()
 
+    # --- the plain FP64 path on the same frames, and max |dS| of FP32 ----------
+    fp64 = precision_leg(types, dev, base, fbytes, W, K, stream, dist, world, local_rank)
+
+    # --- dS/dr evaluations (differentiation form) -------------------------------
+    grad = None if args.no_grad else grad_leg(W, K, stream, dist, local_rank)
+
     # --- sharded frames: sum the accumulators once ------------------------------
     if dist:
         acc = plan.accumulators()
@@ -357,6 +468,8 @@ def run_ours(args, rank, world, local_rank):
             "gpu_launches": launches,
             "gpu_launches_note": "own kernels (prep, scan, scatter, spread, bin) per frame; "
                                  "cuFFT kernels not counted",
+            "fp64": fp64,
+            "grad": grad,
             "clocks": clk.summary(),
             "wall_s": t_wall,
         }
@@ -377,6 +490,7 @@ def main():
     ap.add_argument("--precision", default="single", choices=["single", "double"])
     ap.add_argument("--upsampfac", type=float, default=0.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-grad", action="store_true", help="skip the dS/dr leg")
     ap.add_argument("--scale", type=float, default=1.0,
                     help="shrink the box by this factor at fixed density (profiling only)")
     args = ap.parse_args()

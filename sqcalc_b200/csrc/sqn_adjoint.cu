@@ -90,8 +90,10 @@ __global__ void __launch_bounds__(256, 2)
 }
 
 // One warp per atom in bin-sorted order: U_i(s_j) by ES interpolation of the
-// three real grids, then dL/dr_j = 2 c_j sum_i b_i U_i.  Lanes take (dy, dz)
-// pairs of the support; each walks its x row.
+// three real grids, then dL/dr_j = 2 c_j sum_i b_i U_i.  Lanes 0..w-1 evaluate
+// the kernel values of the support along each axis (the same expression as
+// the spread); lanes then take (dy, dz) pairs of the support and walk the x
+// row, the values broadcast by shuffles.
 template <typename R>
 __global__ void __launch_bounds__(256)
     k_interp(const R *__restrict__ recs, const int32_t *__restrict__ orig,
@@ -100,35 +102,48 @@ __global__ void __launch_bounds__(256)
   const int lane = threadIdx.x & 31;
   const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
   const int w = g.w, ww = w * w;
+  const R halfw = R(0.5) * (R)w - R(0.5);
+  const R c2 = R(4) / ((R)w * (R)w);
+  const R beta = (R)g.beta;
   for (int64_t p = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); p < g.natoms;
        p += nwarps) {
     const int j = orig[p];
     AtomCell c;
     atom_cell(pos, j, g, c);
-    const R *rec = recs + p * g.rec_stride;
+    R rec[REC_SLOTS];
+    load_rec(recs + p * REC_SLOTS, rec);
     const int sp = (int)(unpack_rec<R>(rec[0]) >> 24);
-    const R *kx = rec + 1, *ky = rec + 1 + w, *kz = rec + 1 + 2 * w;
+    const int kl = lane < w ? lane : 0;
+    const R kxl = es_at(kl, rec[1], halfw, c2, beta);
+    const R kyl = es_at(kl, rec[2], halfw, c2, beta);
+    const R kzl = es_at(kl, rec[3], halfw, c2, beta);
     double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-    for (int idx = lane; idx < ww; idx += 32) {
-      const int dz = idx / w, dy = idx - dz * w;
+    for (int base = 0; base < ww; base += 32) {
+      const int idx = base + lane;
+      const bool act = idx < ww;
+      const int dz = act ? idx / w : 0, dy = act ? idx - dz * w : 0;
       int iy = c.ix0[1] + dy;
       if (iy >= g.nf[1]) iy -= g.nf[1];
       int iz = c.ix0[2] + dz;
       if (iz >= g.nf[2]) iz -= g.nf[2];
       const int64_t rowoff = ((int64_t)iz * g.nf[1] + iy) * g.pitch;
+      const R wyz = __shfl_sync(FULL, kyl, dy) * __shfl_sync(FULL, kzl, dz);
       R u0 = 0, u1 = 0, u2 = 0;
       for (int dx = 0; dx < w; ++dx) {
         int ix = c.ix0[0] + dx;
         if (ix >= g.nf[0]) ix -= g.nf[0];
-        const R k = kx[dx];
-        u0 += k * U[rowoff + ix];
-        u1 += k * U[g.vol_real + rowoff + ix];
-        u2 += k * U[2 * g.vol_real + rowoff + ix];
+        const R k = __shfl_sync(FULL, kxl, dx);
+        if (act) {
+          u0 += k * U[rowoff + ix];
+          u1 += k * U[g.vol_real + rowoff + ix];
+          u2 += k * U[2 * g.vol_real + rowoff + ix];
+        }
       }
-      const double wyz = (double)(ky[dy] * kz[dz]);
-      a0 += wyz * (double)u0;
-      a1 += wyz * (double)u1;
-      a2 += wyz * (double)u2;
+      if (act) {
+        a0 += (double)wyz * (double)u0;
+        a1 += (double)wyz * (double)u1;
+        a2 += (double)wyz * (double)u2;
+      }
     }
     a0 = warp_sum(a0);
     a1 = warp_sum(a1);

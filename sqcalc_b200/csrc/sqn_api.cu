@@ -477,7 +477,7 @@ int setup_plan(sqn_plan *p, const sqn_plan_desc *d) {
   g.vol_real = p->nf[0] * p->nf[1] * p->nf[2];
   g.natoms = d->natoms;
   g.rec_stride = rec_stride(w, p->fp64);
-  g.chunk = spread_chunk(g.rec_stride, p->fp64);
+  g.chunk = spread_chunk(p->fp64, p->ntr);
   if ((int64_t)g.ntiles * p->ntr >= INT32_MAX) return SQN_ERR_NOT_SUPPORTED;
   p->nkeys = g.ntiles;  // one bin per tile; records carry their species
 
@@ -691,6 +691,7 @@ template <typename R> int grad_frame(sqn_plan *p, const double *dpos, bool want_
   cudaStream_t s = p->stream;
   FrameGeom g = p->fg;
   g.ntr = 1;  // the total T(h) = sum_j c_j exp(i q.r_j): one weighted transform
+  g.chunk = spread_chunk(p->fp64, 1);
   BinGeom b = p->bg;
   b.ntr = 1;
   b.partials = 0;

@@ -174,5 +174,30 @@ template <> __device__ __forceinline__ uint32_t unpack_rec<double>(double v) {
   return (uint32_t)__double_as_longlong(v);
 }
 
+// Whole point records (REC_SLOTS = 4 values, 16- or 32-byte aligned).
+__device__ __forceinline__ void store_rec(float *r, float a, float b, float c, float d) {
+  *reinterpret_cast<float4 *>(r) = make_float4(a, b, c, d);
+}
+__device__ __forceinline__ void store_rec(double *r, double a, double b, double c, double d) {
+  reinterpret_cast<double2 *>(r)[0] = make_double2(a, b);
+  reinterpret_cast<double2 *>(r)[1] = make_double2(c, d);
+}
+__device__ __forceinline__ void load_rec(const float *r, float (&v)[4]) {
+  const float4 a = *reinterpret_cast<const float4 *>(r);
+  v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+}
+__device__ __forceinline__ void load_rec(const double *r, double (&v)[4]) {
+  const double2 a = reinterpret_cast<const double2 *>(r)[0];
+  const double2 b = reinterpret_cast<const double2 *>(r)[1];
+  v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+
+// ES kernel value at support cell k (0 <= k < w) of an atom whose record
+// offset along the axis is off.
+template <typename R>
+__device__ __forceinline__ R es_at(int k, R off, R halfw, R c2, R beta) {
+  return es_phi(((R)k - halfw) - off, c2, beta);
+}
+
 }  // namespace dev
 }  // namespace sqn

@@ -17,24 +17,26 @@ constexpr int PATCH_X = 8;
 constexpr int PATCH_Y = 4;
 constexpr int SPREAD_WARPS = (TILE_X / PATCH_X) * (TILE_Y / PATCH_Y);  // 16
 constexpr int SPREAD_THREADS = 32 * SPREAD_WARPS;                       // 512
+constexpr int SPREAD_ROW = TILE_X + TILE_Y + TILE_Z;                    // staged values per point
+static_assert((TILE_X & (TILE_X - 1)) == 0 && (TILE_Y & (TILE_Y - 1)) == 0 &&
+                  (TILE_Z & (TILE_Z - 1)) == 0,
+              "tile extents are powers of two");
 constexpr int MAX_W = 16;
 constexpr int MAX_BINS_DIM = 4;                // bins per dim a tile may need (w <= 16)
 constexpr int MAX_NB = 64;                     // neighbour bins of a tile
 constexpr int MAX_FAST_T = 8;                  // species held in registers
 
-// Point records written by the bin sort and read by the spread kernel: one
-// record of rec_stride R-sized slots per atom:
-//   slot 0            packed word: bits 0-7 / 8-15 / 16-23 first support cell
-//                     relative to the home tile origin in x / y / z, bits 24-31
-//                     species index (stored in the slot's low 32 bits)
-//   slots 1 .. 3w     ES kernel values phi(k - (X_d - ix0_d)), k = 0..w-1, for
-//                     x, then y, then z
-// The stride is a multiple of 32 bytes (one DRAM sector).
-inline int rec_stride(int w, bool fp64) {
-  const int n = 3 * w + 1;
-  const int q = fp64 ? 4 : 8;
-  return (n + q - 1) / q * q;
-}
+// Point records written by the bin sort and read by the spread and
+// interpolation kernels: four R-sized slots per atom,
+//   slot 0     packed word: bits 0-7 / 8-15 / 16-23 first support cell relative
+//              to the home tile origin in x / y / z, bits 24-31 species index
+//              (stored in the slot's low 32 bits)
+//   slots 1-3  off_d = (X_d - ix0_d) - (w/2 - 1/2), the offset of the atom from
+//              the centre of its support along each axis, in R precision; the ES
+//              kernel value at support cell k is phi((k - (w/2 - 1/2)) - off_d)
+// 16 bytes per atom in FP32, 32 in FP64 (one vector load each).
+constexpr int REC_SLOTS = 4;
+inline int rec_stride(int, bool) { return REC_SLOTS; }
 
 // Geometry and kernel parameters, passed by value to the per-frame kernels.
 struct FrameGeom {
@@ -94,8 +96,8 @@ cudaError_t launch_bin(const int4 *rows, int nrows, const void *G, const BinGeom
 cudaError_t launch_norms(const int4 *rows, int nrows, const BinGeom &b, const double *amp,
                          const double *xcoef, const double *counts_t, double *den,
                          double *cnt, int nsm, cudaStream_t s);
-size_t spread_smem_bytes(int chunk, int stride, bool fp64);
-int spread_chunk(int stride, bool fp64);
+size_t spread_smem_bytes(int chunk, bool fp64);
+int spread_chunk(bool fp64, int ntr);
 cudaError_t spread_set_attributes();
 
 // Adjoint (sqn_adjoint.cu).

@@ -5,11 +5,12 @@
 //              kernel support on the fine grid and its home tile; count the
 //              tile's bin                                        [HBM: positions]
 //   k_scan     exclusive scan of the bin counts (one CTA) and reset the counts
-//   k_scatter  write each atom's record into its bin slot: packed start cell +
-//              species and the 3w separable kernel values, evaluated once
+//   k_scatter  write each atom's 16-byte record into its bin slot: packed start
+//              cell + species and its three offsets from the support centre
 //   k_spread   gather spreading: one CTA owns one 32 x 16 x 8 fine-grid tile
-//              for every transform, stages the records of the bins that can
-//              reach it in shared memory, and each warp accumulates its 8 x 4
+//              for every transform, stages the ES kernel values of the points
+//              of the bins that can reach it, already shifted onto the tile's
+//              cells, in shared memory, and each warp accumulates its 8 x 4
 //              patch (8 z-cells per lane, per transform) in registers from the
 //              points that reach the patch; every cell is written exactly
 //              once, so the grid needs no zeroing and no atomics
@@ -92,9 +93,6 @@ __global__ void k_scatter(const double *__restrict__ pos, const uint8_t *__restr
                           FrameGeom g, const uint32_t *__restrict__ key,
                           const uint32_t *__restrict__ slot, const int *__restrict__ starts,
                           R *__restrict__ recs, int32_t *__restrict__ orig) {
-  const R halfw = R(0.5) * (R)g.w - R(0.5);
-  const R c2 = R(4) / ((R)g.w * (R)g.w);
-  const R beta = (R)g.beta;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < g.natoms;
        i += (int64_t)gridDim.x * blockDim.x) {
     AtomCell c;
@@ -104,16 +102,26 @@ __global__ void k_scatter(const double *__restrict__ pos, const uint8_t *__restr
     (void)home_key(c, g, l0, l1, l2);
     const int64_t dst = (int64_t)starts[key[i]] + slot[i];
     if (orig) orig[dst] = (int32_t)i;
-    R *r = recs + dst * g.rec_stride;
-    r[0] = pack_rec<R>((uint32_t)l0 | ((uint32_t)l1 << 8) | ((uint32_t)l2 << 16) |
-                        ((uint32_t)sp << 24));
-    // The separable kernel values of the w support cells along each axis,
-    // evaluated once per atom (the spread reuses them for every tile).
+    store_rec(recs + dst * REC_SLOTS,
+              pack_rec<R>((uint32_t)l0 | ((uint32_t)l1 << 8) | ((uint32_t)l2 << 16) |
+                          ((uint32_t)sp << 24)),
+              (R)c.off[0], (R)c.off[1], (R)c.off[2]);
+  }
+}
+
+// The 8 z values of a staged row (16-byte aligned) with vector loads.
+__device__ __forceinline__ void load_zrow(const float *src, float (&z)[TILE_Z]) {
+  const float4 a = reinterpret_cast<const float4 *>(src)[0];
+  const float4 b = reinterpret_cast<const float4 *>(src)[1];
+  z[0] = a.x; z[1] = a.y; z[2] = a.z; z[3] = a.w;
+  z[4] = b.x; z[5] = b.y; z[6] = b.z; z[7] = b.w;
+}
+__device__ __forceinline__ void load_zrow(const double *src, double (&z)[TILE_Z]) {
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      const R off = (R)c.off[d];
-      for (int k = 0; k < g.w; ++k) r[1 + d * g.w + k] = es_phi(((R)k - halfw) - off, c2, beta);
-    }
+  for (int k = 0; k < TILE_Z / 2; ++k) {
+    const double2 v = reinterpret_cast<const double2 *>(src)[k];
+    z[2 * k] = v.x;
+    z[2 * k + 1] = v.y;
   }
 }
 
@@ -130,22 +138,24 @@ __device__ __forceinline__ bool cyc_meet(int r, int w, int b, int len, int n) {
 // ---------------------------------------------------------------------------
 // Gather spreading, one CTA per 32 x 16 x 8 tile for all transforms.
 // NT > 0: exactly NT transforms; NT == 0: any ntr <= MAX_FAST_T.
-// Shared memory per staged point: its record (kernel values), its shifted z
-// row (strength folded in), (rx, ry, rz, species) relative to the tile, the
-// mask of the 8 x 4 patches it reaches, and its record index.
+// Shared memory per staged point: its kernel values already shifted onto the
+// tile's cells (32 x, 16 y, 8 z with the strength folded in; zero where the
+// support does not reach), its three support offsets, (rx, ry, rz, species)
+// relative to the tile and the mask of the 8 x 4 patches it reaches.  A warp's visit
+// of a point is then two scalar loads, a multiply, two vector loads and eight
+// FMAs per lane.
 // ---------------------------------------------------------------------------
 template <typename R, int NT>
 __global__ void __launch_bounds__(SPREAD_THREADS, (sizeof(R) == 4 || NT == 1) ? 2 : 1)
     k_spread(const R *__restrict__ recs, const int *__restrict__ starts, FrameGeom g,
              const R *__restrict__ strength, R *__restrict__ grid) {
   constexpr int TM = NT > 0 ? NT : MAX_FAST_T;
-  const int chunk = g.chunk, stride = g.rec_stride;
+  const int chunk = g.chunk;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  R *s_vals = reinterpret_cast<R *>(smem_raw);                        // [chunk][stride]
-  R *s_zrow = s_vals + (size_t)chunk * stride;                        // [chunk][TILE_Z]
-  int4 *s_meta = reinterpret_cast<int4 *>(s_zrow + (size_t)chunk * TILE_Z);  // [chunk]
-  int *s_rec = reinterpret_cast<int *>(s_meta + chunk);               // [chunk]
-  unsigned *s_mask = reinterpret_cast<unsigned *>(s_rec + chunk);     // [chunk]
+  R *s_rows = reinterpret_cast<R *>(smem_raw);                        // [chunk][SPREAD_ROW]
+  R *s_off = s_rows + (size_t)chunk * SPREAD_ROW;                      // [chunk][4]
+  int4 *s_meta = reinterpret_cast<int4 *>(s_off + (size_t)chunk * 4);  // [chunk]
+  unsigned *s_mask = reinterpret_cast<unsigned *>(s_meta + chunk);     // [chunk]
   __shared__ int s_bstart[MAX_NB];
   __shared__ int s_bpref[MAX_NB + 1];
   __shared__ int s_borg[MAX_NB][3];
@@ -192,21 +202,37 @@ __global__ void __launch_bounds__(SPREAD_THREADS, (sizeof(R) == 4 || NT == 1) ? 
   __syncthreads();
   const int nb0 = s_nbl[0], nb1 = s_nbl[1];
   const int nb = nb0 * nb1 * s_nbl[2];
-  if (tid < nb) {
-    const int bx = s_bl[0][tid % nb0], by = s_bl[1][(tid / nb0) % nb1],
-              bz = s_bl[2][tid / (nb0 * nb1)];
-    const int key = (bz * g.ntile[1] + by) * g.ntile[0] + bx;
-    const int st = starts[key];
-    s_bstart[tid] = st;
-    s_bpref[tid + 1] = starts[key + 1] - st;
-    s_borg[tid][0] = bx * g.tile[0];
-    s_borg[tid][1] = by * g.tile[1];
-    s_borg[tid][2] = bz * g.tile[2];
-  }
-  __syncthreads();
-  if (tid == 0) {
-    s_bpref[0] = 0;
-    for (int b = 0; b < nb; ++b) s_bpref[b + 1] += s_bpref[b];
+  if (warp == 0) {
+    // two bins per lane (nb <= MAX_NB = 64), inclusive prefix by shuffles
+    int cnt2[2];
+    int sum = 0;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int b = 2 * lane + h;
+      cnt2[h] = 0;
+      if (b < nb) {
+        const int bx = s_bl[0][b % nb0], by = s_bl[1][(b / nb0) % nb1],
+                  bz = s_bl[2][b / (nb0 * nb1)];
+        const int key = (bz * g.ntile[1] + by) * g.ntile[0] + bx;
+        const int st = starts[key];
+        cnt2[h] = starts[key + 1] - st;
+        s_bstart[b] = st;
+        s_borg[b][0] = bx * g.tile[0];
+        s_borg[b][1] = by * g.tile[1];
+        s_borg[b][2] = bz * g.tile[2];
+      }
+      sum += cnt2[h];
+    }
+    int incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(FULL, incl, o);
+      if (lane >= o) incl += t;
+    }
+    const int excl = incl - sum;
+    if (2 * lane < nb + 1) s_bpref[2 * lane] = excl;
+    if (2 * lane + 1 < nb + 1) s_bpref[2 * lane + 1] = excl + cnt2[0];
+    if (lane == 31 && nb == MAX_NB) s_bpref[MAX_NB] = incl;
   }
   __syncthreads();
   const int total = s_bpref[nb];
@@ -217,19 +243,22 @@ __global__ void __launch_bounds__(SPREAD_THREADS, (sizeof(R) == 4 || NT == 1) ? 
 #pragma unroll
     for (int z = 0; z < TILE_Z; ++z) acc[t][z] = R(0);
   const unsigned xbit = 1u << (warp & 3), ybit = 1u << (4 + (warp >> 2));
-  const int units = stride * (int)sizeof(R) / 16;  // 16-byte units per record
+  const R halfw = R(0.5) * (R)w - R(0.5);
+  const R c2 = R(4) / ((R)w * (R)w);
+  const R beta = (R)g.beta;
 
   for (int base = 0; base < total; base += chunk) {
     // 1. candidates that overlap the tile, compacted (order kept)
     const int i = base + tid;
     bool keep = false;
     int4 meta = make_int4(0, 0, 0, 0);
-    int ridx = 0;
+    R rec[REC_SLOTS];
     if (tid < chunk && i < total) {
       int b = 0;
       while (i >= s_bpref[b + 1]) ++b;
-      ridx = s_bstart[b] + (i - s_bpref[b]);
-      const uint32_t packed = unpack_rec<R>(recs[(int64_t)ridx * stride]);
+      const int ridx = s_bstart[b] + (i - s_bpref[b]);
+      load_rec(recs + (int64_t)ridx * REC_SLOTS, rec);
+      const uint32_t packed = unpack_rec<R>(rec[0]);
       int rx = s_borg[b][0] + (int)(packed & 255u) - X0;
       int ry = s_borg[b][1] + (int)((packed >> 8) & 255u) - Y0;
       int rz = s_borg[b][2] + (int)((packed >> 16) & 255u) - Z0;
@@ -270,47 +299,50 @@ __global__ void __launch_bounds__(SPREAD_THREADS, (sizeof(R) == 4 || NT == 1) ? 
       for (int t = 0; t < TM; ++t)
         if (t == my_t) p += tstart[t];
       for (int k = 0; k < warp; ++k) p += s_wcount[my_t * SPREAD_WARPS + k];
-      s_meta[p] = meta;
-      s_rec[p] = ridx;
-    }
-    __syncthreads();
-
-    // 2. copy the kept records into shared memory (16-byte vector loads)
-    {
-      const float4 *src = reinterpret_cast<const float4 *>(recs);
-      float4 *dst = reinterpret_cast<float4 *>(s_vals);
-      for (int e = tid; e < npts * units; e += SPREAD_THREADS) {
-        const int p = e / units, u = e - p * units;
-        dst[e] = src[(int64_t)s_rec[p] * units + u];
-      }
-    }
-    __syncthreads();
-
-    // 3. per point: the patches it reaches and its z row shifted into the tile
-    for (int p = tid; p < npts; p += SPREAD_THREADS) {
-      const int4 m = s_meta[p];
+      // the 8 x 4 patches of the tile this point reaches
       unsigned mask = 0u;
 #pragma unroll
       for (int k = 0; k < TILE_X / PATCH_X; ++k)
-        if (cyc_meet(m.x, w, k * PATCH_X, min(PATCH_X, tx - k * PATCH_X), g.nf[0]))
+        if (cyc_meet(meta.x, w, k * PATCH_X, min(PATCH_X, tx - k * PATCH_X), g.nf[0]))
           mask |= 1u << k;
 #pragma unroll
       for (int k = 0; k < TILE_Y / PATCH_Y; ++k)
-        if (cyc_meet(m.y, w, k * PATCH_Y, min(PATCH_Y, ty - k * PATCH_Y), g.nf[1]))
+        if (cyc_meet(meta.y, w, k * PATCH_Y, min(PATCH_Y, ty - k * PATCH_Y), g.nf[1]))
           mask |= 1u << (4 + k);
+      s_meta[p] = meta;
       s_mask[p] = mask;
-      const R *v = s_vals + (size_t)p * stride + 1 + 2 * w;
-      const R sw = strength[m.w];
-#pragma unroll
-      for (int z = 0; z < TILE_Z; ++z) {
-        int k = z - m.z;
-        if (k < 0) k += g.nf[2];
-        s_zrow[p * TILE_Z + z] = (z < tz && k < w) ? v[k] * sw : R(0);
+      store_rec(s_off + (size_t)p * 4, R(0), rec[1], rec[2], rec[3]);
+    }
+    __syncthreads();
+
+    // 2. kernel values shifted onto the tile's cells: row c of point p holds
+    //    phi at tile cell c (x: c < 32, y: next 16, z: last 8, times the
+    //    strength), zero outside the support or the grid.  One thread per
+    //    (point, axis) clears its row and writes the w support values that
+    //    fall in the tile (the same thread, so no barrier between the two).
+    for (int e = tid; e < 3 * npts; e += SPREAD_THREADS) {
+      const int d = e >= 2 * npts ? 2 : (e >= npts ? 1 : 0);
+      const int p = e - d * npts;
+      const int4 m = s_meta[p];
+      const int rel = d == 0 ? m.x : (d == 1 ? m.y : m.z);
+      const int len = d == 0 ? TILE_X : (d == 1 ? TILE_Y : TILE_Z);
+      const int lim = d == 0 ? tx : (d == 1 ? ty : tz);
+      const int n = g.nf[d];
+      const R off = s_off[(size_t)p * 4 + 1 + d];
+      const R sc = d == 2 ? strength[m.w] : R(1);
+      R *row = s_rows + (size_t)p * SPREAD_ROW + (d == 0 ? 0 : (d == 1 ? TILE_X : TILE_X + TILE_Y));
+      for (int j = 0; j < len; j += 4) store_rec(row + j, R(0), R(0), R(0), R(0));
+      // support cell k sits at tile cell rel + k, cyclically (rel in [0, n))
+      for (int k = 0; k < w; ++k) {
+        int cell = rel + k;
+        if (cell >= n) cell -= n;
+        const R v = es_at(k, off, halfw, c2, beta) * sc;
+        if (cell < lim) row[cell] = v;
       }
     }
     __syncthreads();
 
-    // 4. each warp walks only the points that reach its patch, transform by
+    // 3. each warp walks only the points that reach its patch, transform by
     //    transform (static accumulator indices)
 #pragma unroll
     for (int t = 0; t < TM; ++t) {
@@ -327,14 +359,10 @@ __global__ void __launch_bounds__(SPREAD_THREADS, (sizeof(R) == 4 || NT == 1) ? 
         while (am) {
           const int q = pb + __ffs(am) - 1;
           am &= am - 1u;
-          const int4 m = s_meta[q];
-          const R *v = s_vals + (size_t)q * stride + 1;
-          int kx = cx - m.x;
-          if (kx < 0) kx += g.nf[0];
-          int ky = cy - m.y;
-          if (ky < 0) ky += g.nf[1];
-          const R a = (kx < w ? v[kx] : R(0)) * (ky < w ? v[w + ky] : R(0));
-          const R *zr = s_zrow + q * TILE_Z;
+          const R *row = s_rows + q * SPREAD_ROW;
+          const R a = row[cx] * row[TILE_X + cy];
+          R zr[TILE_Z];
+          load_zrow(row + TILE_X + TILE_Y, zr);
 #pragma unroll
           for (int z = 0; z < TILE_Z; ++z) acc[t][z] = fma(a, zr[z], acc[t][z]);
         }
@@ -542,20 +570,20 @@ cudaError_t launch_scatter(const double *pos, const uint8_t *species, const Fram
   return cudaGetLastError();
 }
 
-size_t spread_point_bytes(int stride, bool fp64) {
+size_t spread_point_bytes(bool fp64) {
   const size_t r = fp64 ? 8 : 4;
-  return (size_t)stride * r + (size_t)TILE_Z * r + sizeof(int4) + 2 * sizeof(int);
+  return (size_t)(SPREAD_ROW + 4) * r + sizeof(int4) + sizeof(unsigned);
 }
 
-size_t spread_smem_bytes(int chunk, int stride, bool fp64) {
-  return (size_t)chunk * spread_point_bytes(stride, fp64);
+size_t spread_smem_bytes(int chunk, bool fp64) {
+  return (size_t)chunk * spread_point_bytes(fp64);
 }
 
-int spread_chunk(int stride, bool fp64) {
-  // Two CTAs per SM when the staging fits in ~110 KB, else one (<= 220 KB).
-  const size_t per = spread_point_bytes(stride, fp64);
-  int c = (int)((110 * 1024) / per);
-  if (c < 128) c = (int)((220 * 1024) / per);
+int spread_chunk(bool fp64, int ntr) {
+  // Two CTAs per SM (FP32, or one transform) share ~216 KB of shared memory;
+  // the FP64 multi-transform kernel runs one CTA per SM.
+  const size_t budget = (fp64 && ntr != 1) ? 216 * 1024 : 106 * 1024;
+  int c = (int)(budget / spread_point_bytes(fp64));
   c = c > SPREAD_THREADS ? SPREAD_THREADS : c;
   return c / 32 * 32;
 }
@@ -593,7 +621,7 @@ template <typename R>
 cudaError_t launch_spread(const R *recs, const int *starts, const FrameGeom &g,
                           const R *strength, R *grid, cudaStream_t s) {
   const dim3 grd((unsigned)g.ntiles);
-  const size_t sm = spread_smem_bytes(g.chunk, g.rec_stride, sizeof(R) == 8);
+  const size_t sm = spread_smem_bytes(g.chunk, sizeof(R) == 8);
   switch (g.ntr) {
     case 1: k_spread<R, 1><<<grd, SPREAD_THREADS, sm, s>>>(recs, starts, g, strength, grid); break;
     case 2: k_spread<R, 2><<<grd, SPREAD_THREADS, sm, s>>>(recs, starts, g, strength, grid); break;
