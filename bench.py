@@ -420,12 +420,10 @@ def run_ours(args, rank, world, local_rank):
     # --- dS/dr evaluations (differentiation form) -------------------------------
     grad = None if args.no_grad else grad_leg(W, K, stream, dist, local_rank)
 
-    # --- sharded frames: sum the accumulators once ------------------------------
+    # --- sharded frames: sum the FP64 accumulators once (one all-reduce) --------
     if dist:
-        acc = plan.accumulators()
-        t = torch.from_numpy(np.concatenate([acc["num"], acc["partial_num"].reshape(-1)])).to(
-            f"cuda:{local_rank}")
-        td.all_reduce(t)
+        from sqcalc_b200.shard import reduce_plan
+        reduce_plan(plan)
     plan.close()
 
     if rank == 0:

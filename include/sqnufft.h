@@ -169,6 +169,18 @@ int sqn_finalize(sqn_plan *plan, int32_t faber_ziman, double *S_total, double *S
 /* Zero the accumulators and the frame count. */
 int sqn_reset(sqn_plan *plan);
 
+/* Frames sharded over ranks (one process per GPU, each with its own plan on
+ * the same system).  The plan's FP64 sums -- shell sums, pair sums and, with
+ * want_grid, the per-mode sums -- are one device buffer of *count doubles at
+ * *acc (syncs first); *nframes receives the frames accumulated here.  The
+ * caller adds the buffers of all ranks in place with one sum all-reduce
+ * (ncclAllReduce on the device pointer), then calls sqn_set_frame_count with
+ * the total so that sqn_finalize normalises over all frames.  Replaces nothing
+ * in the reference, which reads one trajectory in one process
+ * (src/sqc_structure_factor.f90:457-470 per frame). */
+int sqn_accumulator_view(sqn_plan *plan, double **acc, int64_t *count, int64_t *nframes);
+int sqn_set_frame_count(sqn_plan *plan, int64_t nframes);
+
 /* Per-stage device time summed over the frames since the last reset, in ms:
  * out[0] wrap+bin sort, out[1] spread, out[2] FFT, out[3] deconvolve+bin,
  * out[4] frames timed.  Needs SQN_FLAG_TIMING. */

@@ -29,7 +29,8 @@ EXPORTS = (
     "sqn_abi_version", "sqn_error_string", "sqn_default_desc", "sqn_plan_create",
     "sqn_plan_info_get", "sqn_accumulate_frames", "sqn_sync", "sqn_get_accumulators",
     "sqn_peek_num_async", "sqn_finalize", "sqn_reset", "sqn_stage_times", "sqn_launch_count",
-    "sqn_plan_destroy", "sqn_spread_frame_noalloc", "sqn_sq_grad",
+    "sqn_plan_destroy", "sqn_spread_frame_noalloc", "sqn_sq_grad", "sqn_accumulator_view",
+    "sqn_set_frame_count",
 )
 ERR_SCRATCH_LIMIT = 49
 NOALLOC_SCRATCH_BYTES = 32 * 1024 * 1024
@@ -118,6 +119,9 @@ def load():
     L.sqn_launch_count.restype = i64
     L.sqn_plan_destroy.argtypes = [vp]
     L.sqn_sq_grad.argtypes = [vp, vp, ctypes.c_int32, vp, vp, vp]
+    L.sqn_accumulator_view.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(i64),
+                                       ctypes.POINTER(i64)]
+    L.sqn_set_frame_count.argtypes = [vp, i64]
     L.sqn_spread_frame_noalloc.argtypes = [vp, i64, vp, ctypes.c_int32, vp, vp, vp, vp,
                                            ctypes.c_int32, ctypes.c_double, vp, vp]
     if L.sqn_abi_version() != ABI_VERSION:
@@ -268,6 +272,16 @@ class Plan:
         check(self._L.sqn_sq_grad(self._h, _ptr(a), HOST, _ptr(g), _ptr(S), _ptr(grad)),
               "sqn_sq_grad")
         return S, grad
+
+    def accumulator_view(self):
+        """(device pointer, number of doubles, frames so far) of the plan's FP64 sums."""
+        ptr, count, nf = ctypes.c_void_p(), ctypes.c_int64(), ctypes.c_int64()
+        check(self._L.sqn_accumulator_view(self._h, ctypes.byref(ptr), ctypes.byref(count),
+                                           ctypes.byref(nf)), "sqn_accumulator_view")
+        return int(ptr.value or 0), int(count.value), int(nf.value)
+
+    def set_frame_count(self, nframes):
+        check(self._L.sqn_set_frame_count(self._h, int(nframes)), "sqn_set_frame_count")
 
     def peek_num_async(self, host_buf_ptr):
         check(self._L.sqn_peek_num_async(self._h, ctypes.c_void_p(host_buf_ptr)), "sqn_peek")

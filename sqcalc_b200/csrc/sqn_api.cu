@@ -538,13 +538,14 @@ int setup_plan(sqn_plan *p, const sqn_plan_desc *d) {
   if ((st = dalloc(p, &p->d_amp_sp, (size_t)p->nspecies))) return st;
   if ((st = dalloc(p, &p->d_xcoef_sp, 9 * (size_t)p->nspecies))) return st;
   if ((st = dalloc(p, &p->d_counts_sp, (size_t)p->nspecies))) return st;
-  if ((st = dalloc(p, &p->d_acc, (size_t)p->nquant * d->nq))) return st;
+  // The FP64 sums (shell sums, pair sums, then the per-mode sums with
+  // want_grid) share one allocation, so that ranks holding disjoint frames can
+  // add them with a single all-reduce (sqn_accumulator_view).
+  if (d->want_grid) p->gnum_half = (int64_t)(p->hm[0] + 1) * p->modes[1] * p->modes[2];
+  if ((st = dalloc(p, &p->d_acc, (size_t)p->nquant * d->nq + (size_t)p->gnum_half))) return st;
+  if (d->want_grid) p->d_gnum = p->d_acc + (size_t)p->nquant * d->nq;
   if ((st = dalloc(p, &p->d_den, (size_t)d->nq))) return st;
   if ((st = dalloc(p, &p->d_cnt, (size_t)d->nq))) return st;
-  if (d->want_grid) {
-    p->gnum_half = (int64_t)(p->hm[0] + 1) * p->modes[1] * p->modes[2];
-    if ((st = dalloc(p, &p->d_gnum, (size_t)p->gnum_half))) return st;
-  }
 
   // --- constant tables ----------------------------------------------------
   cudaStream_t s = p->stream;
@@ -1056,12 +1057,30 @@ int sqn_finalize(sqn_plan *p, int32_t faber_ziman, double *S_total, double *S_pa
   return SQN_OK;
 }
 
+int sqn_accumulator_view(sqn_plan *p, double **acc, int64_t *count, int64_t *nframes) {
+  if (!p) return SQN_ERR_PLAN_NOTVALID;
+  if (!acc || !count) return SQN_ERR_INVALID_ARGUMENT;
+  DeviceGuard guard(p->device);
+  if (cudaStreamSynchronize(p->stream) != cudaSuccess) return SQN_ERR_CUDA;
+  *acc = p->d_acc;
+  *count = (int64_t)p->nquant * p->desc.nq + p->gnum_half;
+  if (nframes) *nframes = p->nframes;
+  return SQN_OK;
+}
+
+int sqn_set_frame_count(sqn_plan *p, int64_t nframes) {
+  if (!p) return SQN_ERR_PLAN_NOTVALID;
+  if (nframes < 0) return SQN_ERR_INVALID_ARGUMENT;
+  p->nframes = nframes;
+  return SQN_OK;
+}
+
 int sqn_reset(sqn_plan *p) {
   if (!p) return SQN_ERR_PLAN_NOTVALID;
   DeviceGuard guard(p->device);
   if (cudaStreamSynchronize(p->stream) != cudaSuccess) return SQN_ERR_CUDA;
-  cudaError_t e = cudaMemset(p->d_acc, 0, sizeof(double) * (size_t)p->nquant * p->desc.nq);
-  if (e == cudaSuccess && p->d_gnum) e = cudaMemset(p->d_gnum, 0, sizeof(double) * (size_t)p->gnum_half);
+  cudaError_t e = cudaMemset(p->d_acc, 0,
+                             sizeof(double) * ((size_t)p->nquant * p->desc.nq + (size_t)p->gnum_half));
   p->nframes = 0;
   p->tev_used = 0;
   for (double &v : p->stage_ms) v = 0.0;
