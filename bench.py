@@ -267,6 +267,71 @@ def precision_leg(types, dev, base, fbytes, W, K, stream, dist, world, local_ran
     return fp64
 
 
+BATCH_SYSTEMS, BATCH_QMAX, BATCH_NQ, BATCH_FRAMES = 64, 8.0, 400, 20
+
+
+def batched_leg(W, K, stream, dist, local_rank):
+    """Batched form: 64 independent cubic systems, N ~ U[5k, 200k] at 0.08 A^-3,
+    2 types 1:2, uniform positions, q_max 8, FP32 + FP64 accumulation, partials.
+    One step = one frame of every system = one CUDA graph launch (the systems'
+    pipelines are parallel branches of the graph).  Reported beside it: the same
+    plans launched one after another from the host without the graph."""
+    import torch
+    from sqcalc_b200 import _lib
+    from sqcalc_b200.synthetic import batched_systems
+
+    systems = batched_systems(BATCH_SYSTEMS, SEED + 3)
+    kws = [dict(cell=np.eye(3).reshape(9) * box, origin=np.zeros(3), type_id=types, qmin=0.0,
+                qmax=BATCH_QMAX, nq=BATCH_NQ, partials=True, precision=_lib.PREC_SINGLE,
+                eps=EPS, device=local_rank) for _, box, types in systems]
+    t0 = time.perf_counter()
+    batch = _lib.Batch(kws, stream=stream.cuda_stream)
+    t_create = time.perf_counter() - t0
+    gen = torch.Generator(device=f"cuda:{local_rank}").manual_seed(SEED + 5)
+    nfr = 4  # distinct i.i.d. frames per system, cycled
+    dev = [torch.rand((nfr, n, 3), generator=gen, device=f"cuda:{local_rank}",
+                      dtype=torch.float64) * box for n, box, _ in systems]
+    torch.cuda.synchronize()
+    step = lambda f: batch.accumulate([d[f % nfr].data_ptr() for d in dev],  # noqa: E731
+                                      where=_lib.DEVICE, nframes=1)
+    for f in range(W):
+        step(f)
+    batch.sync()
+    k = min(K, BATCH_FRAMES)
+    l0 = sum(v.launch_count() for v in batch.plans)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for f in range(k):
+        step(W + f)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    t = _max_over_ranks(ev0.elapsed_time(ev1) * 1e-3, dist, local_rank)
+    launches = sum(v.launch_count() for v in batch.plans) - l0
+    # the same plans without the graph: host-issued launches, system after system
+    batch.sync()
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    for f in range(k):
+        for v, d in zip(batch.plans, dev):
+            v.accumulate((d[(W + f) % nfr].data_ptr(), 1), where=_lib.DEVICE)
+    for v in batch.plans:
+        v.sync()
+    t_nograph = time.perf_counter() - t1
+    natoms = sum(n for n, _, _ in systems)
+    out = {"metric": "batched S(q) system-frames/s", "unit": "system-frames/s",
+           "value": k * BATCH_SYSTEMS / t, "atom_frames_per_s": k * natoms / t,
+           "ms_per_step": 1e3 * t / k, "steps": k, "systems": BATCH_SYSTEMS,
+           "natoms_total": natoms, "graph_launches_per_step": 1,
+           "gpu_launches_per_step": launches / k,
+           "no_graph_ms_per_step_wall": 1e3 * t_nograph / k, "create_s": t_create,
+           "config": {"workload": "batched form: 64 cubic systems, N~U[5k,200k] at 0.08 A^-3, "
+                                  "2 types 1:2, uniform, qmax 8, nq 400, partials, FP32+FP64acc, "
+                                  "eps 1e-6",
+                      "fine_grids": sorted({int(v.info.nf[0]) for v in batch.plans})}}
+    batch.close()
+    return out
+
+
 GRAD_N, GRAD_BOX, GRAD_QMIN, GRAD_QMAX, GRAD_NQ = 100_000, 100.0, 0.5, 8.0, 375
 
 
@@ -420,6 +485,9 @@ def run_ours(args, rank, world, local_rank):
     # --- dS/dr evaluations (differentiation form) -------------------------------
     grad = None if args.no_grad else grad_leg(W, K, stream, dist, local_rank)
 
+    # --- batched form: many systems behind one CUDA graph -------------------------
+    batched = None if args.no_batch else batched_leg(W, K, stream, dist, local_rank)
+
     # --- sharded frames: sum the FP64 accumulators once (one all-reduce) --------
     if dist:
         from sqcalc_b200.shard import reduce_plan
@@ -468,6 +536,7 @@ def run_ours(args, rank, world, local_rank):
                                  "cuFFT kernels not counted",
             "fp64": fp64,
             "grad": grad,
+            "batched": batched,
             "clocks": clk.summary(),
             "wall_s": t_wall,
         }
@@ -489,6 +558,7 @@ def main():
     ap.add_argument("--upsampfac", type=float, default=0.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-grad", action="store_true", help="skip the dS/dr leg")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-systems leg")
     ap.add_argument("--scale", type=float, default=1.0,
                     help="shrink the box by this factor at fixed density (profiling only)")
     args = ap.parse_args()

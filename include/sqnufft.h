@@ -202,6 +202,36 @@ int sqn_sq_grad(sqn_plan *plan, const double *pos, int32_t where, const double *
 /* Number of this library's own kernel launches so far (cuFFT's not counted). */
 int64_t sqn_launch_count(const sqn_plan *plan);
 
+/* ---- Batches of independent systems ------------------------------------
+ * Many uneven systems (each its own cell, atoms, types and grid) whose frames
+ * are accumulated together: one plan per system, and one frame of EVERY system
+ * captured once into a CUDA graph -- the root stream forks to one stream per
+ * system (its prep, scan, scatter, spread, FFT and bin launches form one
+ * branch) and joins -- so that a step over all systems is a single graph
+ * launch with the systems' kernels running side by side.  No counterpart in the
+ * reference, which runs one system per process.
+ *
+ * sqn_batch_create: descs[nsystems] as for sqn_plan_create (same device; each
+ *   desc's stream is ignored, its timing flag cleared); stream is the root
+ *   stream (NULL: the batch creates one).
+ * sqn_batch_accumulate: pos[k] holds nframes frames [nframes][natoms_k][3] of
+ *   system k (host or device, all the same); per frame the positions are staged
+ *   on the root stream and the graph is replayed.  Asynchronous for device
+ *   positions.
+ * sqn_batch_plan: the plan of system k (owned by the batch) for
+ *   sqn_get_accumulators / sqn_finalize after sqn_batch_sync; do not accumulate
+ *   on it directly while graph replays are in flight.
+ * sqn_batch_graph_launches: graph replays so far. */
+typedef struct sqn_batch_s sqn_batch;
+int sqn_batch_create(const sqn_plan_desc *descs, int32_t nsystems, void *stream,
+                     sqn_batch **out);
+int sqn_batch_accumulate(sqn_batch *batch, const double *const *pos, int64_t nframes,
+                         int32_t where);
+int sqn_batch_sync(sqn_batch *batch);
+int sqn_batch_plan(sqn_batch *batch, int32_t system, sqn_plan **plan);
+int64_t sqn_batch_graph_launches(const sqn_batch *batch);
+int sqn_batch_destroy(sqn_batch *batch);
+
 /* Size of the fixed device scratch array of sqn_spread_frame_noalloc (per GPU). */
 #define SQN_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
 

@@ -30,7 +30,8 @@ EXPORTS = (
     "sqn_plan_info_get", "sqn_accumulate_frames", "sqn_sync", "sqn_get_accumulators",
     "sqn_peek_num_async", "sqn_finalize", "sqn_reset", "sqn_stage_times", "sqn_launch_count",
     "sqn_plan_destroy", "sqn_spread_frame_noalloc", "sqn_sq_grad", "sqn_accumulator_view",
-    "sqn_set_frame_count",
+    "sqn_set_frame_count", "sqn_batch_create", "sqn_batch_accumulate", "sqn_batch_sync",
+    "sqn_batch_plan", "sqn_batch_graph_launches", "sqn_batch_destroy",
 )
 ERR_SCRATCH_LIMIT = 49
 NOALLOC_SCRATCH_BYTES = 32 * 1024 * 1024
@@ -122,6 +123,13 @@ def load():
     L.sqn_accumulator_view.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(i64),
                                        ctypes.POINTER(i64)]
     L.sqn_set_frame_count.argtypes = [vp, i64]
+    L.sqn_batch_create.argtypes = [ctypes.POINTER(SqnDesc), ctypes.c_int32, vp, ctypes.POINTER(vp)]
+    L.sqn_batch_accumulate.argtypes = [vp, ctypes.POINTER(vp), i64, ctypes.c_int32]
+    L.sqn_batch_sync.argtypes = [vp]
+    L.sqn_batch_plan.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(vp)]
+    L.sqn_batch_graph_launches.argtypes = [vp]
+    L.sqn_batch_graph_launches.restype = i64
+    L.sqn_batch_destroy.argtypes = [vp]
     L.sqn_spread_frame_noalloc.argtypes = [vp, i64, vp, ctypes.c_int32, vp, vp, vp, vp,
                                            ctypes.c_int32, ctypes.c_double, vp, vp]
     if L.sqn_abi_version() != ABI_VERSION:
@@ -158,6 +166,20 @@ class Plan:
                  grad=False):
         L = load()
         self._L = L
+        d = self._describe(cell, origin, type_id, ntypes, weight, amp_const, xray_coef, qmin,
+                           qmax, nq, norm, partials, want_grid, precision, eps, upsampfac,
+                           kernel_width, device, max_grid_modes, timing, stream, grad)
+        h = ctypes.c_void_p()
+        self.status = check(L.sqn_plan_create(ctypes.byref(d), ctypes.byref(h)), "sqn_plan_create")
+        self._attach(h, owned=True)
+
+    def _describe(self, cell, origin, type_id, ntypes=None, weight=WEIGHT_UNIT, amp_const=None,
+                  xray_coef=None, qmin=0.0, qmax=20.0, nq=500, norm=NORM_MEAN, partials=True,
+                  want_grid=False, precision=PREC_DOUBLE, eps=1e-9, upsampfac=0.0,
+                  kernel_width=0, device=0, max_grid_modes=0, timing=False, stream=None,
+                  grad=False):
+        """Fill an SqnDesc; the arrays it points to are kept on self."""
+        L = self._L
         self.type_id = np.ascontiguousarray(type_id, dtype=np.int32)
         self.natoms = int(self.type_id.size)
         self.ntypes = int(ntypes if ntypes is not None else max(int(self.type_id.max()), 1))
@@ -193,11 +215,13 @@ class Plan:
         d.kernel_width = int(kernel_width)
         d.max_grid_modes = int(max_grid_modes)
         d.stream = stream
-        h = ctypes.c_void_p()
-        self.status = check(L.sqn_plan_create(ctypes.byref(d), ctypes.byref(h)), "sqn_plan_create")
+        return d
+
+    def _attach(self, h, owned):
         self._h = h
+        self._owned = owned
         info = SqnInfo()
-        check(L.sqn_plan_info_get(h, ctypes.byref(info)), "sqn_plan_info_get")
+        check(self._L.sqn_plan_info_get(h, ctypes.byref(info)), "sqn_plan_info_get")
         self.info = info
         self.modes = tuple(info.modes)
         self.nmodes = int(info.nmodes)
@@ -300,7 +324,80 @@ class Plan:
 
     def close(self):
         if getattr(self, "_h", None) and self._h.value:
-            self._L.sqn_plan_destroy(self._h)
+            if getattr(self, "_owned", True):
+                self._L.sqn_plan_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """sqn_batch: many independent systems, one CUDA graph launch per frame of all.
+
+    systems: list of dicts of Plan keyword arguments (cell, origin, type_id, ...).
+    plans[k] is a non-owning Plan view of system k for results."""
+
+    def __init__(self, systems, stream=None):
+        L = load()
+        self._L = L
+        n = len(systems)
+        descs = (SqnDesc * max(n, 1))()
+        views = []
+        for k, kw in enumerate(systems):
+            v = Plan.__new__(Plan)
+            v._L = L
+            descs[k] = v._describe(**kw)
+            views.append(v)
+        h = ctypes.c_void_p()
+        self.status = check(L.sqn_batch_create(descs, n, stream, ctypes.byref(h)),
+                            "sqn_batch_create")
+        self._h = h
+        for k, v in enumerate(views):
+            ph = ctypes.c_void_p()
+            check(L.sqn_batch_plan(h, k, ctypes.byref(ph)), "sqn_batch_plan")
+            v._attach(ph, owned=False)
+        self.plans = views
+
+    def accumulate(self, pos, where=HOST, nframes=None):
+        """pos[k]: (nframes, natoms_k, 3) float64 numpy arrays (host), or device
+        pointers (ints) with where=DEVICE and nframes given."""
+        n = len(self.plans)
+        ptrs = (ctypes.c_void_p * n)()
+        if where == DEVICE:
+            for k in range(n):
+                ptrs[k] = int(pos[k])
+            nf = int(nframes)
+        else:
+            self._hold = [np.ascontiguousarray(a, dtype=np.float64) for a in pos]
+            nf = 1 if self._hold[0].ndim == 2 else self._hold[0].shape[0]
+            for k, (a, v) in enumerate(zip(self._hold, self.plans)):
+                if a.size != nf * v.natoms * 3:
+                    raise ValueError("system %d: positions must hold %d frames of %d atoms"
+                                     % (k, nf, v.natoms))
+                ptrs[k] = a.ctypes.data
+        check(self._L.sqn_batch_accumulate(self._h, ptrs, nf, where), "sqn_batch_accumulate")
+
+    def sync(self):
+        check(self._L.sqn_batch_sync(self._h), "sqn_batch_sync")
+
+    def graph_launches(self):
+        return int(self._L.sqn_batch_graph_launches(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            for v in self.plans:
+                v._h = ctypes.c_void_p()
+            self._L.sqn_batch_destroy(self._h)
             self._h = ctypes.c_void_p()
 
     def __enter__(self):

@@ -1150,3 +1150,185 @@ int sqn_plan_destroy(sqn_plan *p) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batches of independent systems behind one CUDA graph
+// ---------------------------------------------------------------------------
+
+struct sqn_batch_s {
+  int device = 0;
+  std::vector<sqn_plan *> plans;
+  cudaStream_t root = nullptr;
+  bool own_root = false;
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> joins;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int64_t replays = 0;
+};
+
+namespace {
+
+void free_batch(sqn_batch *b) {
+  if (!b) return;
+  cudaSetDevice(b->device);
+  if (b->root) cudaStreamSynchronize(b->root);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  for (cudaEvent_t e : b->joins)
+    if (e) cudaEventDestroy(e);
+  if (b->fork) cudaEventDestroy(b->fork);
+  for (sqn_plan *p : b->plans) free_plan(p);
+  if (b->own_root && b->root) cudaStreamDestroy(b->root);
+  delete b;
+}
+
+// One frame of every system, captured once: the root stream forks to each
+// system's own stream (its prep, scan, scatter, spread, FFT and bin launches
+// form one branch) and joins them again.  Each replay reads the positions
+// from the systems' staging buffers d_pos[0].
+int capture_batch(sqn_batch *b) {
+  cudaStream_t root = b->root;
+  if (cudaStreamBeginCapture(root, cudaStreamCaptureModeRelaxed) != cudaSuccess)
+    return SQN_ERR_CUDA;
+  int st = cudaEventRecord(b->fork, root) == cudaSuccess ? SQN_OK : SQN_ERR_CUDA;
+  for (size_t k = 0; k < b->plans.size() && st == SQN_OK; ++k) {
+    sqn_plan *p = b->plans[k];
+    if (cudaStreamWaitEvent(p->stream, b->fork, 0) != cudaSuccess) {
+      st = SQN_ERR_CUDA;
+      break;
+    }
+    st = p->fp64 ? run_frame<double>(p, p->d_pos[0], -1) : run_frame<float>(p, p->d_pos[0], -1);
+    // the capture itself accumulates nothing
+    p->nframes -= 1;
+    p->launches -= 5;
+    if (st == SQN_OK && (cudaEventRecord(b->joins[k], p->stream) != cudaSuccess ||
+                         cudaStreamWaitEvent(root, b->joins[k], 0) != cudaSuccess))
+      st = SQN_ERR_CUDA;
+  }
+  cudaGraph_t g = nullptr;
+  const cudaError_t ee = cudaStreamEndCapture(root, &g);
+  if (st != SQN_OK || ee != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    return st != SQN_OK ? st : SQN_ERR_CUDA;
+  }
+  b->graph = g;
+  if (cudaGraphInstantiate(&b->exec, g, 0) != cudaSuccess) {
+    cudaGetLastError();
+    return SQN_ERR_CUDA;
+  }
+  return SQN_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sqn_batch_create(const sqn_plan_desc *descs, int32_t nsystems, void *stream,
+                     sqn_batch **out) {
+  if (!out) return SQN_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (!descs || nsystems < 1) return SQN_ERR_INVALID_ARGUMENT;
+  for (int32_t k = 1; k < nsystems; ++k)
+    if (descs[k].device != descs[0].device) return SQN_ERR_INVALID_ARGUMENT;
+  sqn_batch *b = new (std::nothrow) sqn_batch_s();
+  if (!b) return SQN_ERR_ALLOC;
+  b->device = descs[0].device;
+  int prev = -1;
+  cudaGetDevice(&prev);
+  int warn = SQN_OK;
+  int st = cudaSetDevice(b->device) == cudaSuccess ? SQN_OK : SQN_ERR_NO_DEVICE;
+  if (st == SQN_OK) {
+    if (stream) {
+      b->root = (cudaStream_t)stream;
+    } else if (cudaStreamCreateWithFlags(&b->root, cudaStreamNonBlocking) == cudaSuccess) {
+      b->own_root = true;
+    } else {
+      st = SQN_ERR_CUDA;
+    }
+  }
+  if (st == SQN_OK && cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess)
+    st = SQN_ERR_CUDA;
+  for (int32_t k = 0; k < nsystems && st == SQN_OK; ++k) {
+    // every system runs on a stream of its own (a branch of the graph)
+    sqn_plan_desc d = descs[k];
+    d.stream = nullptr;
+    d.flags &= ~(uint32_t)SQN_FLAG_TIMING;
+    sqn_plan *p = nullptr;
+    const int ps = sqn_plan_create(&d, &p);
+    if (ps > SQN_WARN_EPS_TOO_SMALL) {
+      st = ps;
+      break;
+    }
+    if (ps != SQN_OK) warn = ps;
+    b->plans.push_back(p);
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) st = SQN_ERR_CUDA;
+    b->joins.push_back(e);
+  }
+  if (st == SQN_OK) {
+    cudaSetDevice(b->device);
+    st = capture_batch(b);
+  }
+  if (st != SQN_OK) {
+    free_batch(b);
+    if (prev >= 0) cudaSetDevice(prev);
+    return st;
+  }
+  if (prev >= 0) cudaSetDevice(prev);
+  *out = b;
+  return warn;
+}
+
+int sqn_batch_accumulate(sqn_batch *b, const double *const *pos, int64_t nframes,
+                         int32_t where) {
+  if (!b) return SQN_ERR_PLAN_NOTVALID;
+  if (!pos || nframes < 0 || (where != SQN_HOST && where != SQN_DEVICE))
+    return SQN_ERR_INVALID_ARGUMENT;
+  for (size_t k = 0; k < b->plans.size(); ++k)
+    if (!pos[k]) return SQN_ERR_INVALID_ARGUMENT;
+  DeviceGuard guard(b->device);
+  const cudaMemcpyKind kind = where == SQN_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+  for (int64_t f = 0; f < nframes; ++f) {
+    // stage this frame of every system (in stream order after the previous
+    // replay has read the staging buffers), then replay the graph
+    for (size_t k = 0; k < b->plans.size(); ++k) {
+      sqn_plan *p = b->plans[k];
+      const size_t n3 = 3 * (size_t)p->desc.natoms;
+      if (cudaMemcpyAsync(p->d_pos[0], pos[k] + n3 * (size_t)f, sizeof(double) * n3, kind,
+                          b->root) != cudaSuccess)
+        return SQN_ERR_CUDA;
+    }
+    if (cudaGraphLaunch(b->exec, b->root) != cudaSuccess) return SQN_ERR_CUDA;
+    b->replays++;
+    for (sqn_plan *p : b->plans) {
+      p->nframes++;
+      p->launches += 5;
+    }
+  }
+  return SQN_OK;
+}
+
+int sqn_batch_sync(sqn_batch *b) {
+  if (!b) return SQN_ERR_PLAN_NOTVALID;
+  DeviceGuard guard(b->device);
+  return cuda_status(cudaStreamSynchronize(b->root));
+}
+
+int sqn_batch_plan(sqn_batch *b, int32_t system, sqn_plan **plan) {
+  if (!b) return SQN_ERR_PLAN_NOTVALID;
+  if (!plan || system < 0 || (size_t)system >= b->plans.size()) return SQN_ERR_INVALID_ARGUMENT;
+  *plan = b->plans[(size_t)system];
+  return SQN_OK;
+}
+
+int64_t sqn_batch_graph_launches(const sqn_batch *b) { return b ? b->replays : -1; }
+
+int sqn_batch_destroy(sqn_batch *b) {
+  if (!b) return SQN_ERR_PLAN_NOTVALID;
+  free_batch(b);
+  return SQN_OK;
+}
+
+}  // extern "C"

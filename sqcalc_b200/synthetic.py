@@ -42,3 +42,19 @@ def uniform_two_types(natoms: int, box: float, seed: int, ratio=(1, 2)):
     types = np.repeat(np.array([1, 2], dtype=np.int32), [n1, natoms - n1])
     rng.shuffle(types)
     return rng.random((natoms, 3)) * box, types
+
+
+def batched_systems(nsystems: int, seed: int, nmin=5_000, nmax=200_000, density=0.08):
+    """Independent cubic systems with N ~ U[nmin, nmax] atoms at the given
+    number density (L = (N / density)^(1/3)), two types 1:2 shuffled.
+    Returns a list of (natoms, box, types)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(nsystems):
+        n = int(rng.integers(nmin, nmax + 1))
+        box = (n / density) ** (1.0 / 3.0)
+        n1 = n // 3
+        types = np.repeat(np.array([1, 2], dtype=np.int32), [n1, n - n1])
+        rng.shuffle(types)
+        out.append((n, box, types))
+    return out
