@@ -404,7 +404,7 @@ def run_ours(args, rank, world, local_rank):
                                   qmin=0.0, qmax=QMAX, nq=NQ, norm=_lib.NORM_MEAN,
                                   partials=True, precision=prec, eps=eps, device=local_rank,
                                   upsampfac=args.upsampfac, timing=timing,
-                                  stream=stream.cuda_stream)
+                                  stream=stream.cuda_stream, fused_fft=args.fused_fft)
 
     # --- device-resident inputs: value --------------------------------------
     dev = torch.from_numpy(frames).to(f"cuda:{local_rank}")
@@ -559,6 +559,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-grad", action="store_true", help="skip the dS/dr leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-systems leg")
+    ap.add_argument("--fused-fft", action="store_true",
+                    help="frame path on the pruned FFT passes fused with the binning")
     ap.add_argument("--scale", type=float, default=1.0,
                     help="shrink the box by this factor at fixed density (profiling only)")
     args = ap.parse_args()

@@ -66,7 +66,10 @@ enum { SQN_HOST = 0, SQN_DEVICE = 1 };
 /* sqn_plan_desc.flags */
 enum {
   SQN_FLAG_TIMING = 1, /* record per-stage CUDA events (sqn_stage_times) */
-  SQN_FLAG_GRAD = 2    /* allocate the adjoint buffers of sqn_sq_grad */
+  SQN_FLAG_GRAD = 2,   /* allocate the adjoint buffers of sqn_sq_grad */
+  SQN_FLAG_FUSED_FFT = 4 /* frame path on the pruned FFT passes fused with the binning
+                            (2,3,5-smooth axes <= 4096) instead of cuFFT R2C + the bin
+                            kernel */
 };
 
 /* Everything sqcalc's configure + gpu_setup know after the first frame
@@ -111,6 +114,8 @@ typedef struct sqn_plan_info {
   int32_t nspecies;         /* type ids that have atoms */
   int64_t device_bytes;     /* device memory the plan holds */
   int64_t tile[3];          /* spread tile in fine-grid cells */
+  int32_t fused_fft;        /* 1: pruned FFT passes fused with the binning; 0: cuFFT + bin kernel */
+  int32_t reserved;
 } sqn_plan_info;
 
 typedef struct sqn_plan_s sqn_plan;

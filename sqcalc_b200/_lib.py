@@ -23,6 +23,7 @@ PREC_DOUBLE, PREC_SINGLE = 0, 1
 HOST, DEVICE = 0, 1
 FLAG_TIMING = 1
 FLAG_GRAD = 2
+FLAG_FUSED_FFT = 4
 
 # Every symbol include/sqnufft.h declares.
 EXPORTS = (
@@ -80,6 +81,8 @@ class SqnInfo(ctypes.Structure):
         ("nspecies", ctypes.c_int32),
         ("device_bytes", ctypes.c_int64),
         ("tile", ctypes.c_int64 * 3),
+        ("fused_fft", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
     ]
 
 
@@ -163,12 +166,12 @@ class Plan:
                  xray_coef=None, qmin=0.0, qmax=20.0, nq=500, norm=NORM_MEAN, partials=True,
                  want_grid=False, precision=PREC_DOUBLE, eps=1e-9, upsampfac=0.0,
                  kernel_width=0, device=0, max_grid_modes=0, timing=False, stream=None,
-                 grad=False):
+                 grad=False, fused_fft=False):
         L = load()
         self._L = L
         d = self._describe(cell, origin, type_id, ntypes, weight, amp_const, xray_coef, qmin,
                            qmax, nq, norm, partials, want_grid, precision, eps, upsampfac,
-                           kernel_width, device, max_grid_modes, timing, stream, grad)
+                           kernel_width, device, max_grid_modes, timing, stream, grad, fused_fft)
         h = ctypes.c_void_p()
         self.status = check(L.sqn_plan_create(ctypes.byref(d), ctypes.byref(h)), "sqn_plan_create")
         self._attach(h, owned=True)
@@ -177,7 +180,7 @@ class Plan:
                   xray_coef=None, qmin=0.0, qmax=20.0, nq=500, norm=NORM_MEAN, partials=True,
                   want_grid=False, precision=PREC_DOUBLE, eps=1e-9, upsampfac=0.0,
                   kernel_width=0, device=0, max_grid_modes=0, timing=False, stream=None,
-                  grad=False):
+                  grad=False, fused_fft=False):
         """Fill an SqnDesc; the arrays it points to are kept on self."""
         L = self._L
         self.type_id = np.ascontiguousarray(type_id, dtype=np.int32)
@@ -209,7 +212,8 @@ class Plan:
         d.partials = int(bool(partials))
         d.want_grid = int(bool(want_grid))
         d.precision = int(precision)
-        d.flags = (FLAG_TIMING if timing else 0) | (FLAG_GRAD if grad else 0)
+        d.flags = ((FLAG_TIMING if timing else 0) | (FLAG_GRAD if grad else 0)
+                   | (FLAG_FUSED_FFT if fused_fft else 0))
         d.eps = float(eps)
         d.upsampfac = float(upsampfac)
         d.kernel_width = int(kernel_width)

@@ -256,6 +256,9 @@ struct sqn_plan_s {
   double *d_acc = nullptr, *d_gnum = nullptr, *d_den = nullptr, *d_cnt = nullptr;
   cufftHandle fft = 0;
   bool fft_ok = false;
+  // fused pruned FFT + binning (sqn_fft.cu); cuFFT + k_bin when off
+  bool fused = false;
+  FftPlan3 fp{};
   // adjoint (SQN_FLAG_GRAD)
   bool grad_ok = false;
   int32_t *d_orig = nullptr;
@@ -349,6 +352,8 @@ std::vector<int4> build_rows(const double *b, const int *hm, double qmax) {
 template <typename R> std::vector<R> to_r(const std::vector<double> &v) {
   return std::vector<R>(v.begin(), v.end());
 }
+
+int setup_fused_fft(sqn_plan *p);
 
 int setup_plan(sqn_plan *p, const sqn_plan_desc *d) {
   p->desc = *d;
@@ -640,6 +645,12 @@ int setup_plan(sqn_plan *p, const sqn_plan_desc *d) {
     if (cufftSetStream(p->fft, s) != CUFFT_SUCCESS) return SQN_ERR_CUFFT;
   }
 
+  // --- fused pruned FFT + binning ------------------------------------------
+  if (d->flags & SQN_FLAG_FUSED_FFT) {
+    const int st2 = setup_fused_fft(p);
+    if (st2 != SQN_OK) return st2;
+  }
+
   // --- adjoint buffers (dS/dr) -----------------------------------------------
   if (d->flags & SQN_FLAG_GRAD) {
     if (xray) return SQN_ERR_NOT_SUPPORTED;
@@ -685,6 +696,94 @@ int setup_plan(sqn_plan *p, const sqn_plan_desc *d) {
   }
   if (cudaStreamSynchronize(s) != cudaSuccess) return SQN_ERR_CUDA;
   return warn;
+}
+
+// Radix stages of an n-point FFT (8s first, then 4 or 2, 3s, 5s); false when
+// n has another prime factor or needs too many stages.
+bool fft_radices(int n, FftAxis &ax) {
+  ax.n = n;
+  ax.nst = 0;
+  int m = n;
+  auto push = [&ax](int r) {
+    if (ax.nst >= FFT_MAX_STAGES) return false;
+    ax.radix[ax.nst++] = r;
+    return true;
+  };
+  while (m % 8 == 0) {
+    if (!push(8)) return false;
+    m /= 8;
+  }
+  if (m % 4 == 0) {
+    if (!push(4)) return false;
+    m /= 4;
+  }
+  if (m % 2 == 0) {
+    if (!push(2)) return false;
+    m /= 2;
+  }
+  while (m % 3 == 0) {
+    if (!push(3)) return false;
+    m /= 3;
+  }
+  while (m % 5 == 0) {
+    if (!push(5)) return false;
+    m /= 5;
+  }
+  return m == 1 && n >= 2;
+}
+
+// Decide whether the frame path runs the fused pruned passes (sqn_fft.cu) and
+// prepare them: radix plans, FP64-computed twiddle tables, shared-memory
+// limits.  Returns SQN_OK also when the plan keeps cuFFT + k_bin.
+int setup_fused_fft(sqn_plan *p) {
+  FftPlan3 &f = p->fp;
+  const BinGeom &b = p->bg;
+  if (p->ntr > MAX_FAST_T) return SQN_OK;
+  for (int d = 0; d < 3; ++d)
+    if (p->nf[d] > FFT_MAX_N || !fft_radices((int)p->nf[d], f.ax[d])) return SQN_OK;
+  f.H1 = p->hm[0] + 1;
+  f.M1 = 2 * p->hm[1] + 1;
+  f.M2 = 2 * p->hm[2] + 1;
+  const size_t rsz = p->fp64 ? 8 : 4;
+  // A2 (ntr x nf2 x M1 x H1 complex) reuses the real grids
+  if ((double)f.M1 * f.H1 * 2.0 > (double)p->nf[1] * p->nf[0]) return SQN_OK;
+  if (p->nf[1] % 2 != 0) return SQN_OK;
+  f.hist_smem = (size_t)b.nquant * b.nq * sizeof(double) <= 48 * 1024;
+  int optin = 0;
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, p->device) !=
+      cudaSuccess)
+    return SQN_ERR_CUDA;
+  const size_t limit = (size_t)optin - 8 * 1024;  // static shared memory and slack
+  for (int pass = 0; pass < 3; ++pass)
+    if (fft_pass_smem(f, pass, p->fp64, p->ntr, b.nquant, b.nq) > limit) return SQN_OK;
+  for (int d = 0; d < 3; ++d) {
+    const int n = f.ax[d].n;
+    std::vector<double> tw(2 * (size_t)n);
+    for (int k = 0; k < n; ++k) {
+      const double a = 2.0 * M_PI * (double)k / (double)n;
+      tw[2 * k] = std::cos(a);
+      tw[2 * k + 1] = -std::sin(a);
+    }
+    char *v = nullptr;
+    int st = dalloc(p, &v, 2 * (size_t)n * rsz);
+    if (st) return st;
+    cudaError_t e;
+    if (p->fp64) {
+      e = cudaMemcpy(v, tw.data(), tw.size() * 8, cudaMemcpyHostToDevice);
+    } else {
+      std::vector<float> tf = to_r<float>(tw);
+      e = cudaMemcpy(v, tf.data(), tf.size() * 4, cudaMemcpyHostToDevice);
+    }
+    if (e != cudaSuccess) return SQN_ERR_CUDA;
+    f.tw[d] = v;
+  }
+  // persistent z-pass CTAs: as many as fit per SM by shared memory, at most 2
+  const size_t sm3 = fft_pass_smem(f, 2, p->fp64, p->ntr, b.nquant, b.nq);
+  int per = (int)((228 * 1024) / (sm3 + 1024));
+  per = std::max(1, std::min(2, per));
+  f.grid3 = p->nsm * per;
+  p->fused = true;
+  return SQN_OK;
 }
 
 // One frame through the weighted forward transform and, with gsh, its adjoint.
@@ -760,19 +859,32 @@ template <typename R> int run_frame(sqn_plan *p, const double *dpos, int slot) {
                        (R *)p->d_grid, s);
   if (e != cudaSuccess) return SQN_ERR_CUDA;
   if (p->timing) cudaEventRecord(ev[2], s);
-  cufftResult fr;
-  if (p->fp64)
-    fr = cufftExecD2Z(p->fft, (cufftDoubleReal *)p->d_grid, (cufftDoubleComplex *)p->d_G);
-  else
-    fr = cufftExecR2C(p->fft, (cufftReal *)p->d_grid, (cufftComplex *)p->d_G);
-  if (fr != CUFFT_SUCCESS) return SQN_ERR_CUFFT;
-  if (p->timing) cudaEventRecord(ev[3], s);
-  e = launch_bin<R>(p->d_rows, p->nrows, p->d_G, p->bg, (const R *)p->d_inv[0],
-                    (const R *)p->d_inv[1], (const R *)p->d_inv[2], p->d_amp, p->d_xcoef,
-                    p->d_acc, p->d_gnum, p->nsm, s);
-  if (e != cudaSuccess) return SQN_ERR_CUDA;
-  if (p->timing) cudaEventRecord(ev[4], s);
-  p->launches += 5;
+  if (p->fused) {
+    // x and y passes (the "FFT" stage), then the z pass with the binning
+    e = launch_fft_xy<R>(p->fp, p->d_grid, p->d_G, p->d_grid, p->bg, g.pitch, s);
+    if (e != cudaSuccess) return SQN_ERR_CUDA;
+    if (p->timing) cudaEventRecord(ev[3], s);
+    e = launch_fft_z_bin<R>(p->fp, p->d_grid, p->bg, (const R *)p->d_inv[0],
+                            (const R *)p->d_inv[1], (const R *)p->d_inv[2], p->d_amp,
+                            p->d_xcoef, p->d_acc, p->d_gnum, s);
+    if (e != cudaSuccess) return SQN_ERR_CUDA;
+    if (p->timing) cudaEventRecord(ev[4], s);
+    p->launches += 7;
+  } else {
+    cufftResult fr;
+    if (p->fp64)
+      fr = cufftExecD2Z(p->fft, (cufftDoubleReal *)p->d_grid, (cufftDoubleComplex *)p->d_G);
+    else
+      fr = cufftExecR2C(p->fft, (cufftReal *)p->d_grid, (cufftComplex *)p->d_G);
+    if (fr != CUFFT_SUCCESS) return SQN_ERR_CUFFT;
+    if (p->timing) cudaEventRecord(ev[3], s);
+    e = launch_bin<R>(p->d_rows, p->nrows, p->d_G, p->bg, (const R *)p->d_inv[0],
+                      (const R *)p->d_inv[1], (const R *)p->d_inv[2], p->d_amp, p->d_xcoef,
+                      p->d_acc, p->d_gnum, p->nsm, s);
+    if (e != cudaSuccess) return SQN_ERR_CUDA;
+    if (p->timing) cudaEventRecord(ev[4], s);
+    p->launches += 5;
+  }
   p->nframes++;
   return SQN_OK;
 }
@@ -886,6 +998,7 @@ int sqn_plan_info_get(const sqn_plan *p, sqn_plan_info *info) {
   info->ntransforms = p->ntr;
   info->nspecies = p->nspecies;
   info->device_bytes = p->device_bytes;
+  info->fused_fft = p->fused ? 1 : 0;
   return SQN_OK;
 }
 
@@ -1201,7 +1314,7 @@ int capture_batch(sqn_batch *b) {
     st = p->fp64 ? run_frame<double>(p, p->d_pos[0], -1) : run_frame<float>(p, p->d_pos[0], -1);
     // the capture itself accumulates nothing
     p->nframes -= 1;
-    p->launches -= 5;
+    p->launches -= p->fused ? 7 : 5;
     if (st == SQN_OK && (cudaEventRecord(b->joins[k], p->stream) != cudaSuccess ||
                          cudaStreamWaitEvent(root, b->joins[k], 0) != cudaSuccess))
       st = SQN_ERR_CUDA;
@@ -1304,7 +1417,7 @@ int sqn_batch_accumulate(sqn_batch *b, const double *const *pos, int64_t nframes
     b->replays++;
     for (sqn_plan *p : b->plans) {
       p->nframes++;
-      p->launches += 5;
+      p->launches += p->fused ? 7 : 5;
     }
   }
   return SQN_OK;

@@ -199,5 +199,68 @@ __device__ __forceinline__ R es_at(int k, R off, R halfw, R c2, R beta) {
   return es_phi(((R)k - halfw) - off, c2, beta);
 }
 
+// One mode per lane, called by all 32 lanes of a warp: classify the mode
+// (kept test and shell, identical to the reference's FP64 evaluation),
+// deconvolve the transforms' values v[t] by dec = 1 / (phihat1 phihat2
+// phihat3), form the weighted total (x-ray f_a(|q|) or constant amplitudes)
+// and, with partials, the pair products Re(rho_a rho_b*) in FP64, and add
+// them with multiplicity 2 for h1 > 0 (the mirror mode -h) to the shell
+// histograms hist[quantity * nq + shell]; with want_grid add |total|^2 to
+// gnum[gidx] (each mode is visited once per frame).  The reference's
+// counterpart is the host loops of src/sqc_structure_factor.f90:481-521
+// and :595-643.
+template <typename R, int TM, bool XR>
+__device__ __forceinline__ void bin_mode(const BinGeom &b, int ntr, bool inrange, int h1, int h2,
+                                         int h3, const double *crow,
+                                         const typename Cplx<R>::T (&v)[TM], R dec,
+                                         const double *__restrict__ amp,
+                                         const double *__restrict__ xcoef, double *hist,
+                                         double *__restrict__ gnum, int64_t gidx, int lane) {
+  double ql = 0.0;
+  int s = 0;
+  const bool keep = inrange && classify_mode(b, crow, h1, h2, h3, s, ql);
+  const unsigned act = __ballot_sync(FULL, keep);
+  if (act == 0u) return;
+  double re[TM], im[TM];
+  double tre = 0.0, tim = 0.0;
+  const double mult = h1 > 0 ? 2.0 : 1.0;
+#pragma unroll
+  for (int t = 0; t < TM; ++t) {
+    re[t] = 0.0;
+    im[t] = 0.0;
+  }
+  if (keep) {
+#pragma unroll
+    for (int t = 0; t < TM; ++t) {
+      if (t < ntr) {
+        re[t] = (double)(v[t].x * dec);
+        im[t] = (double)(v[t].y * dec);
+        const double a = XR ? xray_f(xcoef + 9 * t, ql) : amp[t];
+        tre += a * re[t];
+        tim += a * im[t];
+      }
+    }
+  }
+  const double I = tre * tre + tim * tim;
+  if (b.want_grid && keep) gnum[gidx] += I;
+  const int s0 = __shfl_sync(FULL, s, __ffs(act) - 1);
+  const bool uni = __all_sync(FULL, !keep || s == s0);
+  hist_add(hist, s, mult * I, keep, uni, s0, lane);
+  if (b.partials) {
+    int p = 1;
+#pragma unroll
+    for (int a = 0; a < TM; ++a) {
+#pragma unroll
+      for (int c = a; c < TM; ++c) {
+        if (c < ntr) {
+          hist_add(hist + p * b.nq, s, mult * (re[a] * re[c] + im[a] * im[c]), keep, uni, s0,
+                   lane);
+          ++p;
+        }
+      }
+    }
+  }
+}
+
 }  // namespace dev
 }  // namespace sqn

@@ -100,6 +100,32 @@ size_t spread_smem_bytes(int chunk, bool fp64);
 int spread_chunk(bool fp64, int ntr);
 cudaError_t spread_set_attributes();
 
+// Pruned three-pass FFT fused with the binning (sqn_fft.cu).
+constexpr int FFT_MAX_STAGES = 16;
+constexpr int FFT_MAX_N = 4096;   // longest axis the fused passes take
+struct FftAxis {
+  int n;                          // transform length (2, 3, 5-smooth)
+  int nst;                        // radix stages
+  int radix[FFT_MAX_STAGES];      // 8, 4, 2, 3 or 5 each
+};
+struct FftPlan3 {
+  FftAxis ax[3];
+  const void *tw[3];              // exp(-2 pi i k / n_d), k < n_d, complex R
+  int H1;                         // hm0 + 1 kept x modes (h1 >= 0)
+  int M1, M2;                     // 2 hm1 + 1, 2 hm2 + 1
+  int grid3;                      // persistent CTAs of the z pass
+  bool hist_smem;                 // shell histograms in shared memory
+};
+int fft_columns_per_cta(bool fp64);
+size_t fft_pass_smem(const FftPlan3 &f, int pass, bool fp64, int ntr, int nquant, int nq);
+template <typename R>
+cudaError_t launch_fft_xy(const FftPlan3 &f, const void *grid, void *A1, void *A2,
+                          const BinGeom &b, int64_t pitch, cudaStream_t s);
+template <typename R>
+cudaError_t launch_fft_z_bin(const FftPlan3 &f, const void *A2, const BinGeom &b, const R *inv1,
+                             const R *inv2, const R *inv3, const double *amp,
+                             const double *xcoef, double *acc, double *gnum, cudaStream_t s);
+
 // Adjoint (sqn_adjoint.cu).
 struct Recip {
   double b[9];  // b_j = b[3*j + r]

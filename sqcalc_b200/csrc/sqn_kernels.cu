@@ -430,51 +430,9 @@ __global__ void __launch_bounds__(256, 2)
 #pragma unroll
       for (int t = 0; t < TM; ++t)
         if (t < ntr && inrow) v[t] = G[(int64_t)t * b.vol_cplx + rowbase + h1];
-      double ql = 0.0;
-      int s = 0;
-      const bool keep = inrow && classify_mode(b, crow, h1, h2, h3, s, ql);
-      const unsigned act = __ballot_sync(FULL, keep);
-      if (act == 0u) continue;
-      double re[TM], im[TM];
-      double tre = 0.0, tim = 0.0;
-      const double mult = h1 > 0 ? 2.0 : 1.0;
-#pragma unroll
-      for (int t = 0; t < TM; ++t) {
-        re[t] = 0.0;
-        im[t] = 0.0;
-      }
-      if (keep) {
-        const R dec = inv1[h1] * dyz;
-#pragma unroll
-        for (int t = 0; t < TM; ++t) {
-          if (t < ntr) {
-            re[t] = (double)(v[t].x * dec);
-            im[t] = (double)(v[t].y * dec);
-            const double a = XR ? xray_f(xcoef + 9 * t, ql) : amp[t];
-            tre += a * re[t];
-            tim += a * im[t];
-          }
-        }
-      }
-      const double I = tre * tre + tim * tim;
-      if (b.want_grid && keep) gnum[gbase + h1] += I;
-      const int s0 = __shfl_sync(FULL, s, __ffs(act) - 1);
-      const bool uni = __all_sync(FULL, !keep || s == s0);
-      hist_add(hist, s, mult * I, keep, uni, s0, lane);
-      if (b.partials) {
-        int p = 1;
-#pragma unroll
-        for (int a = 0; a < TM; ++a) {
-#pragma unroll
-          for (int c = a; c < TM; ++c) {
-            if (c < ntr) {
-              hist_add(hist + p * b.nq, s, mult * (re[a] * re[c] + im[a] * im[c]), keep, uni,
-                       s0, lane);
-              ++p;
-            }
-          }
-        }
-      }
+      const R dec = inrow ? inv1[h1] * dyz : R(0);
+      bin_mode<R, TM, XR>(b, ntr, inrow, h1, h2, h3, crow, v, dec, amp, xcoef, hist, gnum,
+                          gbase + h1, lane);
     }
   }
   if (SMEM) {
