@@ -404,7 +404,7 @@ def run_ours(args, rank, world, local_rank):
                                   qmin=0.0, qmax=QMAX, nq=NQ, norm=_lib.NORM_MEAN,
                                   partials=True, precision=prec, eps=eps, device=local_rank,
                                   upsampfac=args.upsampfac, timing=timing,
-                                  stream=stream.cuda_stream, fused_fft=args.fused_fft)
+                                  stream=stream.cuda_stream, fused_fft=True if args.fused_fft else None)
 
     # --- device-resident inputs: value --------------------------------------
     dev = torch.from_numpy(frames).to(f"cuda:{local_rank}")

@@ -67,9 +67,10 @@ enum { SQN_HOST = 0, SQN_DEVICE = 1 };
 enum {
   SQN_FLAG_TIMING = 1, /* record per-stage CUDA events (sqn_stage_times) */
   SQN_FLAG_GRAD = 2,   /* allocate the adjoint buffers of sqn_sq_grad */
-  SQN_FLAG_FUSED_FFT = 4 /* frame path on the pruned FFT passes fused with the binning
-                            (2,3,5-smooth axes <= 4096) instead of cuFFT R2C + the bin
-                            kernel */
+  SQN_FLAG_FUSED_FFT = 4, /* frame path on the pruned FFT passes fused with the binning
+                             (2,3,5-smooth axes <= 4096) instead of cuFFT R2C + the bin
+                             kernel (the default, faster on B200 at the benchmark sizes) */
+  SQN_FLAG_CUFFT = 8       /* cuFFT R2C + the bin kernel (the default) */
 };
 
 /* Everything sqcalc's configure + gpu_setup know after the first frame

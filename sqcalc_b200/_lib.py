@@ -24,6 +24,7 @@ HOST, DEVICE = 0, 1
 FLAG_TIMING = 1
 FLAG_GRAD = 2
 FLAG_FUSED_FFT = 4
+FLAG_CUFFT = 8
 
 # Every symbol include/sqnufft.h declares.
 EXPORTS = (
@@ -166,7 +167,7 @@ class Plan:
                  xray_coef=None, qmin=0.0, qmax=20.0, nq=500, norm=NORM_MEAN, partials=True,
                  want_grid=False, precision=PREC_DOUBLE, eps=1e-9, upsampfac=0.0,
                  kernel_width=0, device=0, max_grid_modes=0, timing=False, stream=None,
-                 grad=False, fused_fft=False):
+                 grad=False, fused_fft=None):
         L = load()
         self._L = L
         d = self._describe(cell, origin, type_id, ntypes, weight, amp_const, xray_coef, qmin,
@@ -180,7 +181,7 @@ class Plan:
                   xray_coef=None, qmin=0.0, qmax=20.0, nq=500, norm=NORM_MEAN, partials=True,
                   want_grid=False, precision=PREC_DOUBLE, eps=1e-9, upsampfac=0.0,
                   kernel_width=0, device=0, max_grid_modes=0, timing=False, stream=None,
-                  grad=False, fused_fft=False):
+                  grad=False, fused_fft=None):
         """Fill an SqnDesc; the arrays it points to are kept on self."""
         L = self._L
         self.type_id = np.ascontiguousarray(type_id, dtype=np.int32)
@@ -213,7 +214,7 @@ class Plan:
         d.want_grid = int(bool(want_grid))
         d.precision = int(precision)
         d.flags = ((FLAG_TIMING if timing else 0) | (FLAG_GRAD if grad else 0)
-                   | (FLAG_FUSED_FFT if fused_fft else 0))
+                   | (0 if fused_fft is None else (FLAG_FUSED_FFT if fused_fft else FLAG_CUFFT)))
         d.eps = float(eps)
         d.upsampfac = float(upsampfac)
         d.kernel_width = int(kernel_width)

@@ -646,7 +646,8 @@ int setup_plan(sqn_plan *p, const sqn_plan_desc *d) {
   }
 
   // --- fused pruned FFT + binning ------------------------------------------
-  if (d->flags & SQN_FLAG_FUSED_FFT) {
+  const bool want_fused = (d->flags & SQN_FLAG_FUSED_FFT) && !(d->flags & SQN_FLAG_CUFFT);
+  if (want_fused) {
     const int st2 = setup_fused_fft(p);
     if (st2 != SQN_OK) return st2;
   }
@@ -729,7 +730,15 @@ bool fft_radices(int n, FftAxis &ax) {
     if (!push(5)) return false;
     m /= 5;
   }
-  return m == 1 && n >= 2;
+  if (m != 1 || n < 2) return false;
+  int ns = 1;
+  for (int st = 0; st < ax.nst; ++st) {
+    ax.nr[st] = make_fastdiv((uint32_t)(n / ax.radix[st]));
+    ax.ns[st] = make_fastdiv((uint32_t)ns);
+    ns *= ax.radix[st];
+  }
+  ax.n_div = make_fastdiv((uint32_t)n);
+  return true;
 }
 
 // Decide whether the frame path runs the fused pruned passes (sqn_fft.cu) and
@@ -744,6 +753,8 @@ int setup_fused_fft(sqn_plan *p) {
   f.H1 = p->hm[0] + 1;
   f.M1 = 2 * p->hm[1] + 1;
   f.M2 = 2 * p->hm[2] + 1;
+  f.H1_div = make_fastdiv((uint32_t)f.H1);
+  f.M2_div = make_fastdiv((uint32_t)f.M2);
   const size_t rsz = p->fp64 ? 8 : 4;
   // A2 (ntr x nf2 x M1 x H1 complex) reuses the real grids
   if ((double)f.M1 * f.H1 * 2.0 > (double)p->nf[1] * p->nf[0]) return SQN_OK;
@@ -776,6 +787,36 @@ int setup_fused_fft(sqn_plan *p) {
     }
     if (e != cudaSuccess) return SQN_ERR_CUDA;
     f.tw[d] = v;
+  }
+  // per h1, the rows h2 whose line along b3 comes within qmax of the origin
+  // (the distance of h1 b1 + h2 b2 from that line bounds |q| from below;
+  // the margin keeps the test conservative under rounding)
+  {
+    const double *rb = p->recip;
+    const double bb = rb[6] * rb[6] + rb[7] * rb[7] + rb[8] * rb[8];
+    const double q2 = p->desc.qmax * p->desc.qmax * (1.0 + 1e-9) + 1e-12;
+    std::vector<int2> span((size_t)f.H1);
+    for (int h1 = 0; h1 < f.H1; ++h1) {
+      int lo = f.M1, hi = -1;
+      for (int h2 = -p->hm[1]; h2 <= p->hm[1]; ++h2) {
+        double v[3];
+        for (int k = 0; k < 3; ++k) v[k] = h1 * rb[k] + h2 * rb[3 + k];
+        const double vv = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+        const double vb = v[0] * rb[6] + v[1] * rb[7] + v[2] * rb[8];
+        if (vv - vb * vb / bb <= q2) {
+          lo = std::min(lo, h2 + p->hm[1]);
+          hi = std::max(hi, h2 + p->hm[1]);
+        }
+      }
+      span[(size_t)h1] = make_int2(lo, hi);
+    }
+    int2 *ds = nullptr;
+    int st = dalloc(p, &ds, span.size());
+    if (st) return st;
+    if (cudaMemcpy(ds, span.data(), span.size() * sizeof(int2), cudaMemcpyHostToDevice) !=
+        cudaSuccess)
+      return SQN_ERR_CUDA;
+    f.h2span = ds;
   }
   // persistent z-pass CTAs: as many as fit per SM by shared memory, at most 2
   const size_t sm3 = fft_pass_smem(f, 2, p->fp64, p->ntr, b.nquant, b.nq);

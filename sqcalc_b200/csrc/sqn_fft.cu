@@ -144,25 +144,68 @@ template <typename C> struct Dft<5, C> {
 // Padded position of element i of a column.
 __device__ __forceinline__ int padi(int i) { return i + (i >> 5); }
 
+__device__ __forceinline__ int fdiv(int x, const FastDiv &f) {
+  return f.d == 1 ? x : (int)__umulhi((uint32_t)x, f.m);
+}
+
 // One radix-RR stage for butterfly j of column col: Stockham, Ns = product
 // of the earlier radices, tw[m] = exp(-2 pi i m / n).
 template <int RR, typename C>
-__device__ __forceinline__ void stage(const C *src, C *dst, int ld, int col, int j, int nr,
+__device__ __forceinline__ void stage(const C *src, C *dst, int ld, int col, int j, int k, int nr,
                                       int Ns, int tstep, const C *tw) {
   C v[RR];
-  const C *s = src + (size_t)col * ld;
+  const C *s = src + col * ld;
 #pragma unroll
   for (int r = 0; r < RR; ++r) v[r] = s[padi(j + r * nr)];
-  const int k = j % Ns;
-  if (k) {
+  // tw[0] = 1 exactly, so k = 0 needs no branch
 #pragma unroll
-    for (int r = 1; r < RR; ++r) v[r] = cmul(v[r], tw[k * r * tstep]);
-  }
+  for (int r = 1; r < RR; ++r) v[r] = cmul(v[r], tw[k * r * tstep]);
   Dft<RR, C>::run(v);
-  C *d = dst + (size_t)col * ld;
+  C *d = dst + col * ld;
   const int o = (j - k) * RR + k;
 #pragma unroll
   for (int r = 0; r < RR; ++r) d[padi(o + r * Ns)] = v[r];
+}
+
+// All butterflies of one radix-RR stage over ncol columns.
+template <int RR, typename C>
+__device__ __forceinline__ void stage_all(const C *a, C *b, int ld, int ncol, const FastDiv &fnr,
+                                          const FastDiv &fns, int Ns, const C *tw) {
+  const int nr = (int)fnr.d;
+  const int tstep = nr / Ns;  // n / (Ns RR)
+  const int tasks = nr * ncol;
+  for (int e = threadIdx.x; e < tasks; e += blockDim.x) {
+    const int col = fdiv(e, fnr), j = e - col * nr;
+    const int k = j - Ns * fdiv(j, fns);  // j mod Ns
+    stage<RR>(a, b, ld, col, j, k, nr, Ns, tstep, tw);
+  }
+}
+
+// Power-of-two lengths: the same stages with every size a compile-time
+// constant (shifts and masks for the index arithmetic).  Radix 8 while three
+// or more factors of two remain, then 4 and/or 2.
+template <int LOGR, int LOGN, int LOGNS, typename C>
+__device__ __forceinline__ void stage_pow2(const C *a, C *b, int ld, int ncol, const C *tw) {
+  constexpr int RR = 1 << LOGR, NR = (1 << LOGN) / RR, NS = 1 << LOGNS;
+  constexpr int TSTEP = NR / NS;
+  const int tasks = NR * ncol;
+  for (int e = threadIdx.x; e < tasks; e += blockDim.x) {
+    const int col = e / NR, j = e & (NR - 1);
+    stage<RR>(a, b, ld, col, j, j & (NS - 1), NR, NS, TSTEP, tw);
+  }
+}
+
+template <int LOGN, int LOGNS, typename C>
+__device__ C *fft_pow2(C *a, C *b, int ld, int ncol, const C *tw) {
+  if constexpr (LOGNS >= LOGN) {
+    return a;
+  } else {
+    constexpr int REM = LOGN - LOGNS;
+    constexpr int LOGR = REM == 4 ? 2 : (REM >= 3 ? 3 : REM);
+    stage_pow2<LOGR, LOGN, LOGNS>(a, b, ld, ncol, tw);
+    __syncthreads();
+    return fft_pow2<LOGN, LOGNS + LOGR>(b, a, ld, ncol, tw);
+  }
 }
 
 // FFT of ncol padded columns (leading dimension ld) in shared memory; a holds
@@ -170,22 +213,24 @@ __device__ __forceinline__ void stage(const C *src, C *dst, int ld, int col, int
 // barrier.
 template <typename C>
 __device__ C *fft_cols(C *a, C *b, const FftAxis &ax, int ncol, int ld, const C *tw) {
-  const int n = ax.n;
+  switch (ax.n) {
+    case 64: return fft_pow2<6, 0>(a, b, ld, ncol, tw);
+    case 128: return fft_pow2<7, 0>(a, b, ld, ncol, tw);
+    case 256: return fft_pow2<8, 0>(a, b, ld, ncol, tw);
+    case 512: return fft_pow2<9, 0>(a, b, ld, ncol, tw);
+    case 1024: return fft_pow2<10, 0>(a, b, ld, ncol, tw);
+    case 2048: return fft_pow2<11, 0>(a, b, ld, ncol, tw);
+    default: break;
+  }
   int Ns = 1;
   for (int st = 0; st < ax.nst; ++st) {
     const int RR = ax.radix[st];
-    const int nr = n / RR;
-    const int tstep = n / (Ns * RR);
-    const int tasks = nr * ncol;
-    for (int e = threadIdx.x; e < tasks; e += blockDim.x) {
-      const int col = e / nr, j = e - col * nr;
-      switch (RR) {
-        case 8: stage<8>(a, b, ld, col, j, nr, Ns, tstep, tw); break;
-        case 4: stage<4>(a, b, ld, col, j, nr, Ns, tstep, tw); break;
-        case 2: stage<2>(a, b, ld, col, j, nr, Ns, tstep, tw); break;
-        case 3: stage<3>(a, b, ld, col, j, nr, Ns, tstep, tw); break;
-        default: stage<5>(a, b, ld, col, j, nr, Ns, tstep, tw); break;
-      }
+    switch (RR) {
+      case 8: stage_all<8>(a, b, ld, ncol, ax.nr[st], ax.ns[st], Ns, tw); break;
+      case 4: stage_all<4>(a, b, ld, ncol, ax.nr[st], ax.ns[st], Ns, tw); break;
+      case 2: stage_all<2>(a, b, ld, ncol, ax.nr[st], ax.ns[st], Ns, tw); break;
+      case 3: stage_all<3>(a, b, ld, ncol, ax.nr[st], ax.ns[st], Ns, tw); break;
+      default: stage_all<5>(a, b, ld, ncol, ax.nr[st], ax.ns[st], Ns, tw); break;
     }
     __syncthreads();
     C *t = a;
@@ -200,10 +245,10 @@ template <typename C> __device__ void load_twiddles(C *s_tw, const C *tw, int n)
   for (int i = threadIdx.x; i < n; i += blockDim.x) s_tw[i] = tw[i];
 }
 
-// Does any mode (h1, h2, h3) have |q| <= qmax?  The distance of h1 b1 + h2 b2
-// from the line along b3 is a lower bound of |q| over h3; the margin keeps the
-// test conservative under rounding.
-__device__ __forceinline__ bool line_reaches(const BinGeom &b, int h1, int h2) {
+// h3 interval [lo, hi] (indices h3 + hm2) of column (h1, h2) that can hold
+// modes with |q| <= qmax: |v + h3 b3|^2 <= qmax^2 for v = h1 b1 + h2 b2, widened
+// by one on each side against rounding; lo > hi when empty.
+__device__ __forceinline__ int2 h3_span(const BinGeom &b, int h1, int h2) {
   double v[3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) v[k] = (double)h1 * b.recip[k] + (double)h2 * b.recip[3 + k];
@@ -211,8 +256,14 @@ __device__ __forceinline__ bool line_reaches(const BinGeom &b, int h1, int h2) {
   const double vv = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
   const double vb = v[0] * b3[0] + v[1] * b3[1] + v[2] * b3[2];
   const double bb = b3[0] * b3[0] + b3[1] * b3[1] + b3[2] * b3[2];
-  const double d2 = vv - vb * vb / bb;
-  return d2 <= b.qmax * b.qmax * (1.0 + 1e-9) + 1e-12;
+  const double q2 = b.qmax * b.qmax * (1.0 + 1e-9) + 1e-12;
+  const double disc = vb * vb - bb * (vv - q2);
+  if (disc < 0.0) return make_int2(1, 0);
+  const double r = sqrt(disc);
+  const int hm2 = b.hm[2];
+  const int lo = max(-hm2, (int)floor((-vb - r) / bb) - 1);
+  const int hi = min(hm2, (int)ceil((-vb + r) / bb) + 1);
+  return make_int2(lo + hm2, hi + hm2);
 }
 
 // ---------------------------------------------------------------------------
@@ -223,41 +274,57 @@ __global__ void __launch_bounds__(256)
     k_fft_x(const R *__restrict__ grid, typename Cplx<R>::T *__restrict__ A1, FftAxis ax,
             int64_t npairs, int64_t pitch, int H1, const typename Cplx<R>::T *__restrict__ tw) {
   using C = typename Cplx<R>::T;
+  using V2 = typename Cplx<R>::T;  // two consecutive reals of a row
   extern __shared__ __align__(16) unsigned char smem[];
-  const int n = ax.n, ld = padi(n) + 1;
+  const int n = ax.n, ld = padi(n) + 1, nh = n >> 1;
   C *s_tw = reinterpret_cast<C *>(smem);
   C *a = s_tw + n;
-  C *b = a + (size_t)PC * ld;
+  C *b = a + PC * ld;
   load_twiddles(s_tw, tw, n);
   const int64_t pair0 = (int64_t)blockIdx.x * PC;
-  for (int e = threadIdx.x; e < PC * n; e += blockDim.x) {
-    const int p = e / n, i = e - p * n;
+#pragma unroll
+  for (int p = 0; p < PC; ++p) {
     const int64_t pr = pair0 + p;
-    C v;
-    v.x = R(0);
-    v.y = R(0);
-    if (pr < npairs) {
-      v.x = grid[(2 * pr) * pitch + i];
-      v.y = grid[(2 * pr + 1) * pitch + i];
+    const bool ok = pr < npairs;
+    const V2 *r0 = reinterpret_cast<const V2 *>(grid + (2 * pr) * pitch);
+    const V2 *r1 = reinterpret_cast<const V2 *>(grid + (2 * pr + 1) * pitch);
+    C *col = a + p * ld;
+    for (int i2 = threadIdx.x; i2 < nh; i2 += blockDim.x) {
+      V2 u, w;
+      u.x = u.y = w.x = w.y = R(0);
+      if (ok) {
+        u = r0[i2];
+        w = r1[i2];
+      }
+      C v0, v1;
+      v0.x = u.x;
+      v0.y = w.x;
+      v1.x = u.y;
+      v1.y = w.y;
+      col[padi(2 * i2)] = v0;
+      col[padi(2 * i2 + 1)] = v1;
     }
-    a[(size_t)p * ld + padi(i)] = v;
   }
   __syncthreads();
   const C *z = fft_cols(a, b, ax, PC, ld, s_tw);
   // X1[h] = (Z[h] + conj Z[n-h]) / 2, X2[h] = (Z[h] - conj Z[n-h]) / (2i)
-  for (int e = threadIdx.x; e < PC * H1; e += blockDim.x) {
-    const int p = e / H1, h = e - p * H1;
+#pragma unroll
+  for (int p = 0; p < PC; ++p) {
     const int64_t pr = pair0 + p;
-    if (pr >= npairs) continue;
-    const C zh = z[(size_t)p * ld + padi(h)];
-    const C zm = z[(size_t)p * ld + padi(h == 0 ? 0 : n - h)];
-    C x1, x2;
-    x1.x = R(0.5) * (zh.x + zm.x);
-    x1.y = R(0.5) * (zh.y - zm.y);
-    x2.x = R(0.5) * (zh.y + zm.y);
-    x2.y = R(0.5) * (zm.x - zh.x);
-    A1[(2 * pr) * H1 + h] = x1;
-    A1[(2 * pr + 1) * H1 + h] = x2;
+    if (pr >= npairs) break;
+    const C *zc = z + p * ld;
+    C *o0 = A1 + (2 * pr) * H1, *o1 = A1 + (2 * pr + 1) * H1;
+    for (int h = threadIdx.x; h < H1; h += blockDim.x) {
+      const C zh = zc[padi(h)];
+      const C zm = zc[padi(h == 0 ? 0 : n - h)];
+      C x1, x2;
+      x1.x = R(0.5) * (zh.x + zm.x);
+      x1.y = R(0.5) * (zh.y - zm.y);
+      x2.x = R(0.5) * (zh.y + zm.y);
+      x2.y = R(0.5) * (zm.x - zh.x);
+      o0[h] = x1;
+      o1[h] = x2;
+    }
   }
 }
 
@@ -267,45 +334,46 @@ __global__ void __launch_bounds__(256)
 template <typename R, int PC>
 __global__ void __launch_bounds__(256)
     k_fft_y(const typename Cplx<R>::T *__restrict__ A1, typename Cplx<R>::T *__restrict__ A2,
-            FftAxis ax, BinGeom bg, int H1, int M1,
+            FftAxis ax, BinGeom bg, int H1, int M1, const int2 *__restrict__ h2span,
             const typename Cplx<R>::T *__restrict__ tw) {
   using C = typename Cplx<R>::T;
   extern __shared__ __align__(16) unsigned char smem[];
   const int n = ax.n, ld = padi(n) + 1;
   C *s_tw = reinterpret_cast<C *>(smem);
   C *a = s_tw + n;
-  C *b = a + (size_t)PC * ld;
-  __shared__ unsigned char s_need[FFT_MAX_N];
+  C *b = a + PC * ld;
   const int nblk = (H1 + PC - 1) / PC;
   const int plane = blockIdx.x / nblk;
   const int h1b = (blockIdx.x - plane * nblk) * PC;
   load_twiddles(s_tw, tw, n);
-  const int hm1 = bg.hm[1];
-  // rows h2 whose whole h1 block misses the q sphere are never read
-  for (int j = threadIdx.x; j < M1; j += blockDim.x) {
-    bool need = false;
-    for (int c = 0; c < PC && h1b + c < H1; ++c) need = need || line_reaches(bg, h1b + c, j - hm1);
-    s_need[j] = need ? 1 : 0;
-  }
-  const C *src = A1 + (int64_t)plane * n * H1;
+  // rows h2 outside every column's span of the block are never read
+  int jlo = M1, jhi = -1;
+#pragma unroll
+  for (int c = 0; c < PC; ++c)
+    if (h1b + c < H1) {
+      const int2 sp = h2span[h1b + c];
+      jlo = min(jlo, sp.x);
+      jhi = max(jhi, sp.y);
+    }
+  const C *src = A1 + (int64_t)plane * n * H1 + h1b;
   for (int e = threadIdx.x; e < PC * n; e += blockDim.x) {
     const int y = e / PC, c = e - y * PC;
     C v;
     v.x = R(0);
     v.y = R(0);
-    if (h1b + c < H1) v = src[(int64_t)y * H1 + h1b + c];
-    a[(size_t)c * ld + padi(y)] = v;
+    if (h1b + c < H1) v = src[(int64_t)y * H1 + c];
+    a[c * ld + padi(y)] = v;
   }
   __syncthreads();
   const C *yv = fft_cols(a, b, ax, PC, ld, s_tw);
-  C *dst = A2 + (int64_t)plane * M1 * H1;
-  for (int e = threadIdx.x; e < PC * M1; e += blockDim.x) {
-    const int j = e / PC, c = e - j * PC;
-    const int h1 = h1b + c;
-    if (h1 >= H1 || !s_need[j]) continue;
-    const int h2 = j - hm1;
-    const int k = h2 >= 0 ? h2 : n + h2;
-    dst[(int64_t)j * H1 + h1] = yv[(size_t)c * ld + padi(k)];
+  const int hm1 = bg.hm[1];
+  C *dst = A2 + (int64_t)plane * M1 * H1 + h1b;
+  const int rows = jhi - jlo + 1;
+  for (int e = threadIdx.x; e < PC * rows; e += blockDim.x) {
+    const int jj = e / PC, c = e - jj * PC;
+    if (h1b + c >= H1) continue;
+    const int j = jlo + jj, h2 = j - hm1;
+    dst[(int64_t)j * H1 + c] = yv[c * ld + padi(h2 >= 0 ? h2 : n + h2)];
   }
 }
 
@@ -313,24 +381,26 @@ __global__ void __launch_bounds__(256)
 // Pass 3: columns along z, every transform, then the fused binning
 // ---------------------------------------------------------------------------
 template <typename R, int PC, int NT, bool SMEM, bool XR>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(FFT_Z_THREADS, 2)
     k_fft_z_bin(const typename Cplx<R>::T *__restrict__ A2, FftAxis ax, BinGeom b, int H1,
-                int M1, const typename Cplx<R>::T *__restrict__ tw, const R *__restrict__ inv1,
+                int M1, FastDiv M2_div, const int2 *__restrict__ h2span,
+                const typename Cplx<R>::T *__restrict__ tw, const R *__restrict__ inv1,
                 const R *__restrict__ inv2, const R *__restrict__ inv3,
                 const double *__restrict__ amp, const double *__restrict__ xcoef,
                 double *__restrict__ acc, double *__restrict__ gnum) {
   using C = typename Cplx<R>::T;
   constexpr int TM = NT > 0 ? NT : MAX_FAST_T;
   extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int2 s_span[PC];
   const int n = ax.n, ld = padi(n) + 1;
   const int ntr = NT > 0 ? NT : b.ntr;
   const int hm2 = b.hm[2], M2 = 2 * hm2 + 1;
   const int nhist = b.nquant * b.nq;
   C *s_tw = reinterpret_cast<C *>(smem);
   C *a = s_tw + n;
-  C *bb = a + (size_t)PC * ld;
-  C *res = bb + (size_t)PC * ld;  // [ntr][PC][M2]
-  double *s_hist = reinterpret_cast<double *>(res + (size_t)ntr * PC * M2);
+  C *bb = a + PC * ld;
+  C *res = bb + PC * ld;  // [ntr][PC][M2]
+  double *s_hist = reinterpret_cast<double *>(res + ntr * PC * M2);
   double *hist = SMEM ? s_hist : acc;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
   load_twiddles(s_tw, tw, n);
@@ -344,9 +414,15 @@ __global__ void __launch_bounds__(256)
   for (int it = blockIdx.x; it < items; it += gridDim.x) {
     const int j = it / nblk, h1b = (it - j * nblk) * PC;
     const int h2 = j - b.hm[1];
-    bool need = false;
-    for (int c = 0; c < PC && h1b + c < H1; ++c) need = need || line_reaches(b, h1b + c, h2);
-    if (!need) continue;  // uniform across the CTA
+    bool need = false;  // the same test as the y pass: uniform across the CTA
+#pragma unroll
+    for (int c = 0; c < PC; ++c)
+      if (h1b + c < H1) {
+        const int2 sp = h2span[h1b + c];
+        need = need || (j >= sp.x && j <= sp.y);
+      }
+    if (!need) continue;
+    if (tid < PC) s_span[tid] = h1b + tid < H1 ? h3_span(b, h1b + tid, h2) : make_int2(1, 0);
     for (int t = 0; t < ntr; ++t) {
       const C *src = A2 + t * tstride + (int64_t)j * H1 + h1b;
       for (int e = tid; e < PC * n; e += blockDim.x) {
@@ -355,30 +431,32 @@ __global__ void __launch_bounds__(256)
         v.x = R(0);
         v.y = R(0);
         if (h1b + c < H1) v = src[(int64_t)z * zstride + c];
-        a[(size_t)c * ld + padi(z)] = v;
+        a[c * ld + padi(z)] = v;
       }
       __syncthreads();
       const C *zv = fft_cols(a, bb, ax, PC, ld, s_tw);
-      C *r = res + (size_t)t * PC * M2;
+      C *r = res + t * PC * M2;
       for (int e = tid; e < PC * M2; e += blockDim.x) {
-        const int c = e / M2, i = e - c * M2;
+        const int c = fdiv(e, M2_div), i = e - c * M2;
         const int h3 = i - hm2;
-        r[e] = zv[(size_t)c * ld + padi(h3 >= 0 ? h3 : n + h3)];
+        r[e] = zv[c * ld + padi(h3 >= 0 ? h3 : n + h3)];
       }
       __syncthreads();
     }
-    // modes (h1b + c, h2, h3): lanes along h3
+    // modes (h1b + c, h2, h3) inside the column's span: lanes along h3
     const R d2 = inv2[abs(h2)];
     const int total = PC * M2;
     for (int e0 = warp * 32; e0 < total; e0 += nwarps * 32) {
       const int e = e0 + lane;
-      const int c = e / M2, i = e - c * M2;
+      const int c = fdiv(min(e, total - 1), M2_div), i = e - c * M2;
       const int h1 = h1b + c, h3 = i - hm2;
-      const bool inr = e < total && h1 < H1;
+      const int2 sp = s_span[c];
+      const bool inr = e < total && h1 < H1 && i >= sp.x && i <= sp.y;
+      if (__ballot_sync(FULL, inr) == 0u) continue;
       C v[TM];
 #pragma unroll
       for (int t = 0; t < TM; ++t)
-        if (t < ntr && inr) v[t] = res[(size_t)t * PC * M2 + e];
+        if (t < ntr && inr) v[t] = res[t * PC * M2 + e];
       double crow[3];
       row_const(b, h2, h3, crow);
       const R dec = inr ? inv1[h1] * (d2 * inv3[abs(h3)]) : R(0);
@@ -387,7 +465,7 @@ __global__ void __launch_bounds__(256)
       bin_mode<R, TM, XR>(b, ntr, inr, h1, h2, h3, crow, v, dec, amp, xcoef, hist, gnum, gidx,
                           lane);
     }
-    __syncthreads();  // res is rewritten by the next item
+    __syncthreads();  // res and s_span are rewritten by the next item
   }
   if (SMEM) {
     __syncthreads();
@@ -428,13 +506,15 @@ cudaError_t launch_z_xr(const FftPlan3 &f, const void *A2, const BinGeom &b, con
   if (b.xray) {
     e = allow_smem(k_fft_z_bin<R, PC, NT, SMEM, true>, sm);
     if (e != cudaSuccess) return e;
-    k_fft_z_bin<R, PC, NT, SMEM, true><<<f.grid3, 256, sm, s>>>(
-        (const C *)A2, f.ax[2], b, f.H1, f.M1, (const C *)f.tw[2], i1, i2, i3, amp, xc, acc, gnum);
+    k_fft_z_bin<R, PC, NT, SMEM, true><<<f.grid3, FFT_Z_THREADS, sm, s>>>(
+        (const C *)A2, f.ax[2], b, f.H1, f.M1, f.M2_div, f.h2span, (const C *)f.tw[2], i1, i2,
+        i3, amp, xc, acc, gnum);
   } else {
     e = allow_smem(k_fft_z_bin<R, PC, NT, SMEM, false>, sm);
     if (e != cudaSuccess) return e;
-    k_fft_z_bin<R, PC, NT, SMEM, false><<<f.grid3, 256, sm, s>>>(
-        (const C *)A2, f.ax[2], b, f.H1, f.M1, (const C *)f.tw[2], i1, i2, i3, amp, xc, acc, gnum);
+    k_fft_z_bin<R, PC, NT, SMEM, false><<<f.grid3, FFT_Z_THREADS, sm, s>>>(
+        (const C *)A2, f.ax[2], b, f.H1, f.M1, f.M2_div, f.h2span, (const C *)f.tw[2], i1, i2,
+        i3, amp, xc, acc, gnum);
   }
   return cudaGetLastError();
 }
@@ -479,21 +559,22 @@ cudaError_t launch_xy_pc(const FftPlan3 &f, const void *grid, void *A1, void *A2
   if (e != cudaSuccess) return e;
   const int64_t g2 = (int64_t)b.ntr * b.nf[2] * ((f.H1 + PC - 1) / PC);
   k_fft_y<R, PC><<<(unsigned)g2, 256, sm, s>>>((const C *)A1, (C *)A2, f.ax[1], b, f.H1, f.M1,
-                                                (const C *)f.tw[1]);
+                                                f.h2span, (const C *)f.tw[1]);
   return cudaGetLastError();
 }
 
 }  // namespace
 
 int fft_columns_per_cta(bool fp64) { return fp64 ? 2 : 4; }
+int fft_z_columns_per_cta(bool fp64) { return fp64 ? 2 : 4; }
 
 size_t fft_pass_smem(const FftPlan3 &f, int pass, bool fp64, int ntr, int nquant, int nq) {
   const int pc = fft_columns_per_cta(fp64);
   if (pass < 2)
     return fp64 ? pass12_smem<double>(f.ax[pass].n, pc) : pass12_smem<float>(f.ax[pass].n, pc);
   const size_t hist = f.hist_smem ? (size_t)nquant * nq * sizeof(double) : 0;
-  return fp64 ? pass3_smem<double>(f.ax[2].n, pc, ntr, f.M2, hist)
-              : pass3_smem<float>(f.ax[2].n, pc, ntr, f.M2, hist);
+  return fp64 ? pass3_smem<double>(f.ax[2].n, fft_z_columns_per_cta(fp64), ntr, f.M2, hist)
+              : pass3_smem<float>(f.ax[2].n, fft_z_columns_per_cta(fp64), ntr, f.M2, hist);
 }
 
 template <typename R>

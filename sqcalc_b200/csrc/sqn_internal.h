@@ -103,20 +103,39 @@ cudaError_t spread_set_attributes();
 // Pruned three-pass FFT fused with the binning (sqn_fft.cu).
 constexpr int FFT_MAX_STAGES = 16;
 constexpr int FFT_MAX_N = 4096;   // longest axis the fused passes take
+constexpr int FFT_Z_THREADS = 512;
+// Exact x / d for x * d < 2^32 by one multiply-high: m = ceil(2^32 / d), d > 1
+// (Granlund and Montgomery, PLDI 1994); d == 1 is passed through.
+struct FastDiv {
+  uint32_t d, m;
+};
+inline FastDiv make_fastdiv(uint32_t d) {
+  FastDiv f;
+  f.d = d;
+  f.m = d > 1 ? (uint32_t)((((uint64_t)1 << 32) + d - 1) / d) : 0u;
+  return f;
+}
 struct FftAxis {
   int n;                          // transform length (2, 3, 5-smooth)
   int nst;                        // radix stages
   int radix[FFT_MAX_STAGES];      // 8, 4, 2, 3 or 5 each
+  FastDiv nr[FFT_MAX_STAGES];     // n / radix of each stage
+  FastDiv ns[FFT_MAX_STAGES];     // product of the earlier radices
+  FastDiv n_div;                  // n
 };
 struct FftPlan3 {
   FftAxis ax[3];
   const void *tw[3];              // exp(-2 pi i k / n_d), k < n_d, complex R
   int H1;                         // hm0 + 1 kept x modes (h1 >= 0)
   int M1, M2;                     // 2 hm1 + 1, 2 hm2 + 1
+  FastDiv H1_div, M2_div;
+  const int2 *h2span;             // per h1: [lo, hi] of h2 + hm1 whose line along b3
+                                  // reaches |q| <= qmax (lo > hi: none)
   int grid3;                      // persistent CTAs of the z pass
   bool hist_smem;                 // shell histograms in shared memory
 };
 int fft_columns_per_cta(bool fp64);
+int fft_z_columns_per_cta(bool fp64);
 size_t fft_pass_smem(const FftPlan3 &f, int pass, bool fp64, int ntr, int nquant, int nq);
 template <typename R>
 cudaError_t launch_fft_xy(const FftPlan3 &f, const void *grid, void *A1, void *A2,
