@@ -77,6 +77,9 @@ def workload_config(extra=None):
 # clocks during the timed region
 # ---------------------------------------------------------------------------
 class ClockSampler:
+    """nvidia-smi samples every 50 ms with their arrival time; started before
+    the warm-up so that it is running when the timed region begins, and
+    summarised over the samples that arrived inside that region."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -85,12 +88,13 @@ class ClockSampler:
         self.idx = device_index
         self.proc = None
         self.lines = []
+        self.window = None
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + self.FIELDS,
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -100,10 +104,19 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.monotonic(), line.strip()))
+
+    def wait_first(self, timeout=5.0):
+        t0 = time.monotonic()
+        while self.proc is not None and not self.lines and time.monotonic() - t0 < timeout:
+            time.sleep(0.01)
+
+    def mark(self, t0, t1):
+        self.window = (t0, t1)
 
     def __exit__(self, *exc):
         if self.proc is not None:
+            time.sleep(0.06)  # one more sample after the region
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -113,7 +126,12 @@ class ClockSampler:
     def summary(self):
         sm, mx, reasons = [], [], set()
         names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        for line in self.lines:
+        lines = self.lines
+        if self.window is not None:
+            t0, t1 = self.window
+            inside = [x for x in lines if t0 <= x[0] <= t1 + 0.05]
+            lines = inside if inside else lines[-1:]
+        for _, line in lines:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -421,12 +439,15 @@ def run_ours(args, rank, world, local_rank):
     launches0 = plan.launch_count()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local_rank) as clk:
+        clk.wait_first()
         t_wall = time.perf_counter()
+        tm0 = time.monotonic()
         ev0.record(stream)
         for f in range(W, W + K):
             plan.accumulate((base + f * fbytes, 1), where=_lib.DEVICE)
         ev1.record(stream)
         torch.cuda.synchronize()
+        clk.mark(tm0, time.monotonic())
         t_wall = time.perf_counter() - t_wall
     launches = plan.launch_count() - launches0
     info = plan.info

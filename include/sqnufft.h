@@ -208,6 +208,43 @@ int sqn_sq_grad(sqn_plan *plan, const double *pos, int32_t where, const double *
 /* Number of this library's own kernel launches so far (cuFFT's not counted). */
 int64_t sqn_launch_count(const sqn_plan *plan);
 
+/* ---- cuFINUFFT-shaped type-1 NUFFT ----------------------------------------
+ * fk[t][k] = sum_j c[t][j] exp(iflag i (k1 x_j + k2 y_j + k3 z_j)) for
+ * k_d in [-N_d/2, (N_d-1)/2], the type-1, dim-3 transform of
+ * cufinufft[f]_makeplan / setpts / execute / destroy
+ * (external/finufft/include/cufinufft.h, bound by sqcalc in
+ * src/sqc_cufinufft.f90:183-259): the same arguments and life cycle, so the
+ * library can stand in for those calls literally and be compared with them
+ * transform for transform.  type must be 1 and dim 3 (else
+ * SQN_ERR_NOT_SUPPORTED); n_modes[3] = (N1, N2, N3); iflag >= 0 means +1;
+ * ntransf transforms share the points; tol as cuFINUFFT's tol.
+ * setpts: M points, device arrays x, y, z (period 2 pi, any real value), sorted
+ * once per call.  execute: device arrays c [ntransf][M] and fk
+ * [ntransf][N3][N2][N1] of interleaved (re, im) doubles (floats for the f
+ * variants), modes in opts.modeord order (0: -N/2 first, 1: 0 first).
+ * execute is synchronous on the plan's stream. */
+typedef struct sqn_type1_s sqn_type1_plan;
+typedef struct sqn_type1_opts {
+  int32_t gpu_device_id; /* cufinufft_opts.gpu_device_id */
+  int32_t modeord;       /* cufinufft_opts.modeord: 0 CMCL order, 1 FFT order */
+  double upsampfac;      /* 0: chosen by the plan; else > 1 */
+  void *gpu_stream;      /* cufinufft_opts.gpu_stream; NULL: a plan-owned stream */
+} sqn_type1_opts;
+void sqn_type1_default_opts(sqn_type1_opts *opts);
+int sqn_type1_makeplan(int32_t type, int32_t dim, const int64_t *n_modes, int32_t iflag,
+                       int32_t ntransf, double tol, sqn_type1_plan **plan,
+                       const sqn_type1_opts *opts);
+int sqn_type1f_makeplan(int32_t type, int32_t dim, const int64_t *n_modes, int32_t iflag,
+                        int32_t ntransf, float tol, sqn_type1_plan **plan,
+                        const sqn_type1_opts *opts);
+int sqn_type1_setpts(sqn_type1_plan *plan, int64_t M, const double *d_x, const double *d_y,
+                     const double *d_z);
+int sqn_type1f_setpts(sqn_type1_plan *plan, int64_t M, const float *d_x, const float *d_y,
+                      const float *d_z);
+int sqn_type1_execute(sqn_type1_plan *plan, const double *d_c, double *d_fk);
+int sqn_type1f_execute(sqn_type1_plan *plan, const float *d_c, float *d_fk);
+int sqn_type1_destroy(sqn_type1_plan *plan);
+
 /* ---- Batches of independent systems ------------------------------------
  * Many uneven systems (each its own cell, atoms, types and grid) whose frames
  * are accumulated together: one plan per system, and one frame of EVERY system

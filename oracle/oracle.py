@@ -80,6 +80,9 @@ def lib():
                                         ctypes.c_void_p, _dp, _dp]
         L.sqo_direct_grad.argtypes = [ctypes.c_int64, _dp, _dp, _dp, _dp, ctypes.c_int64, _dp,
                                       _ip, _dp, _dp]
+        L.sqo_dirft3d1.argtypes = [ctypes.c_int64, _dp, _dp, _dp, _dp, ctypes.c_int32,
+                                   ctypes.c_int32, ctypes.c_int64, ctypes.c_int64,
+                                   ctypes.c_int64, ctypes.c_int32, _dp]
         _lib = L
     return _lib
 
@@ -352,3 +355,15 @@ def direct_grad(pos, strength, cell, origin, grid: Grid, wgt):
                           _c(grid.qvec, np.float64).reshape(-1), _c(grid.shell, np.int32),
                           _c(wgt, np.float64), out)
     return out.reshape(-1, 3)
+
+
+def dirft3d1(x, y, z, c, n_modes, iflag=1, modeord=0):
+    """Direct type-1 sum; c (ntr, M) complex -> fk (ntr, N3, N2, N1) complex."""
+    c = np.atleast_2d(np.asarray(c, dtype=np.complex128))
+    ntr, M = c.shape
+    N1, N2, N3 = (int(n) for n in n_modes)
+    cf = np.ascontiguousarray(c).view(np.float64).reshape(-1)
+    out = np.zeros(2 * ntr * N1 * N2 * N3)
+    lib().sqo_dirft3d1(M, _c(x, np.float64), _c(y, np.float64), _c(z, np.float64), cf, ntr,
+                       int(iflag), N1, N2, N3, int(modeord), out)
+    return out.view(np.complex128).reshape(ntr, N3, N2, N1)

@@ -258,3 +258,47 @@ void sqo_bin_halfspace(const double *G, int32_t ntr, const int64_t *nf, const in
   free(lnum);
   free(lpar);
 }
+
+/*
+ * Direct type-1 sum, the check of the library's cuFINUFFT-shaped entry points:
+ *   fk[t][k] = sum_j c[t][j] exp(iflag i (k1 x_j + k2 y_j + k3 z_j))
+ * for k_d in [-N_d/2, (N_d-1)/2], written in CMCL order (modeord 0, k1 fastest
+ * from -N1/2) or FFT order (modeord 1, k = 0 first), as the direct transform
+ * FINUFFT's own tests compare against (external/finufft/test/utils/
+ * dirft3d.hpp:13-20).  c and fk hold interleaved (re, im) pairs; FP64.
+ */
+void sqo_dirft3d1(int64_t M, const double *x, const double *y, const double *z,
+                  const double *c, int32_t ntr, int32_t iflag, int64_t N1, int64_t N2,
+                  int64_t N3, int32_t modeord, double *fk) {
+  const int64_t nm = N1 * N2 * N3;
+  const double sg = iflag >= 0 ? 1.0 : -1.0;
+#pragma omp parallel for schedule(static)
+  for (int64_t m = 0; m < nm; ++m) {
+    int64_t r = m;
+    const int64_t i1 = r % N1;
+    r /= N1;
+    const int64_t i2 = r % N2, i3 = r / N2;
+    int64_t k1, k2, k3;
+    if (modeord == 0) {
+      k1 = i1 - N1 / 2;
+      k2 = i2 - N2 / 2;
+      k3 = i3 - N3 / 2;
+    } else {
+      k1 = i1 < (N1 + 1) / 2 ? i1 : i1 - N1;
+      k2 = i2 < (N2 + 1) / 2 ? i2 : i2 - N2;
+      k3 = i3 < (N3 + 1) / 2 ? i3 : i3 - N3;
+    }
+    for (int32_t t = 0; t < ntr; ++t) {
+      double sre = 0.0, sim = 0.0;
+      for (int64_t j = 0; j < M; ++j) {
+        const double ph = sg * ((double)k1 * x[j] + (double)k2 * y[j] + (double)k3 * z[j]);
+        const double cr = cos(ph), si = sin(ph);
+        const double are = c[2 * (t * M + j)], aim = c[2 * (t * M + j) + 1];
+        sre += are * cr - aim * si;
+        sim += are * si + aim * cr;
+      }
+      fk[2 * (t * nm + m)] = sre;
+      fk[2 * (t * nm + m) + 1] = sim;
+    }
+  }
+}

@@ -33,7 +33,9 @@ EXPORTS = (
     "sqn_peek_num_async", "sqn_finalize", "sqn_reset", "sqn_stage_times", "sqn_launch_count",
     "sqn_plan_destroy", "sqn_spread_frame_noalloc", "sqn_sq_grad", "sqn_accumulator_view",
     "sqn_set_frame_count", "sqn_batch_create", "sqn_batch_accumulate", "sqn_batch_sync",
-    "sqn_batch_plan", "sqn_batch_graph_launches", "sqn_batch_destroy",
+    "sqn_batch_plan", "sqn_batch_graph_launches", "sqn_batch_destroy", "sqn_type1_default_opts",
+    "sqn_type1_makeplan", "sqn_type1f_makeplan", "sqn_type1_setpts", "sqn_type1f_setpts",
+    "sqn_type1_execute", "sqn_type1f_execute", "sqn_type1_destroy",
 )
 ERR_SCRATCH_LIMIT = 49
 NOALLOC_SCRATCH_BYTES = 32 * 1024 * 1024
@@ -87,6 +89,15 @@ class SqnInfo(ctypes.Structure):
     ]
 
 
+class Type1Opts(ctypes.Structure):
+    _fields_ = [
+        ("gpu_device_id", ctypes.c_int32),
+        ("modeord", ctypes.c_int32),
+        ("upsampfac", ctypes.c_double),
+        ("gpu_stream", ctypes.c_void_p),
+    ]
+
+
 class SqnError(RuntimeError):
     def __init__(self, code, where=""):
         self.code = int(code)
@@ -134,6 +145,19 @@ def load():
     L.sqn_batch_graph_launches.argtypes = [vp]
     L.sqn_batch_graph_launches.restype = i64
     L.sqn_batch_destroy.argtypes = [vp]
+    L.sqn_type1_default_opts.argtypes = [ctypes.POINTER(Type1Opts)]
+    L.sqn_type1_default_opts.restype = None
+    L.sqn_type1_makeplan.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(i64),
+                                     ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
+                                     ctypes.POINTER(vp), ctypes.POINTER(Type1Opts)]
+    L.sqn_type1f_makeplan.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(i64),
+                                      ctypes.c_int32, ctypes.c_int32, ctypes.c_float,
+                                      ctypes.POINTER(vp), ctypes.POINTER(Type1Opts)]
+    for name in ("sqn_type1_setpts", "sqn_type1f_setpts"):
+        getattr(L, name).argtypes = [vp, i64, vp, vp, vp]
+    for name in ("sqn_type1_execute", "sqn_type1f_execute"):
+        getattr(L, name).argtypes = [vp, vp, vp]
+    L.sqn_type1_destroy.argtypes = [vp]
     L.sqn_spread_frame_noalloc.argtypes = [vp, i64, vp, ctypes.c_int32, vp, vp, vp, vp,
                                            ctypes.c_int32, ctypes.c_double, vp, vp]
     if L.sqn_abi_version() != ABI_VERSION:
@@ -403,6 +427,74 @@ class Batch:
             for v in self.plans:
                 v._h = ctypes.c_void_p()
             self._L.sqn_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Type1Plan:
+    """sqn_type1_*: cuFINUFFT-shaped type-1 3D NUFFT on torch CUDA tensors.
+
+    fk[t, k3, k2, k1] = sum_j c[t, j] exp(iflag i (k1 x_j + k2 y_j + k3 z_j)); the
+    plan runs on torch's current CUDA stream unless a stream handle is given."""
+
+    def __init__(self, n_modes, iflag=1, ntransf=1, eps=1e-6, precision=PREC_DOUBLE,
+                 modeord=0, upsampfac=0.0, device=0, stream=None, nufft_type=1, dim=3):
+        import torch
+        L = load()
+        self._L = L
+        self.fp64 = precision == PREC_DOUBLE
+        self.n_modes = tuple(int(n) for n in n_modes)
+        self.ntransf = int(ntransf)
+        o = Type1Opts()
+        L.sqn_type1_default_opts(ctypes.byref(o))
+        o.gpu_device_id = int(device)
+        o.modeord = int(modeord)
+        o.upsampfac = float(upsampfac)
+        o.gpu_stream = (stream if stream is not None
+                        else torch.cuda.current_stream(device).cuda_stream)
+        nm = (ctypes.c_int64 * 3)(*self.n_modes)
+        h = ctypes.c_void_p()
+        make = L.sqn_type1_makeplan if self.fp64 else L.sqn_type1f_makeplan
+        self.status = check(make(int(nufft_type), int(dim), nm, int(iflag), self.ntransf,
+                                 float(eps), ctypes.byref(h), ctypes.byref(o)),
+                            "sqn_type1_makeplan")
+        self._h = h
+        self._pts = None
+
+    def setpts(self, x, y, z):
+        import torch
+        dt = torch.float64 if self.fp64 else torch.float32
+        pts = [t.to(dtype=dt).contiguous() for t in (x, y, z)]
+        self._pts = pts  # kept alive until the next setpts
+        f = self._L.sqn_type1_setpts if self.fp64 else self._L.sqn_type1f_setpts
+        check(f(self._h, int(pts[0].numel()), *(ctypes.c_void_p(t.data_ptr()) for t in pts)),
+              "sqn_type1_setpts")
+
+    def execute(self, c):
+        import torch
+        ct = torch.complex128 if self.fp64 else torch.complex64
+        c = c.to(dtype=ct).contiguous()
+        N1, N2, N3 = self.n_modes
+        fk = torch.empty((self.ntransf, N3, N2, N1), dtype=ct, device=c.device)
+        f = self._L.sqn_type1_execute if self.fp64 else self._L.sqn_type1f_execute
+        check(f(self._h, ctypes.c_void_p(c.data_ptr()), ctypes.c_void_p(fk.data_ptr())),
+              "sqn_type1_execute")
+        return fk
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            self._L.sqn_type1_destroy(self._h)
             self._h = ctypes.c_void_p()
 
     def __enter__(self):

@@ -23,8 +23,12 @@
 using namespace sqn;
 
 namespace {
-
 constexpr int64_t kRefMaxGridModes = 400000000LL;  // src/sqc_structure_factor.f90:63-64
+}  // namespace
+
+// Host math shared with the type-1 entry points (sqn_type1.cu).
+namespace sqn {
+namespace hostmath {
 
 // ---------------------------------------------------------------------------
 // Host math
@@ -214,7 +218,9 @@ double xray_f_host(const double *c, double q) {
   return f;
 }
 
-}  // namespace
+}  // namespace hostmath
+}  // namespace sqn
+using namespace sqn::hostmath;
 
 // ---------------------------------------------------------------------------
 // Plan

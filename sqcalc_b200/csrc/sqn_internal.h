@@ -5,6 +5,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include <vector>
+
 namespace sqn {
 
 // Spread tile in fine-grid cells (x fastest).  A CTA of 16 warps owns one
@@ -144,6 +146,23 @@ template <typename R>
 cudaError_t launch_fft_z_bin(const FftPlan3 &f, const void *A2, const BinGeom &b, const R *inv1,
                              const R *inv2, const R *inv3, const double *amp,
                              const double *xcoef, double *acc, double *gnum, cudaStream_t s);
+
+// Host math (sqn_api.cu).
+namespace hostmath {
+int64_t next235even(int64_t n);
+int es_width(double eps, double sigma);
+double es_beta(int w, double sigma);
+bool choose_fine_grid(const int *modes, double eps, double sigma_req, int w_req, int wcap,
+                      int64_t *nf, int *w_out, double *sigma_out);
+// phihat(k) of the ES kernel on an nf-point grid for k = 0 .. kmax
+std::vector<double> kernel_ft(int64_t nf, int w, double beta, int kmax);
+}  // namespace hostmath
+
+// Spread with a weight per point instead of per species (one grid; the
+// weights are in bin-sorted record order).
+template <typename R>
+cudaError_t launch_spread_pw(const R *recs, const int *starts, const FrameGeom &g,
+                             const R *wsorted, R *grid, cudaStream_t s);
 
 // Adjoint (sqn_adjoint.cu).
 struct Recip {

@@ -148,7 +148,8 @@ __device__ __forceinline__ bool cyc_meet(int r, int w, int b, int len, int n) {
 template <typename R, int NT>
 __global__ void __launch_bounds__(SPREAD_THREADS, (sizeof(R) == 4 || NT == 1) ? 2 : 1)
     k_spread(const R *__restrict__ recs, const int *__restrict__ starts, FrameGeom g,
-             const R *__restrict__ strength, R *__restrict__ grid) {
+             const R *__restrict__ strength, R *__restrict__ grid,
+             const R *__restrict__ ptw = nullptr) {
   constexpr int TM = NT > 0 ? NT : MAX_FAST_T;
   const int chunk = g.chunk;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -267,7 +268,8 @@ __global__ void __launch_bounds__(SPREAD_THREADS, (sizeof(R) == 4 || NT == 1) ? 
       if (rz < 0) rz += g.nf[2];
       keep = (rx < tx || rx + w > g.nf[0]) && (ry < ty || ry + w > g.nf[1]) &&
              (rz < tz || rz + w > g.nf[2]);
-      meta = make_int4(rx, ry, rz, (int)(packed >> 24));
+      // with per-point weights (one grid) the slot carries the record index
+      meta = make_int4(rx, ry, rz, ptw ? ridx : (int)(packed >> 24));
     }
     // Counting sort of the kept points by transform (order kept within one),
     // so that each transform's points form one contiguous range.
@@ -329,7 +331,7 @@ __global__ void __launch_bounds__(SPREAD_THREADS, (sizeof(R) == 4 || NT == 1) ? 
       const int lim = d == 0 ? tx : (d == 1 ? ty : tz);
       const int n = g.nf[d];
       const R off = s_off[(size_t)p * 4 + 1 + d];
-      const R sc = d == 2 ? strength[m.w] : R(1);
+      const R sc = d == 2 ? (ptw ? ptw[m.w] : strength[m.w]) : R(1);
       R *row = s_rows + (size_t)p * SPREAD_ROW + (d == 0 ? 0 : (d == 1 ? TILE_X : TILE_X + TILE_Y));
       for (int j = 0; j < len; j += 4) store_rec(row + j, R(0), R(0), R(0), R(0));
       // support cell k sits at tile cell rel + k, cyclically (rel in [0, n))
@@ -592,6 +594,16 @@ cudaError_t launch_spread(const R *recs, const int *starts, const FrameGeom &g,
   return cudaGetLastError();
 }
 
+template <typename R>
+cudaError_t launch_spread_pw(const R *recs, const int *starts, const FrameGeom &g,
+                             const R *wsorted, R *grid, cudaStream_t s) {
+  if (g.ntr != 1 || !wsorted) return cudaErrorInvalidValue;
+  const size_t sm = spread_smem_bytes(g.chunk, sizeof(R) == 8);
+  k_spread<R, 1><<<(unsigned)g.ntiles, SPREAD_THREADS, sm, s>>>(recs, starts, g, nullptr, grid,
+                                                                wsorted);
+  return cudaGetLastError();
+}
+
 template <typename R, int NT, bool XR>
 static cudaError_t bin_dispatch_xr(const int4 *rows, int nrows, const void *G, const BinGeom &b,
                                    const R *i1, const R *i2, const R *i3, const double *amp,
@@ -662,6 +674,10 @@ template cudaError_t launch_spread<float>(const float *, const int *, const Fram
                                           const float *, float *, cudaStream_t);
 template cudaError_t launch_spread<double>(const double *, const int *, const FrameGeom &,
                                            const double *, double *, cudaStream_t);
+template cudaError_t launch_spread_pw<float>(const float *, const int *, const FrameGeom &,
+                                             const float *, float *, cudaStream_t);
+template cudaError_t launch_spread_pw<double>(const double *, const int *, const FrameGeom &,
+                                              const double *, double *, cudaStream_t);
 template cudaError_t launch_bin<float>(const int4 *, int, const void *, const BinGeom &,
                                        const float *, const float *, const float *,
                                        const double *, const double *, double *, double *, int,
