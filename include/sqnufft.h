@@ -52,7 +52,8 @@ enum {
   SQN_ERR_CUFFT = 46,               /* cuFFT plan or execution failure */
   SQN_ERR_TIMEOUT = 47,             /* a bounded device wait gave up */
   SQN_ERR_NOT_SUPPORTED = 48,
-  SQN_ERR_SCRATCH_LIMIT = 49        /* request does not fit the fixed no-alloc scratch */
+  SQN_ERR_SCRATCH_LIMIT = 49,       /* request does not fit the fixed no-alloc scratch */
+  SQN_ERR_DUMP = 50                 /* dump file unreadable or malformed (sqn_dump_last_error) */
 };
 
 enum { SQN_WEIGHT_UNIT = 0, SQN_WEIGHT_NEUTRON = 1, SQN_WEIGHT_XRAY = 2 };
@@ -117,6 +118,7 @@ typedef struct sqn_plan_info {
   int64_t tile[3];          /* spread tile in fine-grid cells */
   int32_t fused_fft;        /* 1: pruned FFT passes fused with the binning; 0: cuFFT + bin kernel */
   int32_t reserved;
+  int64_t natoms;           /* atoms per frame */
 } sqn_plan_info;
 
 typedef struct sqn_plan_s sqn_plan;
@@ -244,6 +246,39 @@ int sqn_type1f_setpts(sqn_type1_plan *plan, int64_t M, const float *d_x, const f
 int sqn_type1_execute(sqn_type1_plan *plan, const double *d_c, double *d_fk);
 int sqn_type1f_execute(sqn_type1_plan *plan, const float *d_c, float *d_fk);
 int sqn_type1_destroy(sqn_type1_plan *plan);
+
+/* ---- LAMMPS dump ingest ----------------------------------------------------
+ * A multithreaded reader of LAMMPS text dumps, the counterpart of
+ * lammps_next_frame / resolve_columns (src/sqc_dump.f90:162-313, :502-552):
+ * frames of ITEM: TIMESTEP / NUMBER OF ATOMS / BOX BOUNDS [xy xz yz] / ATOMS with
+ * the columns id, type and x|xu, y|yu, z|zu in file order.  The file is
+ * memory-mapped and each frame's atom lines are parsed by nthreads threads
+ * (<= 0: all cores) with correctly rounded decimal conversion.
+ * sqn_dump_next: fills natoms, timestep, bounds[9] (the three bound rows
+ * lo hi [tilt]; may be NULL), pos [natoms][3], type_id [natoms] and ids [natoms]
+ * (may be NULL) for at most capacity atoms; *natoms = 0 at the end of the file
+ * (status SQN_OK); a frame larger than capacity returns SQN_ERR_INVALID_ARGUMENT
+ * with *natoms set and the frame not consumed; a malformed frame returns
+ * SQN_ERR_DUMP and sqn_dump_last_error gives the reference's ierr (4 structure or
+ * TIMESTEP, 5 atom count, 6 box row, 7 ATOMS before its header, 8 atom line,
+ * 9 missing column).
+ * sqn_accumulate_dump: up to max_frames (< 0: all) frames of the dump into the
+ * plan, parsing frame f + 1 on a host thread into a second pinned buffer while
+ * the plan uploads and transforms frame f; every frame must have the plan's atom
+ * count (else SQN_ERR_NUM_NU_PTS_INVALID; the plan's type ids stand, as the
+ * reference's species set up once) and the box bounds ref_bounds[9] (NULL: those
+ * of the first frame read) to 1e-6 relative (else SQN_ERR_DUMP with
+ * sqn_dump_last_error 10, the reference driver's "box changes" stop); syncs
+ * before returning. */
+typedef struct sqn_dump_s sqn_dump;
+int sqn_dump_open(const char *path, int32_t nthreads, sqn_dump **dump);
+int sqn_dump_next(sqn_dump *dump, int64_t capacity, int64_t *natoms, int64_t *timestep,
+                  double *bounds, double *pos, int32_t *type_id, int64_t *ids);
+int sqn_dump_last_error(const sqn_dump *dump);
+int sqn_dump_rewind(sqn_dump *dump);
+int sqn_dump_close(sqn_dump *dump);
+int sqn_accumulate_dump(sqn_plan *plan, sqn_dump *dump, int64_t max_frames,
+                        const double *ref_bounds, int64_t *frames_done);
 
 /* ---- Batches of independent systems ------------------------------------
  * Many uneven systems (each its own cell, atoms, types and grid) whose frames

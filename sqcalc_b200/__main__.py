@@ -8,12 +8,14 @@ Mirrors the option surface and exit codes of ``sqcalc static --device gpu``
 from __future__ import annotations
 
 import argparse
+import os
 import sys
 import time
 
-import numpy as np
 
-from .dump import DumpError, read_frames
+from . import _lib
+from .cell import Cell
+from .dump import Frame
 from .static import GpuStructureFactor, SqcalcError
 from .weights import MappingError, WeightScheme
 
@@ -60,13 +62,21 @@ def main(argv=None):
         scheme = WeightScheme.from_options(a.weight, a.mapping)
     except MappingError as e:
         _die(2, str(e))
-    frames = read_frames(a.input)
-    try:
-        first = next(frames)
-    except FileNotFoundError:
+    # The library's multithreaded reader: the first frame configures the
+    # method, the rest stream through sqn_accumulate_dump (the parse of one
+    # frame overlaps the upload and transform of the previous one).
+    if not os.path.exists(a.input):
         _die(4, 'cannot open dump file "%s"' % a.input)
-    except (DumpError, StopIteration) as e:
+    try:
+        reader = _lib.DumpReader(a.input, nthreads=a.threads)
+        head = reader.next()
+    except _lib.SqnError as e:
         _die(5, 'no complete frame found in "%s" (%s)' % (a.input, e))
+    if head is None:
+        _die(5, 'no complete frame found in "%s"' % a.input)
+    ts, natoms, bounds, pos, types, ids = head
+    first = Frame(natoms, ts, pos, types, ids,
+                  Cell.from_bounds(bounds[:, 0], bounds[:, 1], bounds[:, 2]))
     method = GpuStructureFactor(norm=a.norm, nq=a.nq, qmin=a.qmin, qmax=a.qmax, eps=a.eps,
                                 want_grid=a.grid is not None, partials=a.partials,
                                 faber_ziman=a.faber_ziman, precision=a.precision,
@@ -75,22 +85,19 @@ def main(argv=None):
         method.configure(first, scheme)
     except SqcalcError as e:
         _die(6, str(e))
-    ref_a = first.cell.a.copy()
     t0 = time.time()
-    frame, n = first, 0
-    while True:
-        if frame.natoms != first.natoms:
+    method.accumulate_frame(first)
+    n = 1
+    try:
+        n += method.plan.accumulate_dump(reader, ref_bounds=bounds.reshape(-1))
+    except _lib.SqnError as e:
+        if e.code == _lib.ERR_NUM_NU_PTS_INVALID:
             _die(8, "number of atoms changes between frames")
-        if np.max(np.abs(frame.cell.a - ref_a)) > 1e-6 * max(1.0, float(np.max(np.abs(ref_a)))):
+        code = reader.last_error()
+        if code == 10:
             _die(9, "the simulation box changes between frames")
-        method.accumulate_frame(frame)
-        n += 1
-        try:
-            frame = next(frames)
-        except StopIteration:
-            break
-        except DumpError as e:
-            _die(7, "malformed dump (reader error %d): %s" % (e.code, e))
+        _die(7, "malformed dump (reader error %d): %s" % (code, e))
+    reader.close()
     method.plan.sync()
     if not a.quiet:
         sys.stderr.write("  frames     : %d in %.3f s\n" % (n, time.time() - t0))

@@ -35,9 +35,14 @@ EXPORTS = (
     "sqn_set_frame_count", "sqn_batch_create", "sqn_batch_accumulate", "sqn_batch_sync",
     "sqn_batch_plan", "sqn_batch_graph_launches", "sqn_batch_destroy", "sqn_type1_default_opts",
     "sqn_type1_makeplan", "sqn_type1f_makeplan", "sqn_type1_setpts", "sqn_type1f_setpts",
-    "sqn_type1_execute", "sqn_type1f_execute", "sqn_type1_destroy",
+    "sqn_type1_execute", "sqn_type1f_execute", "sqn_type1_destroy", "sqn_dump_open",
+    "sqn_dump_next", "sqn_dump_last_error", "sqn_dump_rewind", "sqn_dump_close",
+    "sqn_accumulate_dump",
 )
+ERR_DUMP = 50
 ERR_SCRATCH_LIMIT = 49
+ERR_INVALID_ARGUMENT = 21
+ERR_NUM_NU_PTS_INVALID = 20
 NOALLOC_SCRATCH_BYTES = 32 * 1024 * 1024
 
 
@@ -86,6 +91,7 @@ class SqnInfo(ctypes.Structure):
         ("tile", ctypes.c_int64 * 3),
         ("fused_fft", ctypes.c_int32),
         ("reserved", ctypes.c_int32),
+        ("natoms", ctypes.c_int64),
     ]
 
 
@@ -158,6 +164,13 @@ def load():
     for name in ("sqn_type1_execute", "sqn_type1f_execute"):
         getattr(L, name).argtypes = [vp, vp, vp]
     L.sqn_type1_destroy.argtypes = [vp]
+    L.sqn_dump_open.argtypes = [ctypes.c_char_p, ctypes.c_int32, ctypes.POINTER(vp)]
+    L.sqn_dump_next.argtypes = [vp, i64, ctypes.POINTER(i64), ctypes.POINTER(i64), vp, vp, vp,
+                                vp]
+    L.sqn_dump_last_error.argtypes = [vp]
+    L.sqn_dump_rewind.argtypes = [vp]
+    L.sqn_dump_close.argtypes = [vp]
+    L.sqn_accumulate_dump.argtypes = [vp, vp, i64, vp, ctypes.POINTER(i64)]
     L.sqn_spread_frame_noalloc.argtypes = [vp, i64, vp, ctypes.c_int32, vp, vp, vp, vp,
                                            ctypes.c_int32, ctypes.c_double, vp, vp]
     if L.sqn_abi_version() != ABI_VERSION:
@@ -325,6 +338,15 @@ class Plan:
         check(self._L.sqn_sq_grad(self._h, _ptr(a), HOST, _ptr(g), _ptr(S), _ptr(grad)),
               "sqn_sq_grad")
         return S, grad
+
+    def accumulate_dump(self, reader, max_frames=-1, ref_bounds=None):
+        """Frames of a DumpReader into the plan (parse of frame f + 1 overlapped
+        with the upload and transform of frame f); returns the frame count."""
+        done = ctypes.c_int64()
+        rb = None if ref_bounds is None else np.ascontiguousarray(ref_bounds, dtype=np.float64)
+        check(self._L.sqn_accumulate_dump(self._h, reader.handle, int(max_frames), _ptr(rb),
+                                          ctypes.byref(done)), "sqn_accumulate_dump")
+        return int(done.value)
 
     def accumulator_view(self):
         """(device pointer, number of doubles, frames so far) of the plan's FP64 sums."""
@@ -495,6 +517,72 @@ class Type1Plan:
     def close(self):
         if getattr(self, "_h", None) and self._h.value:
             self._L.sqn_type1_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class DumpReader:
+    """sqn_dump_*: multithreaded LAMMPS text dump reader (memory-mapped)."""
+
+    def __init__(self, path, nthreads=0):
+        L = load()
+        self._L = L
+        h = ctypes.c_void_p()
+        check(L.sqn_dump_open(os.fsencode(path), int(nthreads), ctypes.byref(h)), "sqn_dump_open")
+        self._h = h
+        self._cap = 0
+
+    @property
+    def handle(self):
+        return self._h
+
+    def next(self, capacity=None):
+        """The next frame as (timestep, natoms, bounds (3, 3), pos (N, 3), type_id (N,),
+        ids (N,)), or None at the end of the file."""
+        cap = int(capacity or max(self._cap, 1024))
+        while True:
+            pos = np.empty((cap, 3))
+            types = np.empty(cap, dtype=np.int32)
+            ids = np.empty(cap, dtype=np.int64)
+            bounds = np.zeros(9)
+            n, ts = ctypes.c_int64(), ctypes.c_int64()
+            rc = self._L.sqn_dump_next(self._h, cap, ctypes.byref(n), ctypes.byref(ts), _ptr(bounds),
+                                       _ptr(pos), _ptr(types), _ptr(ids))
+            if rc == ERR_INVALID_ARGUMENT and n.value > cap:
+                cap = int(n.value)
+                continue
+            if rc == ERR_DUMP:
+                raise SqnError(rc, "sqn_dump_next: reader error %d"
+                               % self._L.sqn_dump_last_error(self._h))
+            check(rc, "sqn_dump_next")
+            break
+        natoms = int(n.value)
+        if natoms == 0:
+            return None
+        self._cap = max(self._cap, natoms)
+        return (int(ts.value), natoms, bounds.reshape(3, 3), pos[:natoms], types[:natoms],
+                ids[:natoms])
+
+    def last_error(self):
+        return int(self._L.sqn_dump_last_error(self._h))
+
+    def rewind(self):
+        check(self._L.sqn_dump_rewind(self._h), "sqn_dump_rewind")
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            self._L.sqn_dump_close(self._h)
             self._h = ctypes.c_void_p()
 
     def __enter__(self):

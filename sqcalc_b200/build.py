@@ -14,7 +14,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libsqnufft.so")
 SOURCES = ["sqn_api.cu", "sqn_kernels.cu", "sqn_fft.cu", "sqn_adjoint.cu", "sqn_type1.cu",
-           "sqn_noalloc.cu"]
+           "sqn_noalloc.cu", "sqn_dump.cpp"]
 HEADERS = ["sqn_internal.h", "sqn_device.cuh", os.path.join("..", "..", "include", "sqnufft.h")]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -988,6 +988,7 @@ const char *sqn_error_string(int code) {
     case SQN_ERR_DEGENERATE_CELL: return "degenerate simulation cell";
     case SQN_ERR_TYPE_ID: return "atom type id outside 1..ntypes";
     case SQN_ERR_CUFFT: return "cuFFT failure";
+    case SQN_ERR_DUMP: return "dump file unreadable or malformed";
     case SQN_ERR_TIMEOUT: return "device wait timed out";
     case SQN_ERR_NOT_SUPPORTED: return "configuration not supported by this build";
     default: return "unknown status";
@@ -1046,6 +1047,7 @@ int sqn_plan_info_get(const sqn_plan *p, sqn_plan_info *info) {
   info->nspecies = p->nspecies;
   info->device_bytes = p->device_bytes;
   info->fused_fft = p->fused ? 1 : 0;
+  info->natoms = p->desc.natoms;
   return SQN_OK;
 }
 

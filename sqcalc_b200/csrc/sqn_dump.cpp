@@ -1,0 +1,434 @@
+// LAMMPS text dump ingest for the frame path: a multithreaded reader and a
+// driver that parses the next frame while the GPU transforms the current one.
+//
+// The reader follows lammps_next_frame (src/sqc_dump.f90:162-313) and
+// resolve_columns (:502-552): frames are "ITEM: TIMESTEP", "ITEM: NUMBER OF
+// ATOMS", "ITEM: BOX BOUNDS [xy xz yz] ..." with three bound rows (two or three
+// numbers each) and "ITEM: ATOMS <columns>" with one line per atom; the columns
+// id, type and x|xu, y|yu, z|zu (case-insensitive, first match) are read in file
+// order; a missing type or coordinate column is error 9.  Status of a failed
+// read, as the reference's ierr: 4 malformed structure or TIMESTEP, 5 bad atom
+// count, 6 bad BOX BOUNDS row, 7 ATOMS block before its header items, 8 short or
+// malformed atom line, 9 missing column.
+//
+// B200-side design: the file is memory-mapped; one pass of memchr finds the end
+// of the ATOMS block and the line where each thread starts, then the threads
+// parse their lines with correctly rounded std::from_chars (the same doubles
+// as any correctly rounding reader of the text).  The driver keeps two pinned
+// host frames: while the plan uploads and transforms one, a host thread parses
+// the next into the other.
+#include <fcntl.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cctype>
+#include <cmath>
+#include <cstdlib>
+#include <charconv>
+#include <condition_variable>
+#include <cstdint>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/sqnufft.h"
+
+struct sqn_dump_s {
+  int fd = -1;
+  const char *base = nullptr;
+  size_t size = 0;
+  size_t off = 0;
+  int nthreads = 1;
+  int last_error = 0;
+  int64_t frames = 0;
+};
+
+namespace {
+
+bool is_space(char c) { return c == ' ' || c == '\t' || c == '\r'; }
+
+// The line at off (without the newline); advances off past it.  False at EOF.
+bool next_line(const sqn_dump *d, size_t &off, const char *&b, const char *&e) {
+  if (off >= d->size) return false;
+  b = d->base + off;
+  const void *nl = std::memchr(b, '\n', d->size - off);
+  e = nl ? static_cast<const char *>(nl) : d->base + d->size;
+  off = (size_t)(e - d->base) + (nl ? 1 : 0);
+  return true;
+}
+
+// Whitespace tokens of [b, e).
+int tokens(const char *b, const char *e, std::vector<std::pair<const char *, const char *>> &out) {
+  out.clear();
+  const char *p = b;
+  while (p < e) {
+    while (p < e && is_space(*p)) ++p;
+    if (p >= e) break;
+    const char *s = p;
+    while (p < e && !is_space(*p)) ++p;
+    out.emplace_back(s, p);
+  }
+  return (int)out.size();
+}
+
+bool starts_item(const char *b, const char *e, const char *what) {
+  const size_t n = std::strlen("ITEM: ");
+  const size_t m = std::strlen(what);
+  if ((size_t)(e - b) < n + m) return false;
+  return std::memcmp(b, "ITEM: ", n) == 0 && std::memcmp(b + n, what, m) == 0;
+}
+
+bool parse_double(const char *b, const char *e, double &v) {
+  if (b < e && *b == '+') ++b;
+  auto r = std::from_chars(b, e, v);
+  return r.ec == std::errc() && r.ptr == e;
+}
+
+bool parse_int(const char *b, const char *e, int64_t &v) {
+  if (b < e && *b == '+') ++b;
+  auto r = std::from_chars(b, e, v);
+  if (r.ec == std::errc() && r.ptr == e) return true;
+  double x;  // integers written as reals (e.g. "3.0")
+  if (!parse_double(b, e, x) || x != (double)(int64_t)x) return false;
+  v = (int64_t)x;
+  return true;
+}
+
+std::string lower(const char *b, const char *e) {
+  std::string s(b, e);
+  for (char &c : s) c = (char)std::tolower((unsigned char)c);
+  return s;
+}
+
+struct Columns {
+  int id = -1, type = -1, x = -1, y = -1, z = -1, ncol = 0;
+};
+
+// Parse lines [first, first + count) starting at text offset `off` of a block.
+int parse_lines(const char *p, const char *end, int64_t first, int64_t count, const Columns &c,
+                double *pos, int32_t *type_id, int64_t *ids) {
+  std::vector<std::pair<const char *, const char *>> tk;
+  for (int64_t i = first; i < first + count; ++i) {
+    const char *nl = static_cast<const char *>(std::memchr(p, '\n', (size_t)(end - p)));
+    const char *le = nl ? nl : end;
+    if (tokens(p, le, tk) < c.ncol) return 8;
+    double x, y, z;
+    int64_t t;
+    if (!parse_double(tk[c.x].first, tk[c.x].second, x) ||
+        !parse_double(tk[c.y].first, tk[c.y].second, y) ||
+        !parse_double(tk[c.z].first, tk[c.z].second, z) ||
+        !parse_int(tk[c.type].first, tk[c.type].second, t))
+      return 8;
+    pos[3 * i + 0] = x;
+    pos[3 * i + 1] = y;
+    pos[3 * i + 2] = z;
+    type_id[i] = (int32_t)t;
+    if (ids) {
+      int64_t id = i + 1;
+      if (c.id >= 0 && !parse_int(tk[c.id].first, tk[c.id].second, id)) return 8;
+      ids[i] = id;
+    }
+    p = nl ? nl + 1 : end;
+  }
+  return 0;
+}
+
+// One frame.  0 ok, 1 end of file (no further frame), 4-9 malformed.
+int read_frame(sqn_dump *d, int64_t capacity, int64_t *natoms_out, int64_t *timestep,
+               double *bounds, double *pos, int32_t *type_id, int64_t *ids) {
+  size_t off = d->off;
+  const char *b, *e;
+  // skip to the next TIMESTEP item
+  for (;;) {
+    if (!next_line(d, off, b, e)) return 1;
+    if (starts_item(b, e, "TIMESTEP")) break;
+    // anything but blank lines before a frame is malformed
+    const char *p = b;
+    while (p < e && (is_space(*p))) ++p;
+    if (p != e) return 4;
+  }
+  std::vector<std::pair<const char *, const char *>> tk;
+  int64_t ts = 0, natoms = -1;
+  bool have_box = false;
+  double bx[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  if (!next_line(d, off, b, e) || tokens(b, e, tk) < 1 || !parse_int(tk[0].first, tk[0].second, ts))
+    return 4;
+  Columns c;
+  for (;;) {
+    if (!next_line(d, off, b, e)) return 4;
+    if (starts_item(b, e, "NUMBER OF ATOMS")) {
+      if (!next_line(d, off, b, e) || tokens(b, e, tk) < 1 ||
+          !parse_int(tk[0].first, tk[0].second, natoms) || natoms <= 0)
+        return 5;
+    } else if (starts_item(b, e, "BOX BOUNDS")) {
+      for (int k = 0; k < 3; ++k) {
+        if (!next_line(d, off, b, e)) return 4;
+        const int n = tokens(b, e, tk);
+        if (n < 2) return 6;
+        for (int m = 0; m < std::min(n, 3); ++m)
+          if (!parse_double(tk[m].first, tk[m].second, bx[3 * k + m])) return 6;
+      }
+      have_box = true;
+    } else if (starts_item(b, e, "ATOMS")) {
+      if (natoms < 0 || !have_box) return 7;
+      const int n = tokens(b, e, tk);
+      c.ncol = n - 2;
+      for (int m = 2; m < n; ++m) {
+        const std::string name = lower(tk[m].first, tk[m].second);
+        const int col = m - 2;
+        if (name == "id" && c.id < 0) c.id = col;
+        else if (name == "type" && c.type < 0) c.type = col;
+        else if ((name == "x" || name == "xu") && c.x < 0) c.x = col;
+        else if ((name == "y" || name == "yu") && c.y < 0) c.y = col;
+        else if ((name == "z" || name == "zu") && c.z < 0) c.z = col;
+      }
+      if (c.type < 0 || c.x < 0 || c.y < 0 || c.z < 0) return 9;
+      break;
+    } else if (starts_item(b, e, "TIMESTEP")) {
+      return 4;
+    }
+  }
+  *natoms_out = natoms;
+  if (natoms > capacity) return -1;  // caller's buffers too small
+  // the ATOMS block: find its end and each thread's first line
+  const int nt = (int)std::max<int64_t>(1, std::min<int64_t>(d->nthreads, natoms / 4096 + 1));
+  const int64_t per = (natoms + nt - 1) / nt;
+  std::vector<size_t> starts((size_t)nt + 1, d->size);
+  size_t p = off;
+  for (int64_t i = 0; i < natoms; ++i) {
+    if (i % per == 0) starts[(size_t)(i / per)] = p;
+    if (p >= d->size) return 8;
+    const void *nl = std::memchr(d->base + p, '\n', d->size - p);
+    p = nl ? (size_t)(static_cast<const char *>(nl) - d->base) + 1 : d->size;
+  }
+  const size_t block_end = p;
+  std::vector<int> err((size_t)nt, 0);
+  auto work = [&](int k) {
+    const int64_t first = (int64_t)k * per;
+    const int64_t count = std::min<int64_t>(per, natoms - first);
+    if (count <= 0) return;
+    err[(size_t)k] = parse_lines(d->base + starts[(size_t)k], d->base + block_end, first, count,
+                                 c, pos, type_id, ids);
+  };
+  if (nt == 1) {
+    work(0);
+  } else {
+    std::vector<std::thread> th;
+    for (int k = 1; k < nt; ++k) th.emplace_back(work, k);
+    work(0);
+    for (auto &t : th) t.join();
+  }
+  for (int v : err)
+    if (v) return v;
+  *timestep = ts;
+  if (bounds) std::memcpy(bounds, bx, sizeof(bx));
+  d->off = block_end;
+  d->frames++;
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sqn_dump_open(const char *path, int32_t nthreads, sqn_dump **out) {
+  if (!out) return SQN_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (!path) return SQN_ERR_INVALID_ARGUMENT;
+  const int fd = ::open(path, O_RDONLY);
+  if (fd < 0) return SQN_ERR_DUMP;
+  struct stat sb;
+  if (fstat(fd, &sb) != 0) {
+    ::close(fd);
+    return SQN_ERR_DUMP;
+  }
+  sqn_dump *d = new (std::nothrow) sqn_dump_s();
+  if (!d) {
+    ::close(fd);
+    return SQN_ERR_ALLOC;
+  }
+  d->fd = fd;
+  d->size = (size_t)sb.st_size;
+  if (d->size > 0) {
+    void *m = mmap(nullptr, d->size, PROT_READ, MAP_PRIVATE, fd, 0);
+    if (m == MAP_FAILED) {
+      ::close(fd);
+      delete d;
+      return SQN_ERR_DUMP;
+    }
+    madvise(m, d->size, MADV_SEQUENTIAL);
+    d->base = static_cast<const char *>(m);
+  }
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  d->nthreads = nthreads > 0 ? nthreads : (int)hw;
+  *out = d;
+  return SQN_OK;
+}
+
+int sqn_dump_next(sqn_dump *d, int64_t capacity, int64_t *natoms, int64_t *timestep,
+                  double *bounds, double *pos, int32_t *type_id, int64_t *ids) {
+  if (!d) return SQN_ERR_PLAN_NOTVALID;
+  if (!natoms || !timestep || !pos || !type_id) return SQN_ERR_INVALID_ARGUMENT;
+  *natoms = 0;
+  *timestep = 0;
+  const int r = read_frame(d, capacity, natoms, timestep, bounds, pos, type_id, ids);
+  if (r == 1) {  // end of file: no frame, not an error
+    *natoms = 0;
+    d->last_error = 1;
+    return SQN_OK;
+  }
+  if (r == -1) {
+    d->last_error = 0;
+    return SQN_ERR_INVALID_ARGUMENT;  // *natoms holds the count the buffers need
+  }
+  d->last_error = r;
+  return r == 0 ? SQN_OK : SQN_ERR_DUMP;
+}
+
+int sqn_dump_last_error(const sqn_dump *d) { return d ? d->last_error : 3; }
+
+int sqn_dump_rewind(sqn_dump *d) {
+  if (!d) return SQN_ERR_PLAN_NOTVALID;
+  d->off = 0;
+  d->frames = 0;
+  d->last_error = 0;
+  return SQN_OK;
+}
+
+int sqn_dump_close(sqn_dump *d) {
+  if (!d) return SQN_ERR_PLAN_NOTVALID;
+  if (d->base) munmap(const_cast<char *>(d->base), d->size);
+  if (d->fd >= 0) ::close(d->fd);
+  delete d;
+  return SQN_OK;
+}
+
+int sqn_accumulate_dump(sqn_plan *plan, sqn_dump *d, int64_t max_frames,
+                        const double *ref_bounds, int64_t *frames_done) {
+  if (!plan || !d) return SQN_ERR_PLAN_NOTVALID;
+  if (frames_done) *frames_done = 0;
+  double ref[9];
+  bool have_ref = ref_bounds != nullptr;
+  if (have_ref) std::memcpy(ref, ref_bounds, sizeof(ref));
+  sqn_plan_info info;
+  int st = sqn_plan_info_get(plan, &info);
+  if (st) return st;
+  const int64_t cap = info.natoms;  // every frame must hold the plan's atoms
+  if (cap <= 0) return SQN_ERR_PLAN_NOTVALID;
+  double *buf[2] = {nullptr, nullptr};
+  int32_t *types = nullptr;
+  if (cudaMallocHost(&buf[0], sizeof(double) * 3 * (size_t)cap) != cudaSuccess ||
+      cudaMallocHost(&buf[1], sizeof(double) * 3 * (size_t)cap) != cudaSuccess) {
+    cudaGetLastError();
+    if (buf[0]) cudaFreeHost(buf[0]);
+    return SQN_ERR_ALLOC;
+  }
+  types = static_cast<int32_t *>(std::malloc(sizeof(int32_t) * (size_t)cap));
+  if (!types) {
+    cudaFreeHost(buf[0]);
+    cudaFreeHost(buf[1]);
+    return SQN_ERR_ALLOC;
+  }
+  // Parser thread: fills buffer k, then waits until the main thread has handed
+  // that buffer to the plan (sqn_accumulate_frames returns once it has been read).
+  std::mutex mu;
+  std::condition_variable cv;
+  int ready[2] = {0, 0};      // 1: parsed frame waiting, 2: end of input, <0: error
+  bool free_[2] = {true, true};
+  bool stop = false;
+  int64_t limit = max_frames < 0 ? INT64_MAX : max_frames;
+  std::thread parser([&]() {
+    int k = 0;
+    for (int64_t f = 0;; ++f) {
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        cv.wait(lk, [&] { return free_[k] || stop; });
+        if (stop) return;
+        free_[k] = false;
+      }
+      int code = 1;
+      if (f < limit) {
+        int64_t n = 0, ts = 0;
+        double bx[9];
+        const int r = sqn_dump_next(d, cap, &n, &ts, bx, buf[k], types, nullptr);
+        if (r != SQN_OK) {
+          code = -r;
+        } else if (n == 0) {
+          code = 2;
+        } else if (n != cap) {
+          code = -SQN_ERR_NUM_NU_PTS_INVALID;
+        } else {
+          // the box must not change between frames (relative 1e-6)
+          if (!have_ref) {
+            std::memcpy(ref, bx, sizeof(ref));
+            have_ref = true;
+          }
+          double scale = 1.0, dev = 0.0;
+          for (int i = 0; i < 9; ++i) {
+            scale = std::max(scale, std::fabs(ref[i]));
+            dev = std::max(dev, std::fabs(bx[i] - ref[i]));
+          }
+          if (dev > 1e-6 * scale) {
+            d->last_error = 10;
+            code = -SQN_ERR_DUMP;
+          }
+        }
+      } else {
+        code = 2;
+      }
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        ready[k] = code;
+      }
+      cv.notify_all();
+      if (code != 1) return;
+      k ^= 1;
+    }
+  });
+  int k = 0;
+  int64_t done = 0;
+  for (;;) {
+    int code;
+    {
+      std::unique_lock<std::mutex> lk(mu);
+      cv.wait(lk, [&] { return ready[k] != 0; });
+      code = ready[k];
+      ready[k] = 0;
+    }
+    if (code != 1) {
+      if (code < 0) st = -code;
+      break;
+    }
+    st = sqn_accumulate_frames(plan, buf[k], 1, SQN_HOST);
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      free_[k] = true;
+      if (st != SQN_OK) stop = true;
+    }
+    cv.notify_all();
+    if (st != SQN_OK) break;
+    ++done;
+    k ^= 1;
+  }
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    stop = true;
+  }
+  cv.notify_all();
+  parser.join();
+  if (frames_done) *frames_done = done;
+  const int sync = sqn_sync(plan);
+  cudaFreeHost(buf[0]);
+  cudaFreeHost(buf[1]);
+  std::free(types);
+  return st != SQN_OK ? st : sync;
+}
+
+}  // extern "C"
