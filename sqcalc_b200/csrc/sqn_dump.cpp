@@ -358,7 +358,9 @@ int sqn_accumulate_dump(sqn_plan *plan, sqn_dump *d, int64_t max_frames,
         int64_t n = 0, ts = 0;
         double bx[9];
         const int r = sqn_dump_next(d, cap, &n, &ts, bx, buf[k], types, nullptr);
-        if (r != SQN_OK) {
+        if (r == SQN_ERR_INVALID_ARGUMENT && n > cap) {
+          code = -SQN_ERR_NUM_NU_PTS_INVALID;  // more atoms than the plan
+        } else if (r != SQN_OK) {
           code = -r;
         } else if (n == 0) {
           code = 2;
