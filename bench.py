@@ -350,6 +350,58 @@ def batched_leg(W, K, stream, dist, local_rank):
     return out
 
 
+def ingest_leg(types, frames, stream, local_rank, nframes=3):
+    """End to end from a LAMMPS text dump: the precision-form frames written
+    as text (id type x y z, %.6f), then read by the library's multithreaded
+    reader and streamed through sqn_accumulate_dump (the parse of frame f + 1
+    overlaps the upload and transform of frame f).  Also times the reader
+    alone on the same file."""
+    import tempfile
+    import torch
+    from sqcalc_b200 import _lib
+
+    nframes = min(nframes, len(frames))
+    tmpdir = tempfile.mkdtemp(prefix="sqn_ingest_")
+    path = os.path.join(tmpdir, "frames.dump")
+    ids = np.arange(1, N_ATOMS + 1)
+    with open(path, "w") as fh:
+        for f in range(nframes):
+            fh.write("ITEM: TIMESTEP\n%d\nITEM: NUMBER OF ATOMS\n%d\n"
+                     "ITEM: BOX BOUNDS pp pp pp\n0 %r\n0 %r\n0 %r\nITEM: ATOMS id type x y z\n"
+                     % (f, N_ATOMS, BOX, BOX, BOX))
+            np.savetxt(fh, np.column_stack([ids, types, frames[f]]), fmt="%d %d %.6f %.6f %.6f")
+    size = os.path.getsize(path)
+    cores = os.cpu_count() or 1
+    try:
+        with _lib.DumpReader(path, nthreads=cores) as r:
+            t0 = time.perf_counter()
+            n = 0
+            while r.next(capacity=N_ATOMS) is not None:
+                n += 1
+            t_read = time.perf_counter() - t0
+        with _lib.Plan(np.eye(3).reshape(9) * BOX, np.zeros(3), types,
+                       weight=_lib.WEIGHT_NEUTRON, amp_const=np.array(B_NEUTRON), qmin=0.0,
+                       qmax=QMAX, nq=NQ, partials=True, precision=_lib.PREC_SINGLE, eps=EPS,
+                       device=local_rank, stream=stream.cuda_stream) as p, \
+                _lib.DumpReader(path, nthreads=cores) as r:
+            p.accumulate(frames[0])  # warm the plan
+            p.sync()
+            p.reset()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            done = p.accumulate_dump(r)
+            t_all = time.perf_counter() - t0
+    finally:
+        os.remove(path)
+        os.rmdir(tmpdir)
+    return {"metric": "S(q) frames/s from a LAMMPS text dump (read + upload + transform)",
+            "unit": "frames/s", "value": done / t_all, "frames": done,
+            "reader_only_frames_per_s": n / t_read,
+            "reader_gb_per_s": size / (nframes * 1e9) * n / t_read,
+            "dump_bytes_per_frame": size // nframes, "threads": cores,
+            "timing": "host wall clock around sqn_accumulate_dump (it syncs before returning)"}
+
+
 GRAD_N, GRAD_BOX, GRAD_QMIN, GRAD_QMAX, GRAD_NQ = 100_000, 100.0, 0.5, 8.0, 375
 
 
@@ -506,6 +558,9 @@ def run_ours(args, rank, world, local_rank):
     # --- dS/dr evaluations (differentiation form) -------------------------------
     grad = None if args.no_grad else grad_leg(W, K, stream, dist, local_rank)
 
+    # --- ingest: from a LAMMPS text dump ------------------------------------------
+    ingest = None if args.no_ingest else ingest_leg(types, frames, stream, local_rank)
+
     # --- batched form: many systems behind one CUDA graph -------------------------
     batched = None if args.no_batch else batched_leg(W, K, stream, dist, local_rank)
 
@@ -558,6 +613,7 @@ def run_ours(args, rank, world, local_rank):
             "fp64": fp64,
             "grad": grad,
             "batched": batched,
+            "ingest": ingest,
             "clocks": clk.summary(),
             "wall_s": t_wall,
         }
@@ -580,6 +636,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-grad", action="store_true", help="skip the dS/dr leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-systems leg")
+    ap.add_argument("--no-ingest", action="store_true", help="skip the text-dump ingest leg")
     ap.add_argument("--fused-fft", action="store_true",
                     help="frame path on the pruned FFT passes fused with the binning")
     ap.add_argument("--scale", type=float, default=1.0,
