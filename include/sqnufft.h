@@ -100,6 +100,18 @@ typedef struct sqn_plan_desc {
   int32_t reserved;
   int64_t max_grid_modes;   /* prod(modes) cap; 0 = sqcalc's 4e8, < 0 = none */
   void *stream;             /* cudaStream_t to run on, or NULL for a plan-owned stream */
+  /* Powder XRD pattern (--xrd, structure_factor_t%xrd_*,
+   * src/sqc_structure_factor.f90:125-146): on when xrd_lambda > 0.  Bins uniform
+   * in two-theta over [xrd_2theta_min, xrd_2theta_max] degrees, of width
+   * xrd_step (<= 0: from the box, sf_configure_xrd :846-905, every direction
+   * taken as periodic); each kept mode adds |total|^2 and the amplitude-weighted
+   * pair products, times the Lorentz-polarization factor when xrd_lp. */
+  double xrd_lambda;        /* incident wavelength, Angstrom (--xrd-lambda) */
+  double xrd_2theta_min;    /* --xrd-range (default 1 .. 179) */
+  double xrd_2theta_max;
+  double xrd_step;          /* --xrd-step */
+  int32_t xrd_lp;           /* --lp (1, default) / --no-lp (0) */
+  int32_t reserved2;
 } sqn_plan_desc;
 
 /* What the plan chose. */
@@ -119,6 +131,9 @@ typedef struct sqn_plan_info {
   int32_t fused_fft;        /* 1: pruned FFT passes fused with the binning; 0: cuFFT + bin kernel */
   int32_t reserved;
   int64_t natoms;           /* atoms per frame */
+  int32_t xrd_bins;         /* two-theta bins of the powder pattern (0: off) */
+  int32_t reserved2;
+  double xrd_step;          /* their width, degrees */
 } sqn_plan_info;
 
 typedef struct sqn_plan_s sqn_plan;
@@ -176,6 +191,16 @@ int sqn_finalize(sqn_plan *plan, int32_t faber_ziman, double *S_total, double *S
 
 /* Zero the accumulators and the frame count. */
 int sqn_reset(sqn_plan *plan);
+
+/* The powder XRD pattern (plans with xrd_lambda > 0; syncs first), per atom
+ * and per frame as sf_write_xrd writes it (src/sqc_structure_factor.f90:
+ * 964-1031): two_theta[xrd_bins] bin centres (degrees), I[xrd_bins],
+ * I_partial[ntypes*ntypes*xrd_bins] (first index fastest; a <= b filled, zero
+ * without partials; I = sum_a I_aa + 2 sum_{a<b} I_ab), count[xrd_bins] kept
+ * modes per bin (both mirrors counted; sf_xrd_empty_bins :927-936).  Any pointer
+ * may be NULL. */
+int sqn_get_xrd(sqn_plan *plan, double *two_theta, double *I, double *I_partial, int64_t *count,
+                int64_t *nframes);
 
 /* Frames sharded over ranks (one process per GPU, each with its own plan on
  * the same system).  The plan's FP64 sums -- shell sums, pair sums and, with

@@ -367,3 +367,76 @@ def dirft3d1(x, y, z, c, n_modes, iflag=1, modeord=0):
     lib().sqo_dirft3d1(M, _c(x, np.float64), _c(y, np.float64), _c(z, np.float64), cf, ntr,
                        int(iflag), N1, N2, N3, int(modeord), out)
     return out.view(np.complex128).reshape(ntr, N3, N2, N1)
+
+
+def two_theta_deg(q, lam):
+    """two_theta_deg (src/sqc_structure_factor.f90:907-914)."""
+    st = np.clip(np.asarray(q) * lam / (4.0 * np.pi), -1.0, 1.0)
+    return 2.0 * np.arcsin(st) * 180.0 / np.pi
+
+
+def lorentz_polarization(tth_deg):
+    """lorentz_polarization (src/sqc_structure_factor.f90:917-924)."""
+    tth = np.radians(tth_deg)
+    th = 0.5 * tth
+    return (1.0 + np.cos(tth) ** 2) / (np.sin(th) ** 2 * np.cos(th))
+
+
+def xrd_bins(cell, lam, tmin, tmax, step=0.0):
+    """Bin count and width of sf_configure_xrd (:846-890), every direction periodic."""
+    a = np.asarray(cell, dtype=np.float64)
+    if not step > 0.0:
+        vol = abs(np.linalg.det(a))
+        widths = [vol / np.linalg.norm(np.cross(a[(i + 1) % 3], a[(i + 2) % 3])) for i in range(3)]
+        theta_max = min(0.5 * np.radians(tmax), np.radians(60.0))
+        step = (lam / (min(widths) * np.cos(theta_max))) / (np.pi / 180.0)
+    nb = max(1, int(np.ceil((tmax - tmin) / step)))
+    return nb, (tmax - tmin) / nb
+
+
+def direct_xrd(frames, type_id, cell, origin, weights: Weights, lam, tmin, tmax, step=0.0,
+               lp=True, ntypes=None):
+    """FP64 direct-sum powder pattern over the kept modes of the q range the
+    reference derives from the two-theta range (src/sqc_options.f90:650-651):
+    I(bin) = sum_frames sum_{q in bin} |sum_a w_a(q) rho_a(q)|^2 LP / (nframes N) and
+    I_ab the same with w_a w_b Re(rho_a rho_b*) (sf_accumulate_values :616-619,
+    sf_accumulate_xrd_partials :538-588, sf_write_xrd :964-1031).  Small systems
+    only (N x kept modes complex exponentials per frame)."""
+    type_id = np.asarray(type_id, dtype=np.int32)
+    T = int(ntypes or type_id.max())
+    qmin = 4.0 * np.pi * np.sin(0.5 * np.radians(tmin)) / lam
+    qmax = 4.0 * np.pi * np.sin(0.5 * np.radians(tmax)) / lam
+    grid = configure_grid(cell, qmin, qmax, 10)
+    nb, step = xrd_bins(cell, lam, tmin, tmax, step)
+    tth = two_theta_deg(grid.qlen, lam)
+    b = np.clip(((tth - tmin) / step).astype(np.int64), 0, nb - 1)
+    wt = lorentz_polarization(tth) if lp else np.ones_like(tth)
+    amp, xr = weights.padded(T)
+    amp = np.asarray(amp, dtype=np.float64).reshape(-1)
+    xr = np.asarray(xr, dtype=np.float64).reshape(-1, 9)
+    if weights.kind == WEIGHT_XRAY:
+        s = (grid.qlen / (4.0 * np.pi)) ** 2
+        w = np.stack([xr[t, 8] + sum(xr[t, i] * np.exp(-xr[t, 4 + i] * s) for i in range(4))
+                      for t in range(T)])
+    elif weights.kind == WEIGHT_NEUTRON:
+        w = np.stack([np.full(grid.nmodes, amp[t]) for t in range(T)])
+    else:
+        w = np.ones((T, grid.nmodes))
+    I = np.zeros(nb)
+    Ip = np.zeros((T, T, nb))
+    for pos in frames:
+        d = np.asarray(pos, dtype=np.float64) - np.asarray(origin)
+        rho = np.zeros((T, grid.nmodes), dtype=np.complex128)
+        for t in range(T):
+            sel = d[type_id == t + 1]
+            if len(sel):
+                rho[t] = np.exp(1j * (sel @ grid.qvec.T)).sum(axis=0)
+        tot = (w * rho).sum(axis=0)
+        np.add.at(I, b, np.abs(tot) ** 2 * wt)
+        for ta in range(T):
+            for tb in range(ta, T):
+                v = w[ta] * w[tb] * np.real(rho[ta] * np.conj(rho[tb])) * wt
+                np.add.at(Ip[ta, tb], b, v)
+    norm = len(frames) * len(type_id)
+    cnt = np.bincount(b, minlength=nb)
+    return tmin + (np.arange(nb) + 0.5) * step, I / norm, Ip / norm, cnt, qmin, qmax

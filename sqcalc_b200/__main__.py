@@ -8,6 +8,7 @@ Mirrors the option surface and exit codes of ``sqcalc static --device gpu``
 from __future__ import annotations
 
 import argparse
+import math
 import os
 import sys
 import time
@@ -29,7 +30,7 @@ def parse(argv):
     p = argparse.ArgumentParser(prog="sqcalc_b200 static", add_help=True)
     p.add_argument("-i", "--input", required=True)
     p.add_argument("-m", "--mapping", default=None)
-    p.add_argument("-w", "--weight", default="unit")
+    p.add_argument("-w", "--weight", default=None)
     p.add_argument("--norm", default="mean", choices=["mean", "fz", "self", "n", "natom"])
     g = p.add_mutually_exclusive_group()
     g.add_argument("--partials", dest="partials", action="store_true", default=True)
@@ -38,8 +39,15 @@ def parse(argv):
     p.add_argument("--grid", default=None)
     p.add_argument("--precision", default="double")
     p.add_argument("--eps", type=float, default=None)
-    p.add_argument("--qmin", type=float, default=0.0)
-    p.add_argument("--qmax", type=float, default=20.0)
+    p.add_argument("--qmin", type=float, default=None)
+    p.add_argument("--qmax", type=float, default=None)
+    p.add_argument("--xrd", default=None, metavar="FILE")
+    p.add_argument("--xrd-lambda", type=float, default=None)
+    p.add_argument("--xrd-range", type=float, nargs=2, default=None, metavar=("MIN2TH", "MAX2TH"))
+    p.add_argument("--xrd-step", type=float, default=None)
+    lp = p.add_mutually_exclusive_group()
+    lp.add_argument("--lp", dest="lp", action="store_true", default=None)
+    lp.add_argument("--no-lp", dest="lp", action="store_false")
     p.add_argument("--nq", type=int, default=500)
     p.add_argument("--device", default="gpu", choices=["gpu", "cuda"])
     p.add_argument("--gpu-id", type=int, default=0)
@@ -58,6 +66,33 @@ def main(argv=None):
         a = parse(argv[1:])
     except SystemExit as e:
         sys.exit(2 if e.code else 0)
+    # --xrd and its settings (src/sqc_options.f90:620-658)
+    xrd = None
+    if a.xrd is not None:
+        if a.xrd_lambda is None:
+            _die(2, "--xrd needs --xrd-lambda LAMBDA (the incident wavelength)")
+        if not a.xrd_lambda > 0.0:
+            _die(2, "--xrd-lambda must be a positive wavelength")
+        if a.qmin is not None or a.qmax is not None:
+            _die(2, "--xrd takes the q range from --xrd-lambda and --xrd-range; "
+                    "do not pass --qmin or --qmax with it")
+        lo, hi = a.xrd_range if a.xrd_range else (1.0, 179.0)
+        if not (lo > 0.0 and hi < 180.0 and hi > lo):
+            _die(2, "--xrd-range needs 0 < MIN2TH < MAX2TH < 180 degrees")
+        if a.xrd_step is not None and not a.xrd_step > 0.0:
+            _die(2, "--xrd-step must be a positive number of degrees")
+        xrd = dict(lam=a.xrd_lambda, range=(lo, hi), step=a.xrd_step or 0.0,
+                   lp=True if a.lp is None else a.lp)
+        if a.weight is None:
+            a.weight = "xray"
+        a.qmin = 4.0 * math.pi * math.sin(0.5 * math.radians(lo)) / a.xrd_lambda
+        a.qmax = 4.0 * math.pi * math.sin(0.5 * math.radians(hi)) / a.xrd_lambda
+    elif (a.xrd_lambda is not None or a.xrd_range is not None or a.xrd_step is not None
+          or a.lp is not None):
+        _die(2, "--xrd-lambda, --xrd-range, --xrd-step and --lp/--no-lp belong to --xrd FILE")
+    a.weight = a.weight or "unit"
+    a.qmin = 0.0 if a.qmin is None else a.qmin
+    a.qmax = 20.0 if a.qmax is None else a.qmax
     try:
         scheme = WeightScheme.from_options(a.weight, a.mapping)
     except MappingError as e:
@@ -80,7 +115,7 @@ def main(argv=None):
     method = GpuStructureFactor(norm=a.norm, nq=a.nq, qmin=a.qmin, qmax=a.qmax, eps=a.eps,
                                 want_grid=a.grid is not None, partials=a.partials,
                                 faber_ziman=a.faber_ziman, precision=a.precision,
-                                device=a.gpu_id)
+                                device=a.gpu_id, xrd=xrd)
     try:
         method.configure(first, scheme)
     except SqcalcError as e:
@@ -103,6 +138,8 @@ def main(argv=None):
         sys.stderr.write("  frames     : %d in %.3f s\n" % (n, time.time() - t0))
     try:
         method.write_results(a.output, a.grid)
+        if a.xrd is not None:
+            method.write_xrd(a.xrd)
     except OSError as e:
         _die(11, str(e))
     method.close()

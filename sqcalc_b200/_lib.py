@@ -37,7 +37,7 @@ EXPORTS = (
     "sqn_type1_makeplan", "sqn_type1f_makeplan", "sqn_type1_setpts", "sqn_type1f_setpts",
     "sqn_type1_execute", "sqn_type1f_execute", "sqn_type1_destroy", "sqn_dump_open",
     "sqn_dump_next", "sqn_dump_last_error", "sqn_dump_rewind", "sqn_dump_close",
-    "sqn_accumulate_dump",
+    "sqn_accumulate_dump", "sqn_get_xrd",
 )
 ERR_DUMP = 50
 ERR_SCRATCH_LIMIT = 49
@@ -72,6 +72,12 @@ class SqnDesc(ctypes.Structure):
         ("reserved", ctypes.c_int32),
         ("max_grid_modes", ctypes.c_int64),
         ("stream", ctypes.c_void_p),
+        ("xrd_lambda", ctypes.c_double),
+        ("xrd_2theta_min", ctypes.c_double),
+        ("xrd_2theta_max", ctypes.c_double),
+        ("xrd_step", ctypes.c_double),
+        ("xrd_lp", ctypes.c_int32),
+        ("reserved2", ctypes.c_int32),
     ]
 
 
@@ -92,6 +98,9 @@ class SqnInfo(ctypes.Structure):
         ("fused_fft", ctypes.c_int32),
         ("reserved", ctypes.c_int32),
         ("natoms", ctypes.c_int64),
+        ("xrd_bins", ctypes.c_int32),
+        ("reserved2", ctypes.c_int32),
+        ("xrd_step", ctypes.c_double),
     ]
 
 
@@ -171,6 +180,7 @@ def load():
     L.sqn_dump_rewind.argtypes = [vp]
     L.sqn_dump_close.argtypes = [vp]
     L.sqn_accumulate_dump.argtypes = [vp, vp, i64, vp, ctypes.POINTER(i64)]
+    L.sqn_get_xrd.argtypes = [vp, vp, vp, vp, vp, vp]
     L.sqn_spread_frame_noalloc.argtypes = [vp, i64, vp, ctypes.c_int32, vp, vp, vp, vp,
                                            ctypes.c_int32, ctypes.c_double, vp, vp]
     if L.sqn_abi_version() != ABI_VERSION:
@@ -204,12 +214,13 @@ class Plan:
                  xray_coef=None, qmin=0.0, qmax=20.0, nq=500, norm=NORM_MEAN, partials=True,
                  want_grid=False, precision=PREC_DOUBLE, eps=1e-9, upsampfac=0.0,
                  kernel_width=0, device=0, max_grid_modes=0, timing=False, stream=None,
-                 grad=False, fused_fft=None):
+                 grad=False, fused_fft=None, xrd=None):
         L = load()
         self._L = L
         d = self._describe(cell, origin, type_id, ntypes, weight, amp_const, xray_coef, qmin,
                            qmax, nq, norm, partials, want_grid, precision, eps, upsampfac,
-                           kernel_width, device, max_grid_modes, timing, stream, grad, fused_fft)
+                           kernel_width, device, max_grid_modes, timing, stream, grad, fused_fft,
+                           xrd)
         h = ctypes.c_void_p()
         self.status = check(L.sqn_plan_create(ctypes.byref(d), ctypes.byref(h)), "sqn_plan_create")
         self._attach(h, owned=True)
@@ -218,8 +229,9 @@ class Plan:
                   xray_coef=None, qmin=0.0, qmax=20.0, nq=500, norm=NORM_MEAN, partials=True,
                   want_grid=False, precision=PREC_DOUBLE, eps=1e-9, upsampfac=0.0,
                   kernel_width=0, device=0, max_grid_modes=0, timing=False, stream=None,
-                  grad=False, fused_fft=None):
-        """Fill an SqnDesc; the arrays it points to are kept on self."""
+                  grad=False, fused_fft=None, xrd=None):
+        """Fill an SqnDesc; the arrays it points to are kept on self.  xrd: None, or a
+        dict(lam=..., range=(min, max), step=0.0, lp=True) for the powder pattern."""
         L = self._L
         self.type_id = np.ascontiguousarray(type_id, dtype=np.int32)
         self.natoms = int(self.type_id.size)
@@ -257,6 +269,12 @@ class Plan:
         d.kernel_width = int(kernel_width)
         d.max_grid_modes = int(max_grid_modes)
         d.stream = stream
+        if xrd:
+            d.xrd_lambda = float(xrd["lam"])
+            lo, hi = xrd.get("range", (1.0, 179.0))
+            d.xrd_2theta_min, d.xrd_2theta_max = float(lo), float(hi)
+            d.xrd_step = float(xrd.get("step", 0.0) or 0.0)
+            d.xrd_lp = 1 if xrd.get("lp", True) else 0
         return d
 
     def _attach(self, h, owned):
@@ -338,6 +356,17 @@ class Plan:
         check(self._L.sqn_sq_grad(self._h, _ptr(a), HOST, _ptr(g), _ptr(S), _ptr(grad)),
               "sqn_sq_grad")
         return S, grad
+
+    def xrd(self):
+        """Powder pattern per atom and frame: (two_theta, I, I_partial (T, T, bins),
+        count, nframes); the pair array is indexed [a-1, b-1, bin] (a <= b) like partial_num."""
+        nb, T = int(self.info.xrd_bins), self.ntypes
+        tth, I = np.zeros(nb), np.zeros(nb)
+        Ip, cnt = np.zeros(T * T * nb), np.zeros(nb, dtype=np.int64)
+        nf = ctypes.c_int64()
+        check(self._L.sqn_get_xrd(self._h, _ptr(tth), _ptr(I), _ptr(Ip), _ptr(cnt),
+                                  ctypes.cast(ctypes.byref(nf), ctypes.c_void_p)), "sqn_get_xrd")
+        return tth, I, Ip.reshape(nb, T, T).transpose(2, 1, 0), cnt, int(nf.value)
 
     def accumulate_dump(self, reader, max_frames=-1, ref_bounds=None):
         """Frames of a DumpReader into the plan (parse of frame f + 1 overlapped

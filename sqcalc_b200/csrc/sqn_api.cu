@@ -273,6 +273,8 @@ struct sqn_plan_s {
   cufftHandle fft_fwd1 = 0, fft_inv3 = 0;
   bool fft_fwd1_ok = false, fft_inv3_ok = false;
   int64_t gnum_half = 0;
+  int64_t nsums = 0;           // shell + powder-pattern sums at the head of d_acc
+  double *d_xcnt = nullptr;    // kept modes per two-theta bin
 
   int64_t nframes = 0;
   int slot_next = 0;
@@ -517,6 +519,41 @@ int setup_plan(sqn_plan *p, const sqn_plan_desc *d) {
   b.natoms = d->natoms;
   if (d->norm < 1 || d->norm > 3) return SQN_ERR_INVALID_ARGUMENT;
 
+  // --- powder XRD bins (sf_configure_xrd, src/sqc_structure_factor.f90:846-905)
+  b.xrd = 0;
+  b.xbins = 0;
+  b.xquant = 0;
+  if (d->xrd_lambda > 0.0) {
+    const double tmin = d->xrd_2theta_min, tmax = d->xrd_2theta_max;
+    if (!(tmin > 0.0 && tmax < 180.0 && tmax > tmin)) return SQN_ERR_INVALID_ARGUMENT;
+    const double deg2rad = M_PI / 180.0;
+    double step = d->xrd_step;
+    if (!(step > 0.0)) {
+      // the narrowest cell width, every direction taken as periodic
+      const double *a = d->cell;
+      double bound = 1e300;
+      for (int i = 0; i < 3; ++i) {
+        const double *u = a + 3 * ((i + 1) % 3), *v = a + 3 * ((i + 2) % 3);
+        const double cx = u[1] * v[2] - u[2] * v[1], cy = u[2] * v[0] - u[0] * v[2],
+                     cz = u[0] * v[1] - u[1] * v[0];
+        const double area = std::sqrt(cx * cx + cy * cy + cz * cz);
+        if (area > 0.0) bound = std::min(bound, std::fabs(det3(a)) / area);
+      }
+      if (!(bound > 0.0 && bound < 1e300)) return SQN_ERR_DEGENERATE_CELL;
+      const double theta_max = std::min(0.5 * deg2rad * tmax, 60.0 * deg2rad);
+      step = (d->xrd_lambda / (bound * std::cos(theta_max))) / deg2rad;
+    }
+    const double nb = std::ceil((tmax - tmin) / step);
+    if (!(nb < 1e7)) return SQN_ERR_INVALID_ARGUMENT;
+    b.xbins = std::max(1, (int)nb);
+    b.xstep = (tmax - tmin) / (double)b.xbins;
+    b.xmin = tmin;
+    b.xlambda = d->xrd_lambda;
+    b.xlp = d->xrd_lp ? 1 : 0;
+    b.xquant = p->nquant;
+    b.xrd = 1;
+  }
+
   // --- device buffers --------------------------------------------------------
   const int64_t N = d->natoms;
   const size_t rsz = p->fp64 ? 8 : 4;
@@ -553,8 +590,10 @@ int setup_plan(sqn_plan *p, const sqn_plan_desc *d) {
   // want_grid) share one allocation, so that ranks holding disjoint frames can
   // add them with a single all-reduce (sqn_accumulator_view).
   if (d->want_grid) p->gnum_half = (int64_t)(p->hm[0] + 1) * p->modes[1] * p->modes[2];
-  if ((st = dalloc(p, &p->d_acc, (size_t)p->nquant * d->nq + (size_t)p->gnum_half))) return st;
-  if (d->want_grid) p->d_gnum = p->d_acc + (size_t)p->nquant * d->nq;
+  p->nsums = (int64_t)hist_len(b);  // shell sums, then the powder-pattern sums
+  if ((st = dalloc(p, &p->d_acc, (size_t)p->nsums + (size_t)p->gnum_half))) return st;
+  if (d->want_grid) p->d_gnum = p->d_acc + p->nsums;
+  if (b.xrd && (st = dalloc(p, &p->d_xcnt, (size_t)b.xbins))) return st;
   if ((st = dalloc(p, &p->d_den, (size_t)d->nq))) return st;
   if ((st = dalloc(p, &p->d_cnt, (size_t)d->nq))) return st;
 
@@ -601,12 +640,15 @@ int setup_plan(sqn_plan *p, const sqn_plan_desc *d) {
     if (e != cudaSuccess) return SQN_ERR_CUDA;
   }
   if (cudaMemsetAsync(p->d_counts, 0, sizeof(int) * (size_t)p->nkeys, s) != cudaSuccess ||
-      cudaMemsetAsync(p->d_acc, 0, sizeof(double) * (size_t)p->nquant * d->nq, s) != cudaSuccess ||
+      cudaMemsetAsync(p->d_acc, 0, sizeof(double) * (size_t)p->nsums, s) != cudaSuccess ||
       cudaMemsetAsync(p->d_den, 0, sizeof(double) * (size_t)d->nq, s) != cudaSuccess ||
       cudaMemsetAsync(p->d_cnt, 0, sizeof(double) * (size_t)d->nq, s) != cudaSuccess)
     return SQN_ERR_CUDA;
   if (p->d_gnum &&
       cudaMemsetAsync(p->d_gnum, 0, sizeof(double) * (size_t)p->gnum_half, s) != cudaSuccess)
+    return SQN_ERR_CUDA;
+  if (p->d_xcnt &&
+      cudaMemsetAsync(p->d_xcnt, 0, sizeof(double) * (size_t)b.xbins, s) != cudaSuccess)
     return SQN_ERR_CUDA;
 
   // --- rows, shell normalisation, kept-mode count --------------------------
@@ -621,7 +663,7 @@ int setup_plan(sqn_plan *p, const sqn_plan_desc *d) {
     nb.ntr = p->nspecies;
     nb.xray = xray ? 1 : 0;
     if (launch_norms(p->d_rows, p->nrows, nb, p->d_amp_sp, p->d_xcoef_sp, p->d_counts_sp, p->d_den,
-                     p->d_cnt, p->nsm, s) != cudaSuccess)
+                     p->d_cnt, p->d_xcnt, p->nsm, s) != cudaSuccess)
       return SQN_ERR_CUDA;
     p->launches++;
     p->den.assign(d->nq, 0.0);
@@ -765,14 +807,14 @@ int setup_fused_fft(sqn_plan *p) {
   // A2 (ntr x nf2 x M1 x H1 complex) reuses the real grids
   if ((double)f.M1 * f.H1 * 2.0 > (double)p->nf[1] * p->nf[0]) return SQN_OK;
   if (p->nf[1] % 2 != 0) return SQN_OK;
-  f.hist_smem = (size_t)b.nquant * b.nq * sizeof(double) <= 48 * 1024;
+  f.hist_smem = (size_t)hist_len(b) * sizeof(double) <= 48 * 1024;
   int optin = 0;
   if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, p->device) !=
       cudaSuccess)
     return SQN_ERR_CUDA;
   const size_t limit = (size_t)optin - 8 * 1024;  // static shared memory and slack
   for (int pass = 0; pass < 3; ++pass)
-    if (fft_pass_smem(f, pass, p->fp64, p->ntr, b.nquant, b.nq) > limit) return SQN_OK;
+    if (fft_pass_smem(f, pass, p->fp64, p->ntr, hist_len(b)) > limit) return SQN_OK;
   for (int d = 0; d < 3; ++d) {
     const int n = f.ax[d].n;
     std::vector<double> tw(2 * (size_t)n);
@@ -825,7 +867,7 @@ int setup_fused_fft(sqn_plan *p) {
     f.h2span = ds;
   }
   // persistent z-pass CTAs: as many as fit per SM by shared memory, at most 2
-  const size_t sm3 = fft_pass_smem(f, 2, p->fp64, p->ntr, b.nquant, b.nq);
+  const size_t sm3 = fft_pass_smem(f, 2, p->fp64, p->ntr, hist_len(b));
   int per = (int)((228 * 1024) / (sm3 + 1024));
   per = std::max(1, std::min(2, per));
   f.grid3 = p->nsm * per;
@@ -1007,6 +1049,11 @@ void sqn_default_desc(sqn_plan_desc *d) {
   d->partials = 1;
   d->weight = SQN_WEIGHT_UNIT;
   d->precision = SQN_PREC_DOUBLE;
+  d->xrd_lambda = 0.0;
+  d->xrd_2theta_min = 1.0;
+  d->xrd_2theta_max = 179.0;
+  d->xrd_step = 0.0;
+  d->xrd_lp = 1;
 }
 
 int sqn_plan_create(const sqn_plan_desc *desc, sqn_plan **out) {
@@ -1048,6 +1095,8 @@ int sqn_plan_info_get(const sqn_plan *p, sqn_plan_info *info) {
   info->device_bytes = p->device_bytes;
   info->fused_fft = p->fused ? 1 : 0;
   info->natoms = p->desc.natoms;
+  info->xrd_bins = p->bg.xrd ? p->bg.xbins : 0;
+  info->xrd_step = p->bg.xrd ? p->bg.xstep : 0.0;
   return SQN_OK;
 }
 
@@ -1219,13 +1268,51 @@ int sqn_finalize(sqn_plan *p, int32_t faber_ziman, double *S_total, double *S_pa
   return SQN_OK;
 }
 
+int sqn_get_xrd(sqn_plan *p, double *two_theta, double *I, double *I_partial, int64_t *count,
+                int64_t *nframes) {
+  if (!p) return SQN_ERR_PLAN_NOTVALID;
+  const BinGeom &b = p->bg;
+  if (!b.xrd) return SQN_ERR_NOT_SUPPORTED;
+  DeviceGuard guard(p->device);
+  if (cudaStreamSynchronize(p->stream) != cudaSuccess) return SQN_ERR_CUDA;
+  const int nb = b.xbins, T = p->desc.ntypes;
+  std::vector<double> xs((size_t)b.xquant * nb), xc((size_t)nb);
+  if (cudaMemcpy(xs.data(), p->d_acc + (size_t)b.nquant * b.nq, xs.size() * sizeof(double),
+                 cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(xc.data(), p->d_xcnt, xc.size() * sizeof(double), cudaMemcpyDeviceToHost) !=
+          cudaSuccess)
+    return SQN_ERR_CUDA;
+  // per atom and per frame (sf_write_xrd, src/sqc_structure_factor.f90:1008-1027)
+  const double norm = (double)std::max<int64_t>(p->nframes, 1) * (double)p->desc.natoms;
+  for (int k = 0; k < nb; ++k) {
+    if (two_theta) two_theta[k] = b.xmin + ((double)k + 0.5) * b.xstep;
+    if (I) I[k] = xs[(size_t)k] / norm;
+    if (count) count[k] = (int64_t)std::llround(xc[(size_t)k]);
+  }
+  if (I_partial) {
+    std::memset(I_partial, 0, sizeof(double) * (size_t)T * T * nb);
+    if (p->desc.partials) {
+      int q = 1;
+      for (int a = 0; a < p->ntr; ++a)
+        for (int c = a; c < p->ntr; ++c, ++q) {
+          const int ta = p->species_type[a], tb = p->species_type[c];
+          for (int k = 0; k < nb; ++k)
+            I_partial[(size_t)(ta - 1) + (size_t)T * ((size_t)(tb - 1) + (size_t)T * k)] =
+                xs[(size_t)q * nb + k] / norm;
+        }
+    }
+  }
+  if (nframes) *nframes = p->nframes;
+  return SQN_OK;
+}
+
 int sqn_accumulator_view(sqn_plan *p, double **acc, int64_t *count, int64_t *nframes) {
   if (!p) return SQN_ERR_PLAN_NOTVALID;
   if (!acc || !count) return SQN_ERR_INVALID_ARGUMENT;
   DeviceGuard guard(p->device);
   if (cudaStreamSynchronize(p->stream) != cudaSuccess) return SQN_ERR_CUDA;
   *acc = p->d_acc;
-  *count = (int64_t)p->nquant * p->desc.nq + p->gnum_half;
+  *count = p->nsums + p->gnum_half;
   if (nframes) *nframes = p->nframes;
   return SQN_OK;
 }
@@ -1241,8 +1328,7 @@ int sqn_reset(sqn_plan *p) {
   if (!p) return SQN_ERR_PLAN_NOTVALID;
   DeviceGuard guard(p->device);
   if (cudaStreamSynchronize(p->stream) != cudaSuccess) return SQN_ERR_CUDA;
-  cudaError_t e = cudaMemset(p->d_acc, 0,
-                             sizeof(double) * ((size_t)p->nquant * p->desc.nq + (size_t)p->gnum_half));
+  cudaError_t e = cudaMemset(p->d_acc, 0, sizeof(double) * ((size_t)p->nsums + (size_t)p->gnum_half));
   p->nframes = 0;
   p->tev_used = 0;
   for (double &v : p->stage_ms) v = 0.0;

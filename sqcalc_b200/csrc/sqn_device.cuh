@@ -199,6 +199,23 @@ __device__ __forceinline__ R es_at(int k, R off, R halfw, R c2, R beta) {
   return es_phi(((R)k - halfw) - off, c2, beta);
 }
 
+// Two-theta bin and weight of a mode of length q (two_theta_deg, lorentz_polarization
+// and the bin rule of sf_configure_xrd, src/sqc_structure_factor.f90:894-924).
+__device__ __forceinline__ void xrd_bin_weight(const BinGeom &b, double q, int &xb, double &wt) {
+  constexpr double kPi = 3.14159265358979323846;
+  double st = q * b.xlambda / (4.0 * kPi);
+  st = fmax(-1.0, fmin(1.0, st));
+  const double tth = 2.0 * asin(st) * 180.0 / kPi;
+  xb = (int)((tth - b.xmin) / b.xstep);
+  xb = min(max(xb, 0), b.xbins - 1);
+  wt = 1.0;
+  if (b.xlp) {
+    const double t2 = tth * (kPi / 180.0), th = 0.5 * t2;
+    const double c2 = cos(t2), sth = sin(th);
+    wt = (1.0 + c2 * c2) / (sth * sth * cos(th));
+  }
+}
+
 // One mode per lane, called by all 32 lanes of a warp: classify the mode
 // (kept test and shell, identical to the reference's FP64 evaluation),
 // deconvolve the transforms' values v[t] by dec = 1 / (phihat1 phihat2
@@ -209,25 +226,27 @@ __device__ __forceinline__ R es_at(int k, R off, R halfw, R c2, R beta) {
 // gnum[gidx] (each mode is visited once per frame).  The reference's
 // counterpart is the host loops of src/sqc_structure_factor.f90:481-521
 // and :595-643.
-template <typename R, int TM, bool XR>
+template <typename R, int TM, bool XR, bool XD = false>
 __device__ __forceinline__ void bin_mode(const BinGeom &b, int ntr, bool inrange, int h1, int h2,
                                          int h3, const double *crow,
                                          const typename Cplx<R>::T (&v)[TM], R dec,
                                          const double *__restrict__ amp,
                                          const double *__restrict__ xcoef, double *hist,
-                                         double *__restrict__ gnum, int64_t gidx, int lane) {
+                                         double *__restrict__ gnum, int64_t gidx, int lane,
+                                         double *xhist = nullptr) {
   double ql = 0.0;
   int s = 0;
   const bool keep = inrange && classify_mode(b, crow, h1, h2, h3, s, ql);
   const unsigned act = __ballot_sync(FULL, keep);
   if (act == 0u) return;
-  double re[TM], im[TM];
+  double re[TM], im[TM], am[TM];
   double tre = 0.0, tim = 0.0;
   const double mult = h1 > 0 ? 2.0 : 1.0;
 #pragma unroll
   for (int t = 0; t < TM; ++t) {
     re[t] = 0.0;
     im[t] = 0.0;
+    am[t] = 0.0;
   }
   if (keep) {
 #pragma unroll
@@ -235,9 +254,9 @@ __device__ __forceinline__ void bin_mode(const BinGeom &b, int ntr, bool inrange
       if (t < ntr) {
         re[t] = (double)(v[t].x * dec);
         im[t] = (double)(v[t].y * dec);
-        const double a = XR ? xray_f(xcoef + 9 * t, ql) : amp[t];
-        tre += a * re[t];
-        tim += a * im[t];
+        am[t] = XR ? xray_f(xcoef + 9 * t, ql) : amp[t];
+        tre += am[t] * re[t];
+        tim += am[t] * im[t];
       }
     }
   }
@@ -256,6 +275,32 @@ __device__ __forceinline__ void bin_mode(const BinGeom &b, int ntr, bool inrange
           hist_add(hist + p * b.nq, s, mult * (re[a] * re[c] + im[a] * im[c]), keep, uni, s0,
                    lane);
           ++p;
+        }
+      }
+    }
+  }
+  if (XD && xhist) {
+    // powder pattern: the same per-mode quantities, binned in two-theta with the
+    // Lorentz-polarization weight; the pair products carry the amplitudes
+    // (sf_accumulate_values :616-619, sf_accumulate_xrd_partials :538-588)
+    int xb = 0;
+    double wt = 0.0;
+    if (keep) xrd_bin_weight(b, qlen_exact(b, h1, h2, h3), xb, wt);
+    const int xb0 = __shfl_sync(FULL, xb, __ffs(act) - 1);
+    const bool xuni = __all_sync(FULL, !keep || xb == xb0);
+    hist_add(xhist, xb, mult * wt * I, keep, xuni, xb0, lane);
+    if (b.partials) {
+      int p = 1;
+#pragma unroll
+      for (int a = 0; a < TM; ++a) {
+#pragma unroll
+        for (int c = a; c < TM; ++c) {
+          if (c < ntr) {
+            hist_add(xhist + p * b.xbins, xb,
+                     mult * wt * am[a] * am[c] * (re[a] * re[c] + im[a] * im[c]), keep, xuni,
+                     xb0, lane);
+            ++p;
+          }
         }
       }
     }

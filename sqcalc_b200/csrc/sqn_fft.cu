@@ -395,13 +395,14 @@ __global__ void __launch_bounds__(FFT_Z_THREADS, 2)
   const int n = ax.n, ld = padi(n) + 1;
   const int ntr = NT > 0 ? NT : b.ntr;
   const int hm2 = b.hm[2], M2 = 2 * hm2 + 1;
-  const int nhist = b.nquant * b.nq;
+  const int nhist = hist_len(b);
   C *s_tw = reinterpret_cast<C *>(smem);
   C *a = s_tw + n;
   C *bb = a + PC * ld;
   C *res = bb + PC * ld;  // [ntr][PC][M2]
   double *s_hist = reinterpret_cast<double *>(res + ntr * PC * M2);
   double *hist = SMEM ? s_hist : acc;
+  double *xhist = b.xrd ? hist + b.nquant * b.nq : nullptr;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
   load_twiddles(s_tw, tw, n);
   if (SMEM)
@@ -462,8 +463,8 @@ __global__ void __launch_bounds__(FFT_Z_THREADS, 2)
       const R dec = inr ? inv1[h1] * (d2 * inv3[abs(h3)]) : R(0);
       const int64_t gidx =
           ((int64_t)(h3 + hm2) * b.m2 + (int64_t)(h2 + b.hm[1])) * (int64_t)(b.hm[0] + 1) + h1;
-      bin_mode<R, TM, XR>(b, ntr, inr, h1, h2, h3, crow, v, dec, amp, xcoef, hist, gnum, gidx,
-                          lane);
+      bin_mode<R, TM, XR, true>(b, ntr, inr, h1, h2, h3, crow, v, dec, amp, xcoef, hist, gnum,
+                                gidx, lane, xhist);
     }
     __syncthreads();  // res and s_span are rewritten by the next item
   }
@@ -500,7 +501,7 @@ cudaError_t launch_z_xr(const FftPlan3 &f, const void *A2, const BinGeom &b, con
                         const R *i2, const R *i3, const double *amp, const double *xc,
                         double *acc, double *gnum, cudaStream_t s) {
   using C = typename Cplx<R>::T;
-  const size_t hist = SMEM ? (size_t)b.nquant * b.nq * sizeof(double) : 0;
+  const size_t hist = SMEM ? (size_t)hist_len(b) * sizeof(double) : 0;
   const size_t sm = pass3_smem<R>(f.ax[2].n, PC, b.ntr, 2 * b.hm[2] + 1, hist);
   cudaError_t e;
   if (b.xray) {
@@ -568,11 +569,11 @@ cudaError_t launch_xy_pc(const FftPlan3 &f, const void *grid, void *A1, void *A2
 int fft_columns_per_cta(bool fp64) { return fp64 ? 2 : 4; }
 int fft_z_columns_per_cta(bool fp64) { return fp64 ? 2 : 4; }
 
-size_t fft_pass_smem(const FftPlan3 &f, int pass, bool fp64, int ntr, int nquant, int nq) {
+size_t fft_pass_smem(const FftPlan3 &f, int pass, bool fp64, int ntr, int nhist) {
   const int pc = fft_columns_per_cta(fp64);
   if (pass < 2)
     return fp64 ? pass12_smem<double>(f.ax[pass].n, pc) : pass12_smem<float>(f.ax[pass].n, pc);
-  const size_t hist = f.hist_smem ? (size_t)nquant * nq * sizeof(double) : 0;
+  const size_t hist = f.hist_smem ? (size_t)nhist * sizeof(double) : 0;
   return fp64 ? pass3_smem<double>(f.ax[2].n, fft_z_columns_per_cta(fp64), ntr, f.M2, hist)
               : pass3_smem<float>(f.ax[2].n, fft_z_columns_per_cta(fp64), ntr, f.M2, hist);
 }

@@ -76,7 +76,16 @@ struct BinGeom {
   int m2;             // modes[1]
   int norm;
   int64_t natoms;
+  // powder XRD pattern: xquant * xbins sums right after the nquant * nq shell
+  // sums in the accumulator buffer
+  int xrd, xbins, xquant, xlp;
+  double xlambda, xmin, xstep;  // Angstrom, degrees, degrees
 };
+
+// FP64 sums of one frame pass: shell sums, then the powder-pattern sums.
+__host__ __device__ inline int hist_len(const BinGeom &b) {
+  return b.nquant * b.nq + (b.xrd ? b.xquant * b.xbins : 0);
+}
 
 // Launch wrappers (sqn_kernels.cu).  Each returns cudaGetLastError().
 template <typename R>
@@ -97,7 +106,7 @@ cudaError_t launch_bin(const int4 *rows, int nrows, const void *G, const BinGeom
                        cudaStream_t s);
 cudaError_t launch_norms(const int4 *rows, int nrows, const BinGeom &b, const double *amp,
                          const double *xcoef, const double *counts_t, double *den,
-                         double *cnt, int nsm, cudaStream_t s);
+                         double *cnt, double *xcnt, int nsm, cudaStream_t s);
 size_t spread_smem_bytes(int chunk, bool fp64);
 int spread_chunk(bool fp64, int ntr);
 cudaError_t spread_set_attributes();
@@ -138,7 +147,7 @@ struct FftPlan3 {
 };
 int fft_columns_per_cta(bool fp64);
 int fft_z_columns_per_cta(bool fp64);
-size_t fft_pass_smem(const FftPlan3 &f, int pass, bool fp64, int ntr, int nquant, int nq);
+size_t fft_pass_smem(const FftPlan3 &f, int pass, bool fp64, int ntr, int nhist);
 template <typename R>
 cudaError_t launch_fft_xy(const FftPlan3 &f, const void *grid, void *A1, void *A2,
                           const BinGeom &b, int64_t pitch, cudaStream_t s);

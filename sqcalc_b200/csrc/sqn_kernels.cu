@@ -393,7 +393,7 @@ __global__ void __launch_bounds__(SPREAD_THREADS, (sizeof(R) == 4 || NT == 1) ? 
 // Rows (h2, h3) are dealt to warps; lanes walk h1 >= 0 (32 consecutive complex
 // values per warp and transform, one coalesced read).
 // ---------------------------------------------------------------------------
-template <typename R, int NT, bool SMEM, bool XR>
+template <typename R, int NT, bool SMEM, bool XR, bool XD>
 __global__ void __launch_bounds__(256, 2)
     k_bin(const int4 *__restrict__ rows, int nrows, const typename Cplx<R>::T *__restrict__ G,
           BinGeom b, const R *__restrict__ inv1, const R *__restrict__ inv2,
@@ -402,8 +402,9 @@ __global__ void __launch_bounds__(256, 2)
   extern __shared__ double s_hist[];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nwarps = blockDim.x >> 5;
-  const int nhist = b.nquant * b.nq;
+  const int nhist = hist_len(b);
   double *hist = SMEM ? s_hist : acc;
+  double *xhist = XD ? hist + b.nquant * b.nq : nullptr;
   if (SMEM) {
     for (int i = tid; i < nhist; i += blockDim.x) s_hist[i] = 0.0;
     __syncthreads();
@@ -433,8 +434,8 @@ __global__ void __launch_bounds__(256, 2)
       for (int t = 0; t < TM; ++t)
         if (t < ntr && inrow) v[t] = G[(int64_t)t * b.vol_cplx + rowbase + h1];
       const R dec = inrow ? inv1[h1] * dyz : R(0);
-      bin_mode<R, TM, XR>(b, ntr, inrow, h1, h2, h3, crow, v, dec, amp, xcoef, hist, gnum,
-                          gbase + h1, lane);
+      bin_mode<R, TM, XR, XD>(b, ntr, inrow, h1, h2, h3, crow, v, dec, amp, xcoef, hist, gnum,
+                              gbase + h1, lane, xhist);
     }
   }
   if (SMEM) {
@@ -451,11 +452,12 @@ __global__ void __launch_bounds__(256, 2)
 __global__ void __launch_bounds__(256)
     k_norms(const int4 *__restrict__ rows, int nrows, BinGeom b, const double *__restrict__ amp,
             const double *__restrict__ xcoef, const double *__restrict__ counts_t,
-            double *__restrict__ den, double *__restrict__ cnt) {
+            double *__restrict__ den, double *__restrict__ cnt, double *__restrict__ xcnt) {
   extern __shared__ double s_n[];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nwarps = blockDim.x >> 5;
-  for (int i = tid; i < 2 * b.nq; i += blockDim.x) s_n[i] = 0.0;
+  const int nx = b.xrd ? b.xbins : 0;
+  for (int i = tid; i < 2 * b.nq + nx; i += blockDim.x) s_n[i] = 0.0;
   __syncthreads();
   for (int r = blockIdx.x * nwarps + warp; r < nrows; r += gridDim.x * nwarps) {
     const int4 row = rows[r];
@@ -486,6 +488,12 @@ __global__ void __launch_bounds__(256)
       }
       atomicAdd(&s_n[s], mult * d);
       atomicAdd(&s_n[b.nq + s], mult);
+      if (nx) {
+        int xb;
+        double wt;
+        xrd_bin_weight(b, ql, xb, wt);
+        atomicAdd(&s_n[2 * b.nq + xb], mult);
+      }
     }
   }
   __syncthreads();
@@ -493,6 +501,8 @@ __global__ void __launch_bounds__(256)
     if (s_n[i] != 0.0) atomicAdd(&den[i], s_n[i]);
     if (s_n[b.nq + i] != 0.0) atomicAdd(&cnt[i], s_n[b.nq + i]);
   }
+  for (int i = tid; i < nx; i += blockDim.x)
+    if (s_n[2 * b.nq + i] != 0.0) atomicAdd(&xcnt[i], s_n[2 * b.nq + i]);
 }
 
 }  // namespace
@@ -610,17 +620,28 @@ static cudaError_t bin_dispatch_xr(const int4 *rows, int nrows, const void *G, c
                                    const double *xc, double *acc, double *gnum, int nsm,
                                    cudaStream_t s) {
   using C = typename Cplx<R>::T;
-  const size_t hist = (size_t)b.nquant * b.nq * sizeof(double);
+  const size_t hist = (size_t)hist_len(b) * sizeof(double);
   const int blocks = nsm * 4;
   if (hist <= 160 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(k_bin<R, NT, true, XR>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hist);
-    if (e != cudaSuccess) return e;
-    k_bin<R, NT, true, XR><<<blocks, 256, hist, s>>>(rows, nrows, (const C *)G, b, i1, i2, i3,
-                                                     amp, xc, acc, gnum);
+    if (b.xrd) {
+      cudaError_t e = cudaFuncSetAttribute(k_bin<R, NT, true, XR, true>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hist);
+      if (e != cudaSuccess) return e;
+      k_bin<R, NT, true, XR, true><<<blocks, 256, hist, s>>>(rows, nrows, (const C *)G, b, i1,
+                                                             i2, i3, amp, xc, acc, gnum);
+    } else {
+      cudaError_t e = cudaFuncSetAttribute(k_bin<R, NT, true, XR, false>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hist);
+      if (e != cudaSuccess) return e;
+      k_bin<R, NT, true, XR, false><<<blocks, 256, hist, s>>>(rows, nrows, (const C *)G, b, i1,
+                                                              i2, i3, amp, xc, acc, gnum);
+    }
+  } else if (b.xrd) {
+    k_bin<R, NT, false, XR, true><<<blocks, 256, 0, s>>>(rows, nrows, (const C *)G, b, i1, i2, i3,
+                                                         amp, xc, acc, gnum);
   } else {
-    k_bin<R, NT, false, XR><<<blocks, 256, 0, s>>>(rows, nrows, (const C *)G, b, i1, i2, i3, amp,
-                                                   xc, acc, gnum);
+    k_bin<R, NT, false, XR, false><<<blocks, 256, 0, s>>>(rows, nrows, (const C *)G, b, i1, i2,
+                                                          i3, amp, xc, acc, gnum);
   }
   return cudaGetLastError();
 }
@@ -651,12 +672,12 @@ cudaError_t launch_bin(const int4 *rows, int nrows, const void *G, const BinGeom
 
 cudaError_t launch_norms(const int4 *rows, int nrows, const BinGeom &b, const double *amp,
                          const double *xcoef, const double *counts_t, double *den, double *cnt,
-                         int nsm, cudaStream_t s) {
-  const size_t sh = 2 * (size_t)b.nq * sizeof(double);
+                         double *xcnt, int nsm, cudaStream_t s) {
+  const size_t sh = (2 * (size_t)b.nq + (b.xrd ? (size_t)b.xbins : 0)) * sizeof(double);
   cudaError_t e = cudaFuncSetAttribute(k_norms, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)sh);
   if (e != cudaSuccess) return e;
-  k_norms<<<nsm * 4, 256, sh, s>>>(rows, nrows, b, amp, xcoef, counts_t, den, cnt);
+  k_norms<<<nsm * 4, 256, sh, s>>>(rows, nrows, b, amp, xcoef, counts_t, den, cnt, xcnt);
   return cudaGetLastError();
 }
 

@@ -90,7 +90,7 @@ class GpuStructureFactor:
 
     def __init__(self, norm="mean", nq=500, qmin=0.0, qmax=20.0, eps=None, want_grid=False,
                  partials=True, faber_ziman=False, precision="double", device=0,
-                 upsampfac=0.0, kernel_width=0, max_grid_modes=0, timing=False):
+                 upsampfac=0.0, kernel_width=0, max_grid_modes=0, timing=False, xrd=None):
         self.norm = NORM_NAMES[norm] if isinstance(norm, str) else int(norm)
         self.nq = int(nq)
         self.qmin = float(qmin)
@@ -109,6 +109,7 @@ class GpuStructureFactor:
         self.kernel_width = int(kernel_width)
         self.max_grid_modes = int(max_grid_modes)
         self.timing = bool(timing)
+        self.xrd = xrd  # None or dict(lam=..., range=(lo, hi), step=..., lp=...)
         self.plan = None
         self.scheme = None
         self.natoms = 0
@@ -140,7 +141,8 @@ class GpuStructureFactor:
                                   want_grid=self.want_grid, precision=self.precision,
                                   eps=self.eps, upsampfac=self.upsampfac,
                                   kernel_width=self.kernel_width, device=self.device,
-                                  max_grid_modes=self.max_grid_modes, timing=self.timing)
+                                  max_grid_modes=self.max_grid_modes, timing=self.timing,
+                                  xrd=self.xrd)
         except _lib.SqnError as e:
             if e.code == 42:
                 raise SqcalcError("reciprocal grid exceeds the limit of modes; reduce --qmax")
@@ -202,6 +204,41 @@ class GpuStructureFactor:
                     q = kept.qvec[i]
                     fh.write("%14.8f  %14.8f  %14.8f  %s\n" % (q[0], q[1], q[2], fortran_es(Sg[i])))
         return S, Sp, Sg
+
+    def write_xrd(self, path):
+        """The powder pattern table of sf_write_xrd (src/sqc_structure_factor.f90:964-1031)."""
+        if not self.xrd:
+            return None
+        tth, I, Ip, cnt, nf = self.plan.xrd()
+        lo, hi = self.xrd.get("range", (1.0, 179.0))
+        step = float(self.plan.info.xrd_step)
+        cols = []
+        if self.partials:
+            for t in range(1, self.ntypes + 1):
+                for u in range(t, self.ntypes + 1):
+                    if self.type_counts[t - 1] == 0 or self.type_counts[u - 1] == 0:
+                        continue
+                    cols.append((t, u, "I(" + self.scheme.pair_label(t, u) + ")"))
+        with open(path, "w") as fh:
+            fh.write("# xrd: lambda %.6f A, 2theta %.4f to %.4f deg, step %.5f deg, %d bins, %s\n"
+                     % (self.xrd["lam"], lo, hi, step, len(tth),
+                        "1 frame" if nf == 1 else "%d frames" % nf))
+            if self.xrd.get("lp", True):
+                fh.write("# I(2theta) = sum over the reciprocal lattice points in each bin of "
+                         "|rho(q)|^2 times the Lorentz-polarization factor, per atom\n")
+            else:
+                fh.write("# I(2theta) = sum over the reciprocal lattice points in each bin of "
+                         "|rho(q)|^2, without the Lorentz-polarization factor, per atom\n")
+            if cols:
+                fh.write("# the pair columns add up to the total: "
+                         "I = sum_a I(a-a) + 2 sum_{a<b} I(a-b)\n")
+            fh.write("# 2theta[deg] I" + "".join(" " + c[2] for c in cols) + "\n")
+            for k in range(len(tth)):
+                line = "%12.4f  %s" % (tth[k], fortran_es(I[k]))
+                for t, u, _ in cols:
+                    line += "  " + fortran_es(Ip[t - 1, u - 1, k])
+                fh.write(line + "\n")
+        return tth, I, Ip, cnt
 
     def close(self):
         if self.plan is not None:

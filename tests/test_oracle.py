@@ -105,3 +105,17 @@ def test_enumeration_counts_match_reference_formula():
     m = np.zeros(3, dtype=np.int32)
     O.lib().sqo_modes(np.ascontiguousarray((np.eye(3) * 220.0).reshape(9)), 6.0, m)
     assert list(m) == [423, 423, 423]
+
+
+def test_xrd_conversions_known_answers():
+    # the reference's own checks of the two-theta and LP conversions
+    # (test/test_xrd.f90): fcc Ni (a = 3.52 A) reflections at Cu Kalpha
+    lam = 1.541838
+    for hkl, want in (((1, 1, 1), 44.585405), ((2, 0, 0), 51.955510), ((2, 2, 0), 76.552967)):
+        q = np.sqrt(sum(h * h for h in hkl)) * 2.0 * np.pi / 3.52
+        assert abs(O.two_theta_deg(q, lam) - want) / want < 1e-7
+    q = 4.0 * np.pi * np.sin(np.pi / 8.0) / lam
+    assert abs(O.two_theta_deg(q, lam) - 45.0) < 1e-9
+    assert O.two_theta_deg(1e9, lam) == 180.0
+    assert abs(O.lorentz_polarization(90.0) - 2.0 * np.sqrt(2.0)) < 1e-12
+    assert O.lorentz_polarization(1.0) > O.lorentz_polarization(90.0) < O.lorentz_polarization(179.0)
