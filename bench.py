@@ -350,7 +350,7 @@ def batched_leg(W, K, stream, dist, local_rank):
     return out
 
 
-def ingest_leg(types, frames, stream, local_rank, nframes=3):
+def ingest_leg(types, frames, stream, local_rank, nframes=4):
     """End to end from a LAMMPS text dump: the precision-form frames written
     as text (id type x y z, %.6f), then read by the library's multithreaded
     reader and streamed through sqn_accumulate_dump (the parse of frame f + 1
@@ -384,8 +384,8 @@ def ingest_leg(types, frames, stream, local_rank, nframes=3):
                        qmax=QMAX, nq=NQ, partials=True, precision=_lib.PREC_SINGLE, eps=EPS,
                        device=local_rank, stream=stream.cuda_stream) as p, \
                 _lib.DumpReader(path, nthreads=cores) as r:
-            p.accumulate(frames[0])  # warm the plan
-            p.sync()
+            p.accumulate_dump(r, max_frames=1)  # warm the plan and pin the buffers
+            r.rewind()
             p.reset()
             torch.cuda.synchronize()
             t0 = time.perf_counter()

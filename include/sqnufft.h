@@ -294,7 +294,8 @@ int sqn_type1_destroy(sqn_type1_plan *plan);
  * reference's species set up once) and the box bounds ref_bounds[9] (NULL: those
  * of the first frame read) to 1e-6 relative (else SQN_ERR_DUMP with
  * sqn_dump_last_error 10, the reference driver's "box changes" stop); syncs
- * before returning. */
+ * before returning.  The two pinned frame buffers belong to the dump handle:
+ * allocated by the first call, reused by later ones, freed by sqn_dump_close. */
 typedef struct sqn_dump_s sqn_dump;
 int sqn_dump_open(const char *path, int32_t nthreads, sqn_dump **dump);
 int sqn_dump_next(sqn_dump *dump, int64_t capacity, int64_t *natoms, int64_t *timestep,

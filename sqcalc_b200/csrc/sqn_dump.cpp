@@ -48,6 +48,10 @@ struct sqn_dump_s {
   int nthreads = 1;
   int last_error = 0;
   int64_t frames = 0;
+  // pinned frames of sqn_accumulate_dump, kept for later calls (freed at close)
+  double *pinned[2] = {nullptr, nullptr};
+  int32_t *types = nullptr;
+  int64_t pinned_atoms = 0;
 };
 
 namespace {
@@ -304,6 +308,9 @@ int sqn_dump_rewind(sqn_dump *d) {
 
 int sqn_dump_close(sqn_dump *d) {
   if (!d) return SQN_ERR_PLAN_NOTVALID;
+  for (double *b : d->pinned)
+    if (b) cudaFreeHost(b);
+  std::free(d->types);
   if (d->base) munmap(const_cast<char *>(d->base), d->size);
   if (d->fd >= 0) ::close(d->fd);
   delete d;
@@ -322,20 +329,26 @@ int sqn_accumulate_dump(sqn_plan *plan, sqn_dump *d, int64_t max_frames,
   if (st) return st;
   const int64_t cap = info.natoms;  // every frame must hold the plan's atoms
   if (cap <= 0) return SQN_ERR_PLAN_NOTVALID;
-  double *buf[2] = {nullptr, nullptr};
-  int32_t *types = nullptr;
-  if (cudaMallocHost(&buf[0], sizeof(double) * 3 * (size_t)cap) != cudaSuccess ||
-      cudaMallocHost(&buf[1], sizeof(double) * 3 * (size_t)cap) != cudaSuccess) {
-    cudaGetLastError();
-    if (buf[0]) cudaFreeHost(buf[0]);
-    return SQN_ERR_ALLOC;
+  if (d->pinned_atoms < cap) {
+    for (double *&b : d->pinned)
+      if (b) {
+        cudaFreeHost(b);
+        b = nullptr;
+      }
+    std::free(d->types);
+    d->types = nullptr;
+    d->pinned_atoms = 0;
+    if (cudaMallocHost(&d->pinned[0], sizeof(double) * 3 * (size_t)cap) != cudaSuccess ||
+        cudaMallocHost(&d->pinned[1], sizeof(double) * 3 * (size_t)cap) != cudaSuccess) {
+      cudaGetLastError();
+      return SQN_ERR_ALLOC;
+    }
+    d->types = static_cast<int32_t *>(std::malloc(sizeof(int32_t) * (size_t)cap));
+    if (!d->types) return SQN_ERR_ALLOC;
+    d->pinned_atoms = cap;
   }
-  types = static_cast<int32_t *>(std::malloc(sizeof(int32_t) * (size_t)cap));
-  if (!types) {
-    cudaFreeHost(buf[0]);
-    cudaFreeHost(buf[1]);
-    return SQN_ERR_ALLOC;
-  }
+  double *buf[2] = {d->pinned[0], d->pinned[1]};
+  int32_t *types = d->types;
   // Parser thread: fills buffer k, then waits until the main thread has handed
   // that buffer to the plan (sqn_accumulate_frames returns once it has been read).
   std::mutex mu;
@@ -427,9 +440,6 @@ int sqn_accumulate_dump(sqn_plan *plan, sqn_dump *d, int64_t max_frames,
   parser.join();
   if (frames_done) *frames_done = done;
   const int sync = sqn_sync(plan);
-  cudaFreeHost(buf[0]);
-  cudaFreeHost(buf[1]);
-  std::free(types);
   return st != SQN_OK ? st : sync;
 }
 
