@@ -202,6 +202,20 @@ int sqn_reset(sqn_plan *plan);
 int sqn_get_xrd(sqn_plan *plan, double *two_theta, double *I, double *I_partial, int64_t *count,
                 int64_t *nframes);
 
+/* Density amplitudes of one frame at reciprocal lattice points, the per-frame
+ * input of sqcalc dyn on a grid (--qpoints grid): rho_a(q_h) = sum_{j of type a}
+ * exp(i q_h . r_j), which the reference sums directly, O(N nq) per frame
+ * (dyn_accumulate, src/sqc_dynamics.f90:792-880); here all of them come from one
+ * pass of the frame transforms.  hkl [nmodes][3] host int32 lattice indices with
+ * |h_d| <= (modes_d - 1)/2 (others give 0); rho [nspecies][nmodes] host, as
+ * interleaved (re, im) doubles, species in ascending type id.  Needs a plan with a
+ * transform per species (partials or x-ray weights) on the cuFFT path; does not
+ * touch the accumulators.  The plan's eps holds for |q_h| <= qmax; toward the corners
+ * of the mode cube the deconvolution amplifies the grid's rounding (FP32 plans lose
+ * digits there, FP64 plans stay near eps).  Synchronous. */
+int sqn_density_modes(sqn_plan *plan, const double *pos, int32_t where, const int32_t *hkl,
+                      int64_t nmodes, double *rho);
+
 /* Frames sharded over ranks (one process per GPU, each with its own plan on
  * the same system).  The plan's FP64 sums -- shell sums, pair sums and, with
  * want_grid, the per-mode sums -- are one device buffer of *count doubles at

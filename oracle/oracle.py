@@ -394,6 +394,25 @@ def xrd_bins(cell, lam, tmin, tmax, step=0.0):
     return nb, (tmax - tmin) / nb
 
 
+def direct_density(pos, type_id, cell, hkl):
+    """rho_a(q_h) = sum_{j of type a} exp(+i q_h . r_j) for the lattice points hkl
+    (q_h = h1 b1 + h2 b2 + h3 b3), absolute positions, species in ascending type id:
+    the direct sum of dyn_accumulate (src/sqc_dynamics.f90:860-875).  Returns
+    complex128 (nspecies, nmodes)."""
+    L = lib()
+    flat = _c(np.asarray(cell, dtype=np.float64).reshape(9), np.float64)
+    inv = np.zeros(9)
+    recip = np.zeros(9)
+    L.sqo_cell_setup(flat, inv, recip)
+    q = np.asarray(hkl, dtype=np.float64).reshape(-1, 3) @ recip.reshape(3, 3)
+    type_id = np.asarray(type_id)
+    pos = np.asarray(pos, dtype=np.float64)
+    out = []
+    for t in np.unique(type_id):
+        out.append(np.exp(1j * (pos[type_id == t] @ q.T)).sum(axis=0))
+    return np.stack(out)
+
+
 def direct_xrd(frames, type_id, cell, origin, weights: Weights, lam, tmin, tmax, step=0.0,
                lp=True, ntypes=None):
     """FP64 direct-sum powder pattern over the kept modes of the q range the

@@ -37,7 +37,7 @@ EXPORTS = (
     "sqn_type1_makeplan", "sqn_type1f_makeplan", "sqn_type1_setpts", "sqn_type1f_setpts",
     "sqn_type1_execute", "sqn_type1f_execute", "sqn_type1_destroy", "sqn_dump_open",
     "sqn_dump_next", "sqn_dump_last_error", "sqn_dump_rewind", "sqn_dump_close",
-    "sqn_accumulate_dump", "sqn_get_xrd",
+    "sqn_accumulate_dump", "sqn_get_xrd", "sqn_density_modes",
 )
 ERR_DUMP = 50
 ERR_SCRATCH_LIMIT = 49
@@ -181,6 +181,7 @@ def load():
     L.sqn_dump_close.argtypes = [vp]
     L.sqn_accumulate_dump.argtypes = [vp, vp, i64, vp, ctypes.POINTER(i64)]
     L.sqn_get_xrd.argtypes = [vp, vp, vp, vp, vp, vp]
+    L.sqn_density_modes.argtypes = [vp, vp, ctypes.c_int32, vp, i64, vp]
     L.sqn_spread_frame_noalloc.argtypes = [vp, i64, vp, ctypes.c_int32, vp, vp, vp, vp,
                                            ctypes.c_int32, ctypes.c_double, vp, vp]
     if L.sqn_abi_version() != ABI_VERSION:
@@ -356,6 +357,25 @@ class Plan:
         check(self._L.sqn_sq_grad(self._h, _ptr(a), HOST, _ptr(g), _ptr(S), _ptr(grad)),
               "sqn_sq_grad")
         return S, grad
+
+    def density_modes(self, pos, hkl):
+        """rho_a(q_h) = sum_{j of type a} exp(i q_h . r_j) of one frame at the lattice
+        points hkl (nmodes, 3) int; returns complex128 (nspecies, nmodes), species in
+        ascending type id.  pos: (natoms, 3) float64 host array or torch CUDA tensor."""
+        h = np.ascontiguousarray(hkl, dtype=np.int32).reshape(-1, 3)
+        nsp = int(self.info.nspecies)
+        rho = np.zeros((nsp, h.shape[0], 2))
+        if hasattr(pos, "data_ptr"):
+            import torch
+            pos = pos.contiguous()
+            torch.cuda.current_stream().synchronize()
+            check(self._L.sqn_density_modes(self._h, ctypes.c_void_p(pos.data_ptr()), DEVICE,
+                                            _ptr(h), h.shape[0], _ptr(rho)), "sqn_density_modes")
+        else:
+            a = np.ascontiguousarray(pos, dtype=np.float64)
+            check(self._L.sqn_density_modes(self._h, _ptr(a), HOST, _ptr(h), h.shape[0],
+                                            _ptr(rho)), "sqn_density_modes")
+        return rho[..., 0] + 1j * rho[..., 1]
 
     def xrd(self):
         """Powder pattern per atom and frame: (two_theta, I, I_partial (T, T, bins),

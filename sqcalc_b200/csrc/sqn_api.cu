@@ -269,6 +269,10 @@ struct sqn_plan_s {
     return (flags & SQN_FLAG_FUSED_FFT) && !(flags & SQN_FLAG_CUFFT);
   }
   int64_t c1pitch = 0;  // complex row pitch of the half spectrum
+  // density amplitudes (sqn_density_modes): request buffers, grown on demand
+  int *d_hkl = nullptr;
+  double *d_rho = nullptr;
+  int64_t modes_cap = 0;
   FftPlan3 fp{};
   // adjoint (SQN_FLAG_GRAD)
   bool grad_ok = false;
@@ -323,6 +327,8 @@ void free_plan(sqn_plan *p) {
   if (p->fft_fwd1_ok) cufftDestroy(p->fft_fwd1);
   if (p->fft_inv3_ok) cufftDestroy(p->fft_inv3);
   for (void *v : p->allocs) cudaFree(v);
+  if (p->d_hkl) cudaFree(p->d_hkl);
+  if (p->d_rho) cudaFree(p->d_rho);
   for (int i = 0; i < 2; ++i) {
     if (p->ev_copied[i]) cudaEventDestroy(p->ev_copied[i]);
     if (p->ev_free[i]) cudaEventDestroy(p->ev_free[i]);
@@ -938,6 +944,32 @@ template <typename R> int grad_frame(sqn_plan *p, const double *dpos, bool want_
   return SQN_OK;
 }
 
+// One frame's per-species spectra (sort, spread, R2C) without binning, then
+// the density amplitudes of the requested lattice points.
+template <typename R> int density_frame(sqn_plan *p, const double *dpos, int64_t nm) {
+  const FrameGeom &g = p->fg;
+  cudaStream_t s = p->stream;
+  cudaError_t e = launch_prep<R>(dpos, p->d_species, g, p->d_counts, p->d_key, p->d_slot, s);
+  if (e == cudaSuccess) e = launch_scan(p->d_counts, p->d_starts, p->nkeys, s);
+  if (e == cudaSuccess)
+    e = launch_scatter<R>(dpos, p->d_species, g, p->d_key, p->d_slot, p->d_starts,
+                          (R *)p->d_recs, nullptr, s);
+  if (e == cudaSuccess)
+    e = launch_spread<R>((const R *)p->d_recs, p->d_starts, g, (const R *)p->d_strength,
+                         (R *)p->d_grid, s);
+  if (e != cudaSuccess) return SQN_ERR_CUDA;
+  cufftResult fr = p->fp64 ? cufftExecD2Z(p->fft, (cufftDoubleReal *)p->d_grid,
+                                          (cufftDoubleComplex *)p->d_G)
+                           : cufftExecR2C(p->fft, (cufftReal *)p->d_grid, (cufftComplex *)p->d_G);
+  if (fr != CUFFT_SUCCESS) return SQN_ERR_CUFFT;
+  e = launch_gather_modes<R>(p->d_G, p->bg, p->d_hkl, nm, (const R *)p->d_inv[0],
+                             (const R *)p->d_inv[1], (const R *)p->d_inv[2], p->origin,
+                             p->d_rho, s);
+  if (e != cudaSuccess) return SQN_ERR_CUDA;
+  p->launches += 5;
+  return SQN_OK;
+}
+
 template <typename R> int run_frame(sqn_plan *p, const double *dpos, int slot) {
   const FrameGeom &g = p->fg;
   cudaStream_t s = p->stream;
@@ -1281,6 +1313,52 @@ int sqn_finalize(sqn_plan *p, int32_t faber_ziman, double *S_total, double *S_pa
         }
   }
   if (nframes) *nframes = p->nframes;
+  return SQN_OK;
+}
+
+int sqn_density_modes(sqn_plan *p, const double *pos, int32_t where, const int32_t *hkl,
+                      int64_t nmodes, double *rho) {
+  if (!p) return SQN_ERR_PLAN_NOTVALID;
+  if (!pos || !hkl || !rho || nmodes < 1 || (where != SQN_HOST && where != SQN_DEVICE))
+    return SQN_ERR_INVALID_ARGUMENT;
+  // unit-strength transform per species, on the cuFFT spectrum
+  if (p->fused || p->ntr != p->nspecies || !(p->desc.partials || p->bg.xray))
+    return SQN_ERR_NOT_SUPPORTED;
+  DeviceGuard guard(p->device);
+  cudaStream_t s = p->stream;
+  if (cudaStreamSynchronize(s) != cudaSuccess || cudaStreamSynchronize(p->copy_stream) != cudaSuccess)
+    return SQN_ERR_CUDA;
+  if (nmodes > p->modes_cap) {
+    if (p->d_hkl) cudaFree(p->d_hkl);
+    if (p->d_rho) cudaFree(p->d_rho);
+    p->d_hkl = nullptr;
+    p->d_rho = nullptr;
+    p->modes_cap = 0;
+    if (cudaMalloc(&p->d_hkl, sizeof(int) * 3 * (size_t)nmodes) != cudaSuccess ||
+        cudaMalloc(&p->d_rho, sizeof(double) * 2 * (size_t)p->ntr * nmodes) != cudaSuccess) {
+      cudaGetLastError();
+      return SQN_ERR_ALLOC;
+    }
+    p->modes_cap = nmodes;
+  }
+  const int64_t N = p->desc.natoms;
+  const double *dpos = pos;
+  if (where == SQN_HOST) {
+    if (cudaMemcpyAsync(p->d_pos[0], pos, sizeof(double) * 3 * (size_t)N, cudaMemcpyHostToDevice,
+                        s) != cudaSuccess)
+      return SQN_ERR_CUDA;
+    dpos = p->d_pos[0];
+  }
+  if (cudaMemcpyAsync(p->d_hkl, hkl, sizeof(int) * 3 * (size_t)nmodes, cudaMemcpyHostToDevice,
+                      s) != cudaSuccess)
+    return SQN_ERR_CUDA;
+  const int st = p->fp64 ? density_frame<double>(p, dpos, nmodes)
+                         : density_frame<float>(p, dpos, nmodes);
+  if (st != SQN_OK) return st;
+  if (cudaMemcpyAsync(rho, p->d_rho, sizeof(double) * 2 * (size_t)p->ntr * nmodes,
+                      cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return SQN_ERR_CUDA;
   return SQN_OK;
 }
 

@@ -167,6 +167,12 @@ bool choose_fine_grid(const int *modes, double eps, double sigma_req, int w_req,
 std::vector<double> kernel_ft(int64_t nf, int w, double beta, int kmax);
 }  // namespace hostmath
 
+// Density amplitudes of requested lattice points from the half spectra.
+template <typename R>
+cudaError_t launch_gather_modes(const void *G, const BinGeom &b, const int *hkl, int64_t nm,
+                                const R *inv1, const R *inv2, const R *inv3,
+                                const double *origin, double *rho, cudaStream_t s);
+
 // Spread with a weight per point instead of per species (one grid; the
 // weights are in bin-sorted record order).
 template <typename R>

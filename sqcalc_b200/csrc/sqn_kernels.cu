@@ -505,7 +505,75 @@ __global__ void __launch_bounds__(256)
     if (s_n[2 * b.nq + i] != 0.0) atomicAdd(&xcnt[i], s_n[2 * b.nq + i]);
 }
 
+// Density amplitudes rho_t(h) = sum_{j in t} exp(i q_h . r_j) of requested
+// lattice points h (hkl[3m..3m+2], |h_d| <= hm_d) from the half spectra of the
+// per-species transforms: the forward FFT gives phihat(h) sum exp(-2 pi i h.s),
+// so rho = exp(i q.origin) conj(G(h)) / phihat(h), with G(-h) = conj G(h) for
+// h1 < 0.  Output rho[(t nm + m) 2 + {0, 1}] in FP64; modes outside the cube
+// give 0.
+template <typename R>
+__global__ void k_gather_modes(const typename Cplx<R>::T *__restrict__ G, BinGeom b,
+                               const int *__restrict__ hkl, int64_t nm,
+                               const R *__restrict__ inv1, const R *__restrict__ inv2,
+                               const R *__restrict__ inv3, double o0, double o1, double o2,
+                               double *__restrict__ rho) {
+  for (int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; m < nm;
+       m += (int64_t)gridDim.x * blockDim.x) {
+    const int h1 = hkl[3 * m], h2 = hkl[3 * m + 1], h3 = hkl[3 * m + 2];
+    const bool in = abs(h1) <= b.hm[0] && abs(h2) <= b.hm[1] && abs(h3) <= b.hm[2];
+    int q1 = h1, q2 = h2, q3 = h3;
+    const bool cj = h1 < 0;
+    if (cj) {
+      q1 = -q1;
+      q2 = -q2;
+      q3 = -q3;
+    }
+    const int64_t idx = ((int64_t)(q3 >= 0 ? q3 : b.nf[2] + q3) * b.nf[1] +
+                         (q2 >= 0 ? q2 : b.nf[1] + q2)) * b.c1 + q1;
+    double ph = 0.0;
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      const double q = (double)h1 * b.recip[r] + (double)h2 * b.recip[3 + r] +
+                       (double)h3 * b.recip[6 + r];
+      ph += q * (r == 0 ? o0 : (r == 1 ? o1 : o2));
+    }
+    double sn, cs;
+    sincos(ph, &sn, &cs);
+    const double dec = in ? (double)(inv1[abs(h1)] * inv2[abs(h2)] * inv3[abs(h3)]) : 0.0;
+    for (int t = 0; t < b.ntr; ++t) {
+      double vx = 0.0, vy = 0.0;
+      if (in) {
+        const typename Cplx<R>::T gv = G[(int64_t)t * b.vol_cplx + idx];
+        vx = (double)gv.x * dec;                   // conj(G(h)) / phihat, G(h) from
+        vy = (cj ? (double)gv.y : -(double)gv.y) * dec;  // the stored half
+      }
+      rho[2 * (t * nm + m)] = vx * cs - vy * sn;
+      rho[2 * (t * nm + m) + 1] = vx * sn + vy * cs;
+    }
+  }
+}
+
 }  // namespace
+
+static int grid_for(int64_t n, int threads);
+
+template <typename R>
+cudaError_t launch_gather_modes(const void *G, const BinGeom &b, const int *hkl, int64_t nm,
+                                const R *inv1, const R *inv2, const R *inv3,
+                                const double *origin, double *rho, cudaStream_t s) {
+  k_gather_modes<R><<<grid_for(nm, 256), 256, 0, s>>>(
+      (const typename Cplx<R>::T *)G, b, hkl, nm, inv1, inv2, inv3, origin[0], origin[1],
+      origin[2], rho);
+  return cudaGetLastError();
+}
+template cudaError_t launch_gather_modes<float>(const void *, const BinGeom &, const int *,
+                                                int64_t, const float *, const float *,
+                                                const float *, const double *, double *,
+                                                cudaStream_t);
+template cudaError_t launch_gather_modes<double>(const void *, const BinGeom &, const int *,
+                                                 int64_t, const double *, const double *,
+                                                 const double *, const double *, double *,
+                                                 cudaStream_t);
 
 // ---------------------------------------------------------------------------
 // Launch wrappers
