@@ -264,6 +264,7 @@ def precision_leg(types, dev, base, fbytes, W, K, stream, dist, world, local_ran
     ev0.record(stream)
     for f in range(W, W + k):
         p.accumulate((base + f * fbytes, 1), where=_lib.DEVICE)
+    p.join()
     ev1.record(stream)
     torch.cuda.synchronize()
     t = _max_over_ranks(ev0.elapsed_time(ev1) * 1e-3, dist, local_rank)
@@ -497,6 +498,7 @@ def run_ours(args, rank, world, local_rank):
         ev0.record(stream)
         for f in range(W, W + K):
             plan.accumulate((base + f * fbytes, 1), where=_lib.DEVICE)
+        plan.join()  # the last frame's FFT and binning run on the plan's FFT stream
         ev1.record(stream)
         torch.cuda.synchronize()
         clk.mark(tm0, time.monotonic())
@@ -542,6 +544,7 @@ def run_ours(args, rank, world, local_rank):
                                      _lib.HOST)
         _lib.check(rc, "sqn_accumulate_frames")
         e2e_plan.peek_num_async(pnum.data_ptr())
+    e2e_plan.join()
     ev1.record(stream)
     torch.cuda.synchronize()
     e2e_t = ev0.elapsed_time(ev1) * 1e-3

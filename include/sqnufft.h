@@ -71,7 +71,12 @@ enum {
   SQN_FLAG_FUSED_FFT = 4, /* frame path on the pruned FFT passes fused with the binning
                              (2,3,5-smooth axes <= 4096) instead of cuFFT R2C + the bin
                              kernel (the default, faster on B200 at the benchmark sizes) */
-  SQN_FLAG_CUFFT = 8       /* cuFFT R2C + the bin kernel (the default) */
+  SQN_FLAG_CUFFT = 8,      /* cuFFT R2C + the bin kernel (the default) */
+  SQN_FLAG_SERIAL = 16     /* every stage of a frame on the plan's stream.  Without it
+                              (cuFFT path, no SQN_FLAG_TIMING or SQN_FLAG_GRAD) the plan
+                              keeps a second fine grid and runs the FFT and binning of
+                              frame f on an internal stream while frame f + 1 is sorted
+                              and spread on the plan's stream */
 };
 
 /* Everything sqcalc's configure + gpu_setup know after the first frame
@@ -129,7 +134,8 @@ typedef struct sqn_plan_info {
   int64_t device_bytes;     /* device memory the plan holds */
   int64_t tile[3];          /* spread tile in fine-grid cells */
   int32_t fused_fft;        /* 1: pruned FFT passes fused with the binning; 0: cuFFT + bin kernel */
-  int32_t reserved;
+  int32_t pipelined;        /* 1: two fine grids, FFT + binning of frame f beside the
+                               spread of frame f + 1 (see SQN_FLAG_SERIAL) */
   int64_t natoms;           /* atoms per frame */
   int32_t xrd_bins;         /* two-theta bins of the powder pattern (0: off) */
   int32_t reserved2;
@@ -161,11 +167,17 @@ int sqn_plan_info_get(const sqn_plan *plan, sqn_plan_info *info);
  * Replaces one gpu_accumulate per frame (src/sqc_gpu.f90:213-362: host wrap,
  * uploads, cufinufft_setpts / execute, download, host pair sums and binning).
  * The call returns once the positions have been read; the transforms run
- * asynchronously on the plan's stream (device positions must stay valid until
+ * asynchronously on the plan's stream and its internal FFT stream (device
+ * positions are read in the plan's stream order and must stay valid until
  * sqn_sync). */
 int sqn_accumulate_frames(sqn_plan *plan, const double *pos, int64_t nframes, int32_t where);
 
-/* Wait for all queued work of the plan. */
+/* Make the plan's stream wait for the plan's internal FFT stream, without
+ * blocking the host: work queued on the plan's stream after this call (an event,
+ * a collective on the accumulators) comes after every queued frame. */
+int sqn_join(sqn_plan *plan);
+
+/* Wait for all queued work of the plan (both of its streams). */
 int sqn_sync(sqn_plan *plan);
 
 /* Copy the accumulators out (syncs first).  Any pointer may be NULL.
@@ -178,7 +190,8 @@ int sqn_get_accumulators(sqn_plan *plan, double *num, double *den, int64_t *shel
                          double *partial_num, double *gnum, double *gden, int64_t *nframes);
 
 /* Queue a device-to-host copy of num[nq] into host memory (pinned for an
- * asynchronous copy) on the plan's stream, without waiting. */
+ * asynchronous copy) after the queued frames, without waiting; it is complete
+ * after sqn_sync. */
 int sqn_peek_num_async(sqn_plan *plan, double *num_host);
 
 /* Normalised results (syncs first); NULL pointers are skipped.

@@ -25,6 +25,7 @@ FLAG_TIMING = 1
 FLAG_GRAD = 2
 FLAG_FUSED_FFT = 4
 FLAG_CUFFT = 8
+FLAG_SERIAL = 16
 
 # Every symbol include/sqnufft.h declares.
 EXPORTS = (
@@ -37,7 +38,7 @@ EXPORTS = (
     "sqn_type1_makeplan", "sqn_type1f_makeplan", "sqn_type1_setpts", "sqn_type1f_setpts",
     "sqn_type1_execute", "sqn_type1f_execute", "sqn_type1_destroy", "sqn_dump_open",
     "sqn_dump_next", "sqn_dump_last_error", "sqn_dump_rewind", "sqn_dump_close",
-    "sqn_accumulate_dump", "sqn_get_xrd", "sqn_density_modes",
+    "sqn_accumulate_dump", "sqn_get_xrd", "sqn_density_modes", "sqn_join",
 )
 ERR_DUMP = 50
 ERR_SCRATCH_LIMIT = 49
@@ -96,7 +97,7 @@ class SqnInfo(ctypes.Structure):
         ("device_bytes", ctypes.c_int64),
         ("tile", ctypes.c_int64 * 3),
         ("fused_fft", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("pipelined", ctypes.c_int32),
         ("natoms", ctypes.c_int64),
         ("xrd_bins", ctypes.c_int32),
         ("reserved2", ctypes.c_int32),
@@ -182,6 +183,7 @@ def load():
     L.sqn_accumulate_dump.argtypes = [vp, vp, i64, vp, ctypes.POINTER(i64)]
     L.sqn_get_xrd.argtypes = [vp, vp, vp, vp, vp, vp]
     L.sqn_density_modes.argtypes = [vp, vp, ctypes.c_int32, vp, i64, vp]
+    L.sqn_join.argtypes = [vp]
     L.sqn_spread_frame_noalloc.argtypes = [vp, i64, vp, ctypes.c_int32, vp, vp, vp, vp,
                                            ctypes.c_int32, ctypes.c_double, vp, vp]
     if L.sqn_abi_version() != ABI_VERSION:
@@ -215,13 +217,13 @@ class Plan:
                  xray_coef=None, qmin=0.0, qmax=20.0, nq=500, norm=NORM_MEAN, partials=True,
                  want_grid=False, precision=PREC_DOUBLE, eps=1e-9, upsampfac=0.0,
                  kernel_width=0, device=0, max_grid_modes=0, timing=False, stream=None,
-                 grad=False, fused_fft=None, xrd=None):
+                 grad=False, fused_fft=None, xrd=None, serial=False):
         L = load()
         self._L = L
         d = self._describe(cell, origin, type_id, ntypes, weight, amp_const, xray_coef, qmin,
                            qmax, nq, norm, partials, want_grid, precision, eps, upsampfac,
                            kernel_width, device, max_grid_modes, timing, stream, grad, fused_fft,
-                           xrd)
+                           xrd, serial)
         h = ctypes.c_void_p()
         self.status = check(L.sqn_plan_create(ctypes.byref(d), ctypes.byref(h)), "sqn_plan_create")
         self._attach(h, owned=True)
@@ -230,9 +232,10 @@ class Plan:
                   xray_coef=None, qmin=0.0, qmax=20.0, nq=500, norm=NORM_MEAN, partials=True,
                   want_grid=False, precision=PREC_DOUBLE, eps=1e-9, upsampfac=0.0,
                   kernel_width=0, device=0, max_grid_modes=0, timing=False, stream=None,
-                  grad=False, fused_fft=None, xrd=None):
+                  grad=False, fused_fft=None, xrd=None, serial=False):
         """Fill an SqnDesc; the arrays it points to are kept on self.  xrd: None, or a
-        dict(lam=..., range=(min, max), step=0.0, lp=True) for the powder pattern."""
+        dict(lam=..., range=(min, max), step=0.0, lp=True) for the powder pattern.
+        serial: every stage of a frame on the plan's stream (no second grid)."""
         L = self._L
         self.type_id = np.ascontiguousarray(type_id, dtype=np.int32)
         self.natoms = int(self.type_id.size)
@@ -264,7 +267,8 @@ class Plan:
         d.want_grid = int(bool(want_grid))
         d.precision = int(precision)
         d.flags = ((FLAG_TIMING if timing else 0) | (FLAG_GRAD if grad else 0)
-                   | (0 if fused_fft is None else (FLAG_FUSED_FFT if fused_fft else FLAG_CUFFT)))
+                   | (0 if fused_fft is None else (FLAG_FUSED_FFT if fused_fft else FLAG_CUFFT))
+                   | (FLAG_SERIAL if serial else 0))
         d.eps = float(eps)
         d.upsampfac = float(upsampfac)
         d.kernel_width = int(kernel_width)
@@ -409,6 +413,11 @@ class Plan:
 
     def peek_num_async(self, host_buf_ptr):
         check(self._L.sqn_peek_num_async(self._h, ctypes.c_void_p(host_buf_ptr)), "sqn_peek")
+
+    def join(self):
+        """The plan's stream waits for its FFT stream (events recorded on the plan's
+        stream afterwards cover every queued frame)."""
+        check(self._L.sqn_join(self._h), "sqn_join")
 
     def reset(self):
         check(self._L.sqn_reset(self._h), "sqn_reset")

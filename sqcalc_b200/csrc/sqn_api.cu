@@ -285,6 +285,16 @@ struct sqn_plan_s {
   int64_t nsums = 0;           // shell + powder-pattern sums at the head of d_acc
   double *d_xcnt = nullptr;    // kept modes per two-theta bin
 
+  // Frame pipeline: frame f's FFT and binning run on fft_stream while frame
+  // f + 1 is sorted and spread on the plan's stream into the other fine grid.
+  bool overlap = false;
+  cudaStream_t fft_stream = nullptr;
+  void *d_grid2 = nullptr;
+  int gbuf = 0;
+  cudaEvent_t ev_spread[2] = {nullptr, nullptr}, ev_fftdone[2] = {nullptr, nullptr};
+  cudaEvent_t ev_join = nullptr;
+  bool aux_pending = false;  // work queued on fft_stream since the last join
+
   int64_t nframes = 0;
   int slot_next = 0;
   cudaEvent_t ev_copied[2] = {nullptr, nullptr}, ev_free[2] = {nullptr, nullptr};
@@ -323,6 +333,7 @@ void free_plan(sqn_plan *p) {
   cudaSetDevice(p->device);
   if (p->stream) cudaStreamSynchronize(p->stream);
   if (p->copy_stream) cudaStreamSynchronize(p->copy_stream);
+  if (p->fft_stream) cudaStreamSynchronize(p->fft_stream);
   if (p->fft_ok) cufftDestroy(p->fft);
   if (p->fft_fwd1_ok) cufftDestroy(p->fft_fwd1);
   if (p->fft_inv3_ok) cufftDestroy(p->fft_inv3);
@@ -333,7 +344,13 @@ void free_plan(sqn_plan *p) {
     if (p->ev_copied[i]) cudaEventDestroy(p->ev_copied[i]);
     if (p->ev_free[i]) cudaEventDestroy(p->ev_free[i]);
   }
+  for (int i = 0; i < 2; ++i) {
+    if (p->ev_spread[i]) cudaEventDestroy(p->ev_spread[i]);
+    if (p->ev_fftdone[i]) cudaEventDestroy(p->ev_fftdone[i]);
+  }
+  if (p->ev_join) cudaEventDestroy(p->ev_join);
   for (cudaEvent_t e : p->tev_pool) cudaEventDestroy(e);
+  if (p->fft_stream) cudaStreamDestroy(p->fft_stream);
   if (p->copy_stream) cudaStreamDestroy(p->copy_stream);
   if (p->own_stream && p->stream) cudaStreamDestroy(p->stream);
   cudaSetDevice(cur);
@@ -765,6 +782,32 @@ int setup_plan(sqn_plan *p, const sqn_plan_desc *d) {
       return SQN_ERR_CUFFT;
     p->grad_ok = true;
   }
+
+  // --- frame pipeline: a second fine grid and the FFT stream -----------------
+  // Only when the second grid fits; otherwise the plan runs serially.
+  if (!p->fused && !p->inplace && !p->timing && !(d->flags & SQN_FLAG_SERIAL)) {
+    void *v = nullptr;
+    const size_t gbytes = (size_t)p->ntr * g.vol_real * rsz;
+    if (cudaMalloc(&v, gbytes) == cudaSuccess) {
+      p->allocs.push_back(v);
+      p->device_bytes += (int64_t)gbytes;
+      p->d_grid2 = v;
+      // the FFT stream at the higher priority: its blocks are dispatched as the
+      // spread's retire, and the spread fills the rest of the machine
+      int lo_pri = 0, hi_pri = 0;
+      cudaDeviceGetStreamPriorityRange(&lo_pri, &hi_pri);
+      if (cudaStreamCreateWithPriority(&p->fft_stream, cudaStreamNonBlocking, hi_pri) != cudaSuccess ||
+          cudaEventCreateWithFlags(&p->ev_join, cudaEventDisableTiming) != cudaSuccess)
+        return SQN_ERR_CUDA;
+      for (int i = 0; i < 2; ++i)
+        if (cudaEventCreateWithFlags(&p->ev_spread[i], cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&p->ev_fftdone[i], cudaEventDisableTiming) != cudaSuccess)
+          return SQN_ERR_CUDA;
+      p->overlap = true;
+    } else {
+      cudaGetLastError();
+    }
+  }
   if (cudaStreamSynchronize(s) != cudaSuccess) return SQN_ERR_CUDA;
   return warn;
 }
@@ -898,6 +941,32 @@ int setup_fused_fft(sqn_plan *p) {
 }
 
 // One frame through the weighted forward transform and, with gsh, its adjoint.
+// Order the work queued on the FFT stream before what comes next on the
+// plan's stream.
+int join_fft_stream(sqn_plan *p) {
+  if (!p->aux_pending) return SQN_OK;
+  if (cudaEventRecord(p->ev_join, p->fft_stream) != cudaSuccess ||
+      cudaStreamWaitEvent(p->stream, p->ev_join, 0) != cudaSuccess)
+    return SQN_ERR_CUDA;
+  p->aux_pending = false;
+  return SQN_OK;
+}
+
+// All queued work of the plan finished (both streams).
+int sync_plan(sqn_plan *p) {
+  const int st = join_fft_stream(p);
+  if (st != SQN_OK) return st;
+  return cudaStreamSynchronize(p->stream) == cudaSuccess ? SQN_OK : SQN_ERR_CUDA;
+}
+
+// The frame plan's forward transform of `in` into `out` on stream s.
+cufftResult exec_forward(sqn_plan *p, cudaStream_t s, void *in, void *out) {
+  cufftResult fr = cufftSetStream(p->fft, s);
+  if (fr != CUFFT_SUCCESS) return fr;
+  return p->fp64 ? cufftExecD2Z(p->fft, (cufftDoubleReal *)in, (cufftDoubleComplex *)out)
+                 : cufftExecR2C(p->fft, (cufftReal *)in, (cufftComplex *)out);
+}
+
 template <typename R> int grad_frame(sqn_plan *p, const double *dpos, bool want_grad) {
   cudaStream_t s = p->stream;
   FrameGeom g = p->fg;
@@ -958,10 +1027,7 @@ template <typename R> int density_frame(sqn_plan *p, const double *dpos, int64_t
     e = launch_spread<R>((const R *)p->d_recs, p->d_starts, g, (const R *)p->d_strength,
                          (R *)p->d_grid, s);
   if (e != cudaSuccess) return SQN_ERR_CUDA;
-  cufftResult fr = p->fp64 ? cufftExecD2Z(p->fft, (cufftDoubleReal *)p->d_grid,
-                                          (cufftDoubleComplex *)p->d_G)
-                           : cufftExecR2C(p->fft, (cufftReal *)p->d_grid, (cufftComplex *)p->d_G);
-  if (fr != CUFFT_SUCCESS) return SQN_ERR_CUFFT;
+  if (exec_forward(p, s, p->d_grid, p->d_G) != CUFFT_SUCCESS) return SQN_ERR_CUFFT;
   e = launch_gather_modes<R>(p->d_G, p->bg, p->d_hkl, nm, (const R *)p->d_inv[0],
                              (const R *)p->d_inv[1], (const R *)p->d_inv[2], p->origin,
                              p->d_rho, s);
@@ -992,8 +1058,16 @@ template <typename R> int run_frame(sqn_plan *p, const double *dpos, int slot) {
   if (e != cudaSuccess) return SQN_ERR_CUDA;
   if (slot >= 0) cudaEventRecord(p->ev_free[slot], s);
   if (p->timing) cudaEventRecord(ev[1], s);
+  // With the pipeline, frames alternate between the two grids; a grid is
+  // spread again once the FFT of the frame before last has read it.
+  const int gb = p->overlap ? p->gbuf : 0;
+  void *grid = gb ? p->d_grid2 : p->d_grid;
+  if (p->overlap) {
+    p->gbuf ^= 1;
+    if (cudaStreamWaitEvent(s, p->ev_fftdone[gb], 0) != cudaSuccess) return SQN_ERR_CUDA;
+  }
   e = launch_spread<R>((const R *)p->d_recs, p->d_starts, g, (const R *)p->d_strength,
-                       (R *)p->d_grid, s);
+                       (R *)grid, s);
   if (e != cudaSuccess) return SQN_ERR_CUDA;
   if (p->timing) cudaEventRecord(ev[2], s);
   if (p->fused) {
@@ -1008,16 +1082,22 @@ template <typename R> int run_frame(sqn_plan *p, const double *dpos, int slot) {
     if (p->timing) cudaEventRecord(ev[4], s);
     p->launches += 7;
   } else {
-    cufftResult fr;
-    if (p->fp64)
-      fr = cufftExecD2Z(p->fft, (cufftDoubleReal *)p->d_grid, (cufftDoubleComplex *)p->d_G);
-    else
-      fr = cufftExecR2C(p->fft, (cufftReal *)p->d_grid, (cufftComplex *)p->d_G);
-    if (fr != CUFFT_SUCCESS) return SQN_ERR_CUFFT;
+    cudaStream_t fs = s;
+    if (p->overlap) {
+      fs = p->fft_stream;
+      if (cudaEventRecord(p->ev_spread[gb], s) != cudaSuccess ||
+          cudaStreamWaitEvent(fs, p->ev_spread[gb], 0) != cudaSuccess)
+        return SQN_ERR_CUDA;
+    }
+    if (exec_forward(p, fs, grid, p->d_G) != CUFFT_SUCCESS) return SQN_ERR_CUFFT;
+    if (p->overlap) {
+      if (cudaEventRecord(p->ev_fftdone[gb], fs) != cudaSuccess) return SQN_ERR_CUDA;
+      p->aux_pending = true;
+    }
     if (p->timing) cudaEventRecord(ev[3], s);
     e = launch_bin<R>(p->d_rows, p->nrows, p->d_G, p->bg, (const R *)p->d_inv[0],
                       (const R *)p->d_inv[1], (const R *)p->d_inv[2], p->d_amp, p->d_xcoef,
-                      p->d_acc, p->d_gnum, p->nsm, s);
+                      p->d_acc, p->d_gnum, p->nsm, fs);
     if (e != cudaSuccess) return SQN_ERR_CUDA;
     if (p->timing) cudaEventRecord(ev[4], s);
     p->launches += 5;
@@ -1142,6 +1222,7 @@ int sqn_plan_info_get(const sqn_plan *p, sqn_plan_info *info) {
   info->nspecies = p->nspecies;
   info->device_bytes = p->device_bytes;
   info->fused_fft = p->fused ? 1 : 0;
+  info->pipelined = p->overlap ? 1 : 0;
   info->natoms = p->desc.natoms;
   info->xrd_bins = p->bg.xrd ? p->bg.xbins : 0;
   info->xrd_step = p->bg.xrd ? p->bg.xstep : 0.0;
@@ -1184,25 +1265,33 @@ int sqn_accumulate_frames(sqn_plan *p, const double *pos, int64_t nframes, int32
   return SQN_OK;
 }
 
+int sqn_join(sqn_plan *p) {
+  if (!p) return SQN_ERR_PLAN_NOTVALID;
+  DeviceGuard guard(p->device);
+  return join_fft_stream(p);
+}
+
 int sqn_sync(sqn_plan *p) {
   if (!p) return SQN_ERR_PLAN_NOTVALID;
   DeviceGuard guard(p->device);
-  return cuda_status(cudaStreamSynchronize(p->stream));
+  return sync_plan(p);
 }
 
 int sqn_peek_num_async(sqn_plan *p, double *num_host) {
   if (!p) return SQN_ERR_PLAN_NOTVALID;
   if (!num_host) return SQN_ERR_INVALID_ARGUMENT;
   DeviceGuard guard(p->device);
+  // after the binning of the queued frames, on the stream that runs it
+  cudaStream_t s = p->aux_pending ? p->fft_stream : p->stream;
   return cuda_status(cudaMemcpyAsync(num_host, p->d_acc, sizeof(double) * p->desc.nq,
-                                     cudaMemcpyDeviceToHost, p->stream));
+                                     cudaMemcpyDeviceToHost, s));
 }
 
 int sqn_get_accumulators(sqn_plan *p, double *num, double *den, int64_t *shell_count,
                          double *partial_num, double *gnum, double *gden, int64_t *nframes) {
   if (!p) return SQN_ERR_PLAN_NOTVALID;
   DeviceGuard guard(p->device);
-  if (cudaStreamSynchronize(p->stream) != cudaSuccess) return SQN_ERR_CUDA;
+  if (sync_plan(p) != SQN_OK) return SQN_ERR_CUDA;
   const int nq = p->desc.nq, T = p->desc.ntypes;
   std::vector<double> acc((size_t)p->nquant * nq);
   if (cudaMemcpy(acc.data(), p->d_acc, acc.size() * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
@@ -1326,7 +1415,7 @@ int sqn_density_modes(sqn_plan *p, const double *pos, int32_t where, const int32
     return SQN_ERR_NOT_SUPPORTED;
   DeviceGuard guard(p->device);
   cudaStream_t s = p->stream;
-  if (cudaStreamSynchronize(s) != cudaSuccess || cudaStreamSynchronize(p->copy_stream) != cudaSuccess)
+  if (sync_plan(p) != SQN_OK || cudaStreamSynchronize(p->copy_stream) != cudaSuccess)
     return SQN_ERR_CUDA;
   if (nmodes > p->modes_cap) {
     if (p->d_hkl) cudaFree(p->d_hkl);
@@ -1368,7 +1457,7 @@ int sqn_get_xrd(sqn_plan *p, double *two_theta, double *I, double *I_partial, in
   const BinGeom &b = p->bg;
   if (!b.xrd) return SQN_ERR_NOT_SUPPORTED;
   DeviceGuard guard(p->device);
-  if (cudaStreamSynchronize(p->stream) != cudaSuccess) return SQN_ERR_CUDA;
+  if (sync_plan(p) != SQN_OK) return SQN_ERR_CUDA;
   const int nb = b.xbins, T = p->desc.ntypes;
   std::vector<double> xs((size_t)b.xquant * nb), xc((size_t)nb);
   if (cudaMemcpy(xs.data(), p->d_acc + (size_t)b.nquant * b.nq, xs.size() * sizeof(double),
@@ -1404,7 +1493,7 @@ int sqn_accumulator_view(sqn_plan *p, double **acc, int64_t *count, int64_t *nfr
   if (!p) return SQN_ERR_PLAN_NOTVALID;
   if (!acc || !count) return SQN_ERR_INVALID_ARGUMENT;
   DeviceGuard guard(p->device);
-  if (cudaStreamSynchronize(p->stream) != cudaSuccess) return SQN_ERR_CUDA;
+  if (sync_plan(p) != SQN_OK) return SQN_ERR_CUDA;
   *acc = p->d_acc;
   *count = p->nsums + p->gnum_half;
   if (nframes) *nframes = p->nframes;
@@ -1421,7 +1510,7 @@ int sqn_set_frame_count(sqn_plan *p, int64_t nframes) {
 int sqn_reset(sqn_plan *p) {
   if (!p) return SQN_ERR_PLAN_NOTVALID;
   DeviceGuard guard(p->device);
-  if (cudaStreamSynchronize(p->stream) != cudaSuccess) return SQN_ERR_CUDA;
+  if (sync_plan(p) != SQN_OK) return SQN_ERR_CUDA;
   cudaError_t e = cudaMemset(p->d_acc, 0, sizeof(double) * ((size_t)p->nsums + (size_t)p->gnum_half));
   p->nframes = 0;
   p->tev_used = 0;
@@ -1435,7 +1524,7 @@ int sqn_stage_times(sqn_plan *p, double *out, int32_t n) {
   if (!out || n < 1) return SQN_ERR_INVALID_ARGUMENT;
   if (!p->timing) return SQN_ERR_NOT_SUPPORTED;
   DeviceGuard guard(p->device);
-  if (cudaStreamSynchronize(p->stream) != cudaSuccess) return SQN_ERR_CUDA;
+  if (sync_plan(p) != SQN_OK) return SQN_ERR_CUDA;
   harvest_timing(p);
   double v[5] = {p->stage_ms[0], p->stage_ms[1], p->stage_ms[2], p->stage_ms[3], (double)p->stage_frames};
   for (int i = 0; i < n && i < 5; ++i) out[i] = v[i];
@@ -1453,6 +1542,7 @@ int sqn_sq_grad(sqn_plan *p, const double *pos, int32_t where, const double *dLd
   const int64_t N = p->desc.natoms;
   const int nq = p->desc.nq;
   const double *dpos = pos;
+  if (join_fft_stream(p) != SQN_OK) return SQN_ERR_CUDA;
   if (where == SQN_HOST) {
     // the copy stream may still be filling this slot for an earlier call
     if (cudaStreamSynchronize(p->copy_stream) != cudaSuccess ||
@@ -1597,6 +1687,7 @@ int sqn_batch_create(const sqn_plan_desc *descs, int32_t nsystems, void *stream,
     sqn_plan_desc d = descs[k];
     d.stream = nullptr;
     d.flags &= ~(uint32_t)SQN_FLAG_TIMING;
+    d.flags |= SQN_FLAG_SERIAL;  // one stream per system inside the graph
     sqn_plan *p = nullptr;
     const int ps = sqn_plan_create(&d, &p);
     if (ps > SQN_WARN_EPS_TOO_SMALL) {
