@@ -71,7 +71,8 @@ enum {
   SQN_FLAG_FUSED_FFT = 4, /* frame path on the pruned FFT passes fused with the binning
                              (2,3,5-smooth axes <= 4096) instead of cuFFT R2C + the bin
                              kernel (the default, faster on B200 at the benchmark sizes) */
-  SQN_FLAG_CUFFT = 8,      /* cuFFT R2C + the bin kernel (the default) */
+  SQN_FLAG_CUFFT = 8,      /* cuFFT R2C + the bin kernel (instead of the pruned 512-point
+                              passes that 512^3 grids use by default) */
   SQN_FLAG_SERIAL = 16     /* every stage of a frame on the plan's stream.  Without it
                               (cuFFT path, no SQN_FLAG_TIMING or SQN_FLAG_GRAD) the plan
                               keeps a second fine grid and runs the FFT and binning of
@@ -138,7 +139,8 @@ typedef struct sqn_plan_info {
                                spread of frame f + 1 (see SQN_FLAG_SERIAL) */
   int64_t natoms;           /* atoms per frame */
   int32_t xrd_bins;         /* two-theta bins of the powder pattern (0: off) */
-  int32_t reserved2;
+  int32_t pruned_fft512;    /* 1: the frame FFT runs as pruned 512-point passes of ours
+                               (every axis 512, no SQN_FLAG_CUFFT) instead of cuFFT */
   double xrd_step;          /* their width, degrees */
 } sqn_plan_info;
 

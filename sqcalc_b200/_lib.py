@@ -100,7 +100,7 @@ class SqnInfo(ctypes.Structure):
         ("pipelined", ctypes.c_int32),
         ("natoms", ctypes.c_int64),
         ("xrd_bins", ctypes.c_int32),
-        ("reserved2", ctypes.c_int32),
+        ("pruned_fft512", ctypes.c_int32),
         ("xrd_step", ctypes.c_double),
     ]
 

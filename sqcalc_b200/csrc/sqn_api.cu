@@ -269,6 +269,10 @@ struct sqn_plan_s {
     return (flags & SQN_FLAG_FUSED_FFT) && !(flags & SQN_FLAG_CUFFT);
   }
   int64_t c1pitch = 0;  // complex row pitch of the half spectrum
+  // pruned 512-point passes (every axis 512): compact half spectrum in d_G
+  bool fft512 = false;
+  void *d_tw512 = nullptr;
+  BinGeom bg512{};
   // density amplitudes (sqn_density_modes): request buffers, grown on demand
   int *d_hkl = nullptr;
   double *d_rho = nullptr;
@@ -739,6 +743,38 @@ int setup_plan(sqn_plan *p, const sqn_plan_desc *d) {
     if (st2 != SQN_OK) return st2;
   }
 
+  // --- pruned 512-point passes -------------------------------------------------
+  // cuFFT stays for plans that ask for it, dS/dr plans (in-place spectra),
+  // the fused path and other grid sizes.
+  if (!p->fused && !p->inplace && !(d->flags & SQN_FLAG_CUFFT) && p->nf[0] == 512 &&
+      p->nf[1] == 512 && p->nf[2] == 512) {
+    std::vector<double> tw(2 * 512);
+    for (int m = 0; m < 512; ++m) {
+      const double a = -2.0 * M_PI * (double)m / 512.0;
+      tw[2 * m] = std::cos(a);
+      tw[2 * m + 1] = std::sin(a);
+    }
+    char *v;
+    if ((st = dalloc(p, &v, tw.size() * rsz))) return st;
+    p->d_tw512 = v;
+    cudaError_t ce;
+    if (p->fp64) {
+      ce = cudaMemcpy(v, tw.data(), tw.size() * 8, cudaMemcpyHostToDevice);
+      if (ce == cudaSuccess) ce = fft512_set_attributes<double>();
+    } else {
+      std::vector<float> f = to_r<float>(tw);
+      ce = cudaMemcpy(v, f.data(), f.size() * 4, cudaMemcpyHostToDevice);
+      if (ce == cudaSuccess) ce = fft512_set_attributes<float>();
+    }
+    if (ce != cudaSuccess) return SQN_ERR_CUDA;
+    p->bg512 = b;
+    p->bg512.nf[1] = 2 * p->hm[1] + 1;
+    p->bg512.nf[2] = 2 * p->hm[2] + 1;
+    p->bg512.c1 = p->hm[0] + 1;
+    p->bg512.vol_cplx = p->bg512.c1 * p->bg512.nf[1] * p->bg512.nf[2];
+    p->fft512 = true;
+  }
+
   // --- adjoint buffers (dS/dr) -----------------------------------------------
   if (d->flags & SQN_FLAG_GRAD) {
     if (xray) return SQN_ERR_NOT_SUPPORTED;
@@ -941,6 +977,9 @@ int setup_fused_fft(sqn_plan *p) {
 }
 
 // One frame through the weighted forward transform and, with gsh, its adjoint.
+// Kernels of ours that one frame launches.
+int frame_launches(const sqn_plan *p) { return p->fused ? 7 : (p->fft512 ? 8 : 5); }
+
 // Order the work queued on the FFT stream before what comes next on the
 // plan's stream.
 int join_fft_stream(sqn_plan *p) {
@@ -1089,15 +1128,23 @@ template <typename R> int run_frame(sqn_plan *p, const double *dpos, int slot) {
           cudaStreamWaitEvent(fs, p->ev_spread[gb], 0) != cudaSuccess)
         return SQN_ERR_CUDA;
     }
-    if (exec_forward(p, fs, grid, p->d_G) != CUFFT_SUCCESS) return SQN_ERR_CUFFT;
+    if (p->fft512) {
+      // x pass into d_G, y pass back into the (consumed) grid, z pass into d_G
+      e = launch_fft512<R>((const R *)grid, p->d_G, grid, p->d_G, p->ntr, g.pitch,
+                           p->hm[0] + 1, p->hm[1], p->hm[2], p->d_tw512, p->nsm, fs);
+      if (e != cudaSuccess) return SQN_ERR_CUDA;
+      p->launches += 3;
+    } else if (exec_forward(p, fs, grid, p->d_G) != CUFFT_SUCCESS) {
+      return SQN_ERR_CUFFT;
+    }
     if (p->overlap) {
       if (cudaEventRecord(p->ev_fftdone[gb], fs) != cudaSuccess) return SQN_ERR_CUDA;
       p->aux_pending = true;
     }
     if (p->timing) cudaEventRecord(ev[3], s);
-    e = launch_bin<R>(p->d_rows, p->nrows, p->d_G, p->bg, (const R *)p->d_inv[0],
-                      (const R *)p->d_inv[1], (const R *)p->d_inv[2], p->d_amp, p->d_xcoef,
-                      p->d_acc, p->d_gnum, p->nsm, fs);
+    e = launch_bin<R>(p->d_rows, p->nrows, p->d_G, p->fft512 ? p->bg512 : p->bg,
+                      (const R *)p->d_inv[0], (const R *)p->d_inv[1], (const R *)p->d_inv[2],
+                      p->d_amp, p->d_xcoef, p->d_acc, p->d_gnum, p->nsm, fs);
     if (e != cudaSuccess) return SQN_ERR_CUDA;
     if (p->timing) cudaEventRecord(ev[4], s);
     p->launches += 5;
@@ -1223,6 +1270,7 @@ int sqn_plan_info_get(const sqn_plan *p, sqn_plan_info *info) {
   info->device_bytes = p->device_bytes;
   info->fused_fft = p->fused ? 1 : 0;
   info->pipelined = p->overlap ? 1 : 0;
+  info->pruned_fft512 = p->fft512 ? 1 : 0;
   info->natoms = p->desc.natoms;
   info->xrd_bins = p->bg.xrd ? p->bg.xbins : 0;
   info->xrd_step = p->bg.xrd ? p->bg.xstep : 0.0;
@@ -1633,7 +1681,7 @@ int capture_batch(sqn_batch *b) {
     st = p->fp64 ? run_frame<double>(p, p->d_pos[0], -1) : run_frame<float>(p, p->d_pos[0], -1);
     // the capture itself accumulates nothing
     p->nframes -= 1;
-    p->launches -= p->fused ? 7 : 5;
+    p->launches -= frame_launches(p);
     if (st == SQN_OK && (cudaEventRecord(b->joins[k], p->stream) != cudaSuccess ||
                          cudaStreamWaitEvent(root, b->joins[k], 0) != cudaSuccess))
       st = SQN_ERR_CUDA;
@@ -1737,7 +1785,7 @@ int sqn_batch_accumulate(sqn_batch *b, const double *const *pos, int64_t nframes
     b->replays++;
     for (sqn_plan *p : b->plans) {
       p->nframes++;
-      p->launches += p->fused ? 7 : 5;
+      p->launches += frame_launches(p);
     }
   }
   return SQN_OK;

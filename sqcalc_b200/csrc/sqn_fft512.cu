@@ -1,0 +1,334 @@
+// Pruned three-pass FFT for 512-point axes, one warp per 512-point line with
+// the line held in registers (replaces cuFFT R2C on the frame path when every
+// fine-grid axis is 512).
+//
+// A line of 512 complex values is split n = n1 + 32 n2 (n1 = lane): each lane
+// runs a 16-point DFT over n2 in registers, multiplies by exp(-2 pi i n1 k2 /
+// 512), the warp transposes through a 512-slot scratch line in shared memory
+// (skewed so that neither the writes nor the reads collide on banks), each
+// lane runs a second 16-point DFT, and a radix-2 step across lanes L and
+// L ^ 16 (shuffles) finishes the 32-point DFT.  Lane L = k2 + 16 b then holds
+// X[k2 + 16 a + 256 b], a = 0 .. 15.  Forward sign exp(-2 pi i j k / n), as
+// cuFFT's forward transform; twiddles from an FP64 host table.
+//
+// Passes (only the modes |h_d| <= hm_d of the type-1 NUFFT are kept):
+//   k_fft512_x     two real rows along x form one complex line; the half
+//                  spectrum h1 = 0 .. H1-1 of each row is written (A1[t][z][y][h1])
+//   k_fft512_cols  lines along a strided axis for 16 consecutive h1 of one
+//                  plane, staged in shared memory (coalesced 128-byte rows in
+//                  and out); only the band h = -hm .. hm is written, in FFT
+//                  order (h >= 0 at h, h < 0 at 2 hm + 1 + h).  The y pass
+//                  (A1 -> A2[t][z][h2][h1]) and the z pass
+//                  (A2 -> G[t][h3][h2][h1]) are the same kernel with other strides.
+// The result is the compact half spectrum that k_bin reads with nf1 = 2 hm1 + 1,
+// nf2 = 2 hm2 + 1 and a row length of H1.
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "sqn_device.cuh"
+#include "sqn_internal.h"
+
+namespace sqn {
+namespace {
+
+using namespace dev;
+
+template <typename C> __device__ __forceinline__ C c_add(C a, C b) {
+  a.x += b.x;
+  a.y += b.y;
+  return a;
+}
+template <typename C> __device__ __forceinline__ C c_sub(C a, C b) {
+  a.x -= b.x;
+  a.y -= b.y;
+  return a;
+}
+template <typename C> __device__ __forceinline__ C c_mul(C a, C w) {
+  C r;
+  r.x = a.x * w.x - a.y * w.y;
+  r.y = a.x * w.y + a.y * w.x;
+  return r;
+}
+// a * exp(-i theta) for cos theta = c, sin theta = s
+template <typename C, typename R> __device__ __forceinline__ C c_rot(C a, R c, R s) {
+  C r;
+  r.x = a.x * c + a.y * s;
+  r.y = a.y * c - a.x * s;
+  return r;
+}
+
+// 4-point forward DFT in place.
+template <typename C> __device__ __forceinline__ void dft4(C &v0, C &v1, C &v2, C &v3) {
+  const C a0 = c_add(v0, v2), a1 = c_sub(v0, v2);
+  const C a2 = c_add(v1, v3);
+  C a3 = c_sub(v1, v3);  // times -i
+  const auto t = a3.x;
+  a3.x = a3.y;
+  a3.y = -t;
+  v0 = c_add(a0, a2);
+  v2 = c_sub(a0, a2);
+  v1 = c_add(a1, a3);
+  v3 = c_sub(a1, a3);
+}
+
+// 16-point forward DFT in registers, natural order in and out:
+// n = n1 + 4 n2, k = k2 + 4 k1, twiddle exp(-2 pi i n1 k2 / 16).
+template <typename C> __device__ __forceinline__ void dft16(C (&v)[16]) {
+  using R = decltype(v[0].x);
+  const R c1 = (R)0.92387953251128675613, s1 = (R)0.38268343236508977173;  // cos, sin pi/8
+  const R r2 = (R)0.70710678118654752440;                                  // cos pi/4
+#pragma unroll
+  for (int n1 = 0; n1 < 4; ++n1) dft4(v[n1], v[n1 + 4], v[n1 + 8], v[n1 + 12]);
+  // v[n1 + 4 k2] now holds A[n1][k2]; multiply by exp(-i pi n1 k2 / 8)
+  v[5] = c_rot(v[5], c1, s1);    // n1 1 k2 1: m 1
+  v[9] = c_rot(v[9], r2, r2);    // n1 1 k2 2: m 2
+  v[13] = c_rot(v[13], s1, c1);  // n1 1 k2 3: m 3
+  v[6] = c_rot(v[6], r2, r2);    // n1 2 k2 1: m 2
+  {                              // n1 2 k2 2: m 4, exp(-i pi / 2) = -i
+    const R t = v[10].x;
+    v[10].x = v[10].y;
+    v[10].y = -t;
+  }
+  v[14] = c_rot(v[14], -r2, r2);   // n1 2 k2 3: m 6
+  v[7] = c_rot(v[7], s1, c1);      // n1 3 k2 1: m 3
+  v[11] = c_rot(v[11], -r2, r2);   // n1 3 k2 2: m 6
+  v[15] = c_rot(v[15], -c1, -s1);  // n1 3 k2 3: m 9
+#pragma unroll
+  for (int k2 = 0; k2 < 4; ++k2) dft4(v[4 * k2], v[4 * k2 + 1], v[4 * k2 + 2], v[4 * k2 + 3]);
+  // v[4 k2 + k1] holds X[k2 + 4 k1]; reorder to natural order
+  C o[16];
+#pragma unroll
+  for (int k2 = 0; k2 < 4; ++k2)
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) o[k2 + 4 * k1] = v[4 * k2 + k1];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) v[k] = o[k];
+}
+
+template <typename C> __device__ __forceinline__ C shfl_xor16(C v) {
+  C r;
+  r.x = __shfl_xor_sync(FULL, v.x, 16);
+  r.y = __shfl_xor_sync(FULL, v.y, 16);
+  return r;
+}
+
+// Skewed slot of element (k2, n1) of the transpose (512 slots): the writes
+// (fixed k2, lanes over n1) and the reads (fixed m2, lanes over k2 and m1 with
+// n1 = m1 + 2 m2) both touch every 8-byte bank pair exactly twice.
+__device__ __forceinline__ int tslot(int k2, int n1) { return k2 * 32 + ((n1 + k2) & 31); }
+
+// Forward 512-point DFT of the line whose element lane + 32 j is v[j].  The
+// scratch line has 512 slots; slot i lives at scr[i * sstride].  On return
+// lane L = k2 + 16 b holds X[k2 + 16 a + 256 b] in v[a].  tw[m] = exp(-2 pi i m
+// / 512).  The caller synchronises the warp before reusing the scratch line.
+template <typename C>
+__device__ __forceinline__ void warp_fft512(C (&v)[16], C *scr, int sstride, const C *tw,
+                                            int lane) {
+  dft16(v);  // v[k2] = Y[n1 = lane][k2]
+#pragma unroll
+  for (int k2 = 1; k2 < 16; ++k2) v[k2] = c_mul(v[k2], tw[lane * k2]);
+#pragma unroll
+  for (int k2 = 0; k2 < 16; ++k2) scr[tslot(k2, lane) * sstride] = v[k2];
+  __syncwarp();
+  const int k2 = lane & 15, m1 = lane >> 4;
+#pragma unroll
+  for (int m2 = 0; m2 < 16; ++m2) v[m2] = scr[tslot(k2, m1 + 2 * m2) * sstride];
+  __syncwarp();
+  dft16(v);  // v[a] = sum_m2 Y[m1 + 2 m2][k2] exp(-2 pi i m2 a / 16)
+  if (m1) {
+#pragma unroll
+    for (int a = 1; a < 16; ++a) v[a] = c_mul(v[a], tw[16 * a]);  // exp(-2 pi i a / 32)
+  }
+#pragma unroll
+  for (int a = 0; a < 16; ++a) {
+    const C o = shfl_xor16(v[a]);
+    v[a] = m1 ? c_sub(o, v[a]) : c_add(v[a], o);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Pass 1: rows along x.  Warps take row pairs (2 pr, 2 pr + 1); rows are
+// pitch reals apart, nrows in all.
+// ---------------------------------------------------------------------------
+template <typename R> __host__ __device__ constexpr int x_warps() {
+  return sizeof(R) == 4 ? 8 : 4;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(32 * x_warps<R>())
+    k_fft512_x(const R *__restrict__ grid, typename Cplx<R>::T *__restrict__ A1, int64_t nrows,
+               int64_t pitch, int H1, const typename Cplx<R>::T *__restrict__ tw) {
+  using C = typename Cplx<R>::T;
+  constexpr int X_WARPS = x_warps<R>();
+  __shared__ C s_tw[512];
+  __shared__ C s_line[X_WARPS][512];
+  for (int i = threadIdx.x; i < 512; i += blockDim.x) s_tw[i] = tw[i];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  C *line = s_line[warp];
+  const int64_t npairs = (nrows + 1) >> 1;
+  for (int64_t pr = (int64_t)blockIdx.x * X_WARPS + warp; pr < npairs;
+       pr += (int64_t)gridDim.x * X_WARPS) {
+    const R *r0 = grid + (2 * pr) * pitch;
+    const bool two = 2 * pr + 1 < nrows;
+    C v[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      v[j].x = r0[lane + 32 * j];
+      v[j].y = two ? r0[pitch + lane + 32 * j] : R(0);
+    }
+    warp_fft512(v, line, 1, s_tw, lane);
+    // natural order into the scratch line for the split of the two rows
+    const int k2 = lane & 15, b = lane >> 4;
+#pragma unroll
+    for (int a = 0; a < 16; ++a) line[k2 + 16 * a + 256 * b] = v[a];
+    __syncwarp();
+    // X1[h] = (Z[h] + conj Z[512-h]) / 2, X2[h] = (Z[h] - conj Z[512-h]) / (2i)
+    C *o0 = A1 + (2 * pr) * H1;
+    for (int h = lane; h < H1; h += 32) {
+      const C zh = line[h];
+      const C zm = line[(512 - h) & 511];
+      C x1, x2;
+      x1.x = R(0.5) * (zh.x + zm.x);
+      x1.y = R(0.5) * (zh.y - zm.y);
+      x2.x = R(0.5) * (zh.y + zm.y);
+      x2.y = R(0.5) * (zm.x - zh.x);
+      o0[h] = x1;
+      if (two) o0[H1 + h] = x2;
+    }
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Column passes: 512-point lines along a strided axis, 16 consecutive columns
+// (h1) of one plane per CTA step, 16 warps (one column each).
+// Plane o = t * planes_per_t + p starts at t * tstride + p * pstride; row r of
+// the plane is rstride elements further.
+// ---------------------------------------------------------------------------
+constexpr int COLS = 16;
+constexpr int COL_LD = COLS + 1;  // staged row pitch (complex)
+
+struct ColPass {
+  int64_t in_t, in_p, in_r;     // input strides (complex elements)
+  int64_t out_t, out_p, out_r;  // output strides
+  int planes_per_t;
+  int64_t nplanes;
+  int ncols;  // columns per plane (H1)
+  int hm;     // kept band -hm .. hm
+};
+
+template <typename R>
+__global__ void __launch_bounds__(32 * COLS, sizeof(R) == 4 ? 2 : 1)
+    k_fft512_cols(const typename Cplx<R>::T *__restrict__ in, typename Cplx<R>::T *__restrict__ out,
+                  ColPass cp, const typename Cplx<R>::T *__restrict__ tw) {
+  using C = typename Cplx<R>::T;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C *s_tw = reinterpret_cast<C *>(smem_raw);
+  C *tile = s_tw + 512;  // [512][COL_LD]
+  for (int i = threadIdx.x; i < 512; i += blockDim.x) s_tw[i] = tw[i];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nblk = (cp.ncols + COLS - 1) / COLS;
+  const int M = 2 * cp.hm + 1;
+  const int64_t nsteps = cp.nplanes * nblk;
+  for (int64_t st = blockIdx.x; st < nsteps; st += gridDim.x) {
+    const int64_t plane = st / nblk;
+    const int c0 = (int)(st - plane * nblk) * COLS;
+    const int nc = min(COLS, cp.ncols - c0);
+    const int64_t t = plane / cp.planes_per_t, p = plane - t * cp.planes_per_t;
+    const C *ib = in + t * cp.in_t + p * cp.in_p + c0;
+    C *ob = out + t * cp.out_t + p * cp.out_p + c0;
+    __syncthreads();  // the previous step's stores have read the tile
+    for (int e = threadIdx.x; e < 512 * COLS; e += blockDim.x) {
+      const int r = e >> 4, c = e & (COLS - 1);
+      C v;
+      v.x = v.y = R(0);
+      if (c < nc) v = ib[(int64_t)r * cp.in_r + c];
+      tile[r * COL_LD + c] = v;
+    }
+    __syncthreads();
+    if (warp < nc) {
+      C *col = tile + warp;
+      C v[16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) v[j] = col[(lane + 32 * j) * COL_LD];
+      __syncwarp();
+      // the column itself is the scratch line (slot i at row i)
+      warp_fft512(v, col, COL_LD, s_tw, lane);
+      const int k2 = lane & 15, b = lane >> 4;
+#pragma unroll
+      for (int a = 0; a < 16; ++a) col[(k2 + 16 * a + 256 * b) * COL_LD] = v[a];
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < M * COLS; e += blockDim.x) {
+      const int hw = e >> 4, c = e & (COLS - 1);
+      if (c < nc) {
+        const int h = hw <= cp.hm ? hw : hw - M;
+        ob[(int64_t)hw * cp.out_r + c] = tile[(h & 511) * COL_LD + c];
+      }
+    }
+  }
+}
+
+template <typename R> size_t cols_smem() {
+  return sizeof(typename Cplx<R>::T) * (512 + 512 * COL_LD);
+}
+
+}  // namespace
+
+template <typename R> cudaError_t fft512_set_attributes() {
+  return cudaFuncSetAttribute(k_fft512_cols<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)cols_smem<R>());
+}
+template cudaError_t fft512_set_attributes<float>();
+template cudaError_t fft512_set_attributes<double>();
+
+// grid [ntr][nf2][nf1][pitch] real -> A1 [ntr][nf2][nf1][H1] -> A2 [ntr][nf2][M2][H1]
+// -> G [ntr][M3][M2][H1] (A2 may share the grid's storage; A1 and G share one buffer).
+template <typename R>
+cudaError_t launch_fft512(const R *grid, void *A1, void *A2, void *G, int ntr, int64_t pitch,
+                          int H1, int hm1, int hm2, const void *tw, int nsm, cudaStream_t s) {
+  using C = typename Cplx<R>::T;
+  const int n = 512;
+  const int M2 = 2 * hm1 + 1, M3 = 2 * hm2 + 1;
+  const int64_t nrows = (int64_t)ntr * n * n;
+  k_fft512_x<R><<<nsm * 8, 32 * x_warps<R>(), 0, s>>>(grid, (C *)A1, nrows, pitch, H1,
+                                                      (const C *)tw);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  const size_t sm = cols_smem<R>();
+  const int cta = sizeof(R) == 4 ? 2 : 1;
+  ColPass y;
+  y.in_t = (int64_t)n * n * H1;
+  y.in_p = (int64_t)n * H1;
+  y.in_r = H1;
+  y.out_t = (int64_t)n * M2 * H1;
+  y.out_p = (int64_t)M2 * H1;
+  y.out_r = H1;
+  y.planes_per_t = n;
+  y.nplanes = (int64_t)ntr * n;
+  y.ncols = H1;
+  y.hm = hm1;
+  k_fft512_cols<R><<<nsm * cta, 32 * COLS, sm, s>>>((const C *)A1, (C *)A2, y, (const C *)tw);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  ColPass z;
+  z.in_t = (int64_t)n * M2 * H1;
+  z.in_p = H1;
+  z.in_r = (int64_t)M2 * H1;
+  z.out_t = (int64_t)M3 * M2 * H1;
+  z.out_p = H1;
+  z.out_r = (int64_t)M2 * H1;
+  z.planes_per_t = M2;
+  z.nplanes = (int64_t)ntr * M2;
+  z.ncols = H1;
+  z.hm = hm2;
+  k_fft512_cols<R><<<nsm * cta, 32 * COLS, sm, s>>>((const C *)A2, (C *)G, z, (const C *)tw);
+  return cudaGetLastError();
+}
+template cudaError_t launch_fft512<float>(const float *, void *, void *, void *, int, int64_t,
+                                          int, int, int, const void *, int, cudaStream_t);
+template cudaError_t launch_fft512<double>(const double *, void *, void *, void *, int, int64_t,
+                                           int, int, int, const void *, int, cudaStream_t);
+
+}  // namespace sqn
