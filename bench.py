@@ -611,8 +611,9 @@ def run_ours(args, rank, world, local_rank):
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": fbytes,
                     "d2h_bytes_per_step": NQ * 8},
             "gpu_launches": launches,
-            "gpu_launches_note": "own kernels (prep, scan, scatter, spread, bin) per frame; "
-                                 "cuFFT kernels not counted",
+            "gpu_launches_note": "own kernels per frame: prep, scan, scatter, spread, the "
+                                 "three pruned 512-point FFT passes (512^3 grids; cuFFT "
+                                 "kernels, not counted, otherwise) and bin",
             "fp64": fp64,
             "grad": grad,
             "batched": batched,

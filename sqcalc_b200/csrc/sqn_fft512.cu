@@ -238,13 +238,20 @@ __global__ void __launch_bounds__(32 * COLS, sizeof(R) == 4 ? 2 : 1)
     const int64_t t = plane / cp.planes_per_t, p = plane - t * cp.planes_per_t;
     const C *ib = in + t * cp.in_t + p * cp.in_p + c0;
     C *ob = out + t * cp.out_t + p * cp.out_p + c0;
+    // a thread's loads (column c, rows r0 + 32 k) go out eight at a time
+    const int c = threadIdx.x & (COLS - 1), r0 = threadIdx.x >> 4;
+    const C *src = ib + (int64_t)r0 * cp.in_r + c;
+    const int64_t step = 32 * cp.in_r;
     __syncthreads();  // the previous step's stores have read the tile
-    for (int e = threadIdx.x; e < 512 * COLS; e += blockDim.x) {
-      const int r = e >> 4, c = e & (COLS - 1);
-      C v;
-      v.x = v.y = R(0);
-      if (c < nc) v = ib[(int64_t)r * cp.in_r + c];
-      tile[r * COL_LD + c] = v;
+    if (c < nc) {
+#pragma unroll
+      for (int k0 = 0; k0 < 512 / 32; k0 += 8) {
+        C ld[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) ld[k] = src[(k0 + k) * step];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) tile[(r0 + 32 * (k0 + k)) * COL_LD + c] = ld[k];
+      }
     }
     __syncthreads();
     if (warp < nc) {
