@@ -73,11 +73,12 @@ enum {
                              kernel (the default, faster on B200 at the benchmark sizes) */
   SQN_FLAG_CUFFT = 8,      /* cuFFT R2C + the bin kernel (instead of the pruned 512-point
                               passes that 512^3 grids use by default) */
-  SQN_FLAG_SERIAL = 16     /* every stage of a frame on the plan's stream.  Without it
-                              (cuFFT path, no SQN_FLAG_TIMING or SQN_FLAG_GRAD) the plan
-                              keeps a second fine grid and runs the FFT and binning of
+  SQN_FLAG_PIPELINE = 16   /* keep a second fine grid and run the FFT and binning of
                               frame f on an internal stream while frame f + 1 is sorted
-                              and spread on the plan's stream */
+                              and spread on the plan's stream (not with SQN_FLAG_TIMING,
+                              SQN_FLAG_GRAD or the fused path).  Off by default: on B200
+                              the two halves time-share the SMs, and with the pruned
+                              512-point passes the pipelined plan is slower */
 };
 
 /* Everything sqcalc's configure + gpu_setup know after the first frame
@@ -136,7 +137,7 @@ typedef struct sqn_plan_info {
   int64_t tile[3];          /* spread tile in fine-grid cells */
   int32_t fused_fft;        /* 1: pruned FFT passes fused with the binning; 0: cuFFT + bin kernel */
   int32_t pipelined;        /* 1: two fine grids, FFT + binning of frame f beside the
-                               spread of frame f + 1 (see SQN_FLAG_SERIAL) */
+                               spread of frame f + 1 (see SQN_FLAG_PIPELINE) */
   int64_t natoms;           /* atoms per frame */
   int32_t xrd_bins;         /* two-theta bins of the powder pattern (0: off) */
   int32_t pruned_fft512;    /* 1: the frame FFT runs as pruned 512-point passes of ours

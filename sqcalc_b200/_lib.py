@@ -25,7 +25,7 @@ FLAG_TIMING = 1
 FLAG_GRAD = 2
 FLAG_FUSED_FFT = 4
 FLAG_CUFFT = 8
-FLAG_SERIAL = 16
+FLAG_PIPELINE = 16
 
 # Every symbol include/sqnufft.h declares.
 EXPORTS = (
@@ -217,13 +217,13 @@ class Plan:
                  xray_coef=None, qmin=0.0, qmax=20.0, nq=500, norm=NORM_MEAN, partials=True,
                  want_grid=False, precision=PREC_DOUBLE, eps=1e-9, upsampfac=0.0,
                  kernel_width=0, device=0, max_grid_modes=0, timing=False, stream=None,
-                 grad=False, fused_fft=None, xrd=None, serial=False):
+                 grad=False, fused_fft=None, xrd=None, pipeline=False):
         L = load()
         self._L = L
         d = self._describe(cell, origin, type_id, ntypes, weight, amp_const, xray_coef, qmin,
                            qmax, nq, norm, partials, want_grid, precision, eps, upsampfac,
                            kernel_width, device, max_grid_modes, timing, stream, grad, fused_fft,
-                           xrd, serial)
+                           xrd, pipeline)
         h = ctypes.c_void_p()
         self.status = check(L.sqn_plan_create(ctypes.byref(d), ctypes.byref(h)), "sqn_plan_create")
         self._attach(h, owned=True)
@@ -232,10 +232,11 @@ class Plan:
                   xray_coef=None, qmin=0.0, qmax=20.0, nq=500, norm=NORM_MEAN, partials=True,
                   want_grid=False, precision=PREC_DOUBLE, eps=1e-9, upsampfac=0.0,
                   kernel_width=0, device=0, max_grid_modes=0, timing=False, stream=None,
-                  grad=False, fused_fft=None, xrd=None, serial=False):
+                  grad=False, fused_fft=None, xrd=None, pipeline=False):
         """Fill an SqnDesc; the arrays it points to are kept on self.  xrd: None, or a
         dict(lam=..., range=(min, max), step=0.0, lp=True) for the powder pattern.
-        serial: every stage of a frame on the plan's stream (no second grid)."""
+        pipeline: FFT and binning of frame f on a second stream beside the spread of
+        frame f + 1 (a second fine grid)."""
         L = self._L
         self.type_id = np.ascontiguousarray(type_id, dtype=np.int32)
         self.natoms = int(self.type_id.size)
@@ -268,7 +269,7 @@ class Plan:
         d.precision = int(precision)
         d.flags = ((FLAG_TIMING if timing else 0) | (FLAG_GRAD if grad else 0)
                    | (0 if fused_fft is None else (FLAG_FUSED_FFT if fused_fft else FLAG_CUFFT))
-                   | (FLAG_SERIAL if serial else 0))
+                   | (FLAG_PIPELINE if pipeline else 0))
         d.eps = float(eps)
         d.upsampfac = float(upsampfac)
         d.kernel_width = int(kernel_width)

@@ -821,7 +821,7 @@ int setup_plan(sqn_plan *p, const sqn_plan_desc *d) {
 
   // --- frame pipeline: a second fine grid and the FFT stream -----------------
   // Only when the second grid fits; otherwise the plan runs serially.
-  if (!p->fused && !p->inplace && !p->timing && !(d->flags & SQN_FLAG_SERIAL)) {
+  if (!p->fused && !p->inplace && !p->timing && (d->flags & SQN_FLAG_PIPELINE)) {
     void *v = nullptr;
     const size_t gbytes = (size_t)p->ntr * g.vol_real * rsz;
     if (cudaMalloc(&v, gbytes) == cudaSuccess) {
@@ -1735,7 +1735,7 @@ int sqn_batch_create(const sqn_plan_desc *descs, int32_t nsystems, void *stream,
     sqn_plan_desc d = descs[k];
     d.stream = nullptr;
     d.flags &= ~(uint32_t)SQN_FLAG_TIMING;
-    d.flags |= SQN_FLAG_SERIAL;  // one stream per system inside the graph
+    d.flags &= ~(uint32_t)SQN_FLAG_PIPELINE;  // one stream per system inside the graph
     sqn_plan *p = nullptr;
     const int ps = sqn_plan_create(&d, &p);
     if (ps > SQN_WARN_EPS_TOO_SMALL) {

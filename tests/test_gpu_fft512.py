@@ -33,8 +33,8 @@ def plan(tid, precision, eps, cufft, **kw):
 ])
 def test_pruned_passes_match_cufft(precision, eps, tol, serial, grid):
     tid, fr = frames()
-    with plan(tid, precision, eps, False, serial=serial, want_grid=grid) as pp, \
-            plan(tid, precision, eps, True, serial=serial, want_grid=grid) as pc:
+    with plan(tid, precision, eps, False, pipeline=not serial, want_grid=grid) as pp, \
+            plan(tid, precision, eps, True, pipeline=not serial, want_grid=grid) as pc:
         assert list(pp.info.nf) == [512, 512, 512]
         assert pp.info.pruned_fft512 == 1 and pc.info.pruned_fft512 == 0
         for p in (pp, pc):

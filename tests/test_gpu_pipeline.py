@@ -1,6 +1,6 @@
 """Frame pipeline: the FFT and binning of frame f on the plan's FFT stream
 beside the sort and spread of frame f + 1 (two fine grids) give the sums of a
-serial plan (SQN_FLAG_SERIAL), for host and device frames, through peek, reset,
+serial plan (without SQN_FLAG_PIPELINE), for host and device frames, through peek, reset,
 the accumulator view and the single-frame entry points that share the plan."""
 import numpy as np
 import pytest
@@ -14,7 +14,7 @@ def make(frames, tid, cell, precision, serial, **kw):
     return _lib.Plan(cell.reshape(9), np.zeros(3), tid, ntypes=2, weight=_lib.WEIGHT_NEUTRON,
                      amp_const=np.array([0.6, 1.4]), qmin=0.5, qmax=6.0, nq=60, partials=True,
                      precision=precision, eps=1e-6 if precision == _lib.PREC_SINGLE else 1e-10,
-                     serial=serial, **kw)
+                     pipeline=not serial, **kw)
 
 
 def system(n=20000, nframes=7, seed=4):
@@ -77,4 +77,7 @@ def test_timing_and_grad_plans_stay_serial():
     with make(frames, tid, cell, _lib.PREC_SINGLE, False, timing=True) as p:
         assert p.info.pipelined == 0
     with make(frames, tid, cell, _lib.PREC_SINGLE, False, grad=True) as p:
+        assert p.info.pipelined == 0
+    # serial unless asked for
+    with _lib.Plan(cell.reshape(9), np.zeros(3), tid, ntypes=2, qmax=3.0, nq=20) as p:
         assert p.info.pipelined == 0
