@@ -59,9 +59,15 @@ __device__ __forceinline__ uint32_t home_key(const AtomCell &c, const FrameGeom 
 
 // ES kernel: phi(t) = exp(beta (sqrt(1 - (2t/w)^2) - 1)) on |t| < w/2, else 0
 // (external/finufft/include/cufinufft/spreadinterp.h:84-98).
+// FP32: the hardware approximations of sqrt and 2^x (relative errors near
+// 2^-22 on the kernel values, below the FP32 plans' smallest eps, FLT_EPSILON;
+// the error of a value far out in the tail is relative to that small value).
 __device__ __forceinline__ float es_phi(float t, float c2, float beta) {
   const float z2 = c2 * t * t;
-  return z2 < 1.0f ? expf(beta * (sqrtf(1.0f - z2) - 1.0f)) : 0.0f;
+  if (!(z2 < 1.0f)) return 0.0f;
+  float r;
+  asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(1.0f - z2));
+  return __expf(beta * (r - 1.0f));
 }
 __device__ __forceinline__ double es_phi(double t, double c2, double beta) {
   const double z2 = c2 * t * t;
