@@ -125,6 +125,23 @@ __device__ __forceinline__ void load_zrow(const double *src, double (&z)[TILE_Z]
   }
 }
 
+// c0 += a z0, c1 += a z1: one packed FP32 FMA (fma.rn.f32x2, sm_100) in FP32,
+// two FMAs in FP64.
+__device__ __forceinline__ void fma2(float a, float z0, float z1, float &c0, float &c1) {
+  asm("{\n\t.reg .b64 pa, pz, pc;\n\t"
+      "mov.b64 pa, {%2, %2};\n\t"
+      "mov.b64 pz, {%3, %4};\n\t"
+      "mov.b64 pc, {%0, %1};\n\t"
+      "fma.rn.f32x2 pc, pa, pz, pc;\n\t"
+      "mov.b64 {%0, %1}, pc;\n\t}"
+      : "+f"(c0), "+f"(c1)
+      : "f"(a), "f"(z0), "f"(z1));
+}
+__device__ __forceinline__ void fma2(double a, double z0, double z1, double &c0, double &c1) {
+  c0 = fma(a, z0, c0);
+  c1 = fma(a, z1, c1);
+}
+
 // Does the cyclic support [r, r+w) (mod n) meet the cells [b, b+len)?
 __device__ __forceinline__ bool cyc_meet(int r, int w, int b, int len, int n) {
   if (len <= 0) return false;
@@ -366,7 +383,7 @@ __global__ void __launch_bounds__(SPREAD_THREADS, (sizeof(R) == 4 || NT == 1) ? 
           R zr[TILE_Z];
           load_zrow(row + TILE_X + TILE_Y, zr);
 #pragma unroll
-          for (int z = 0; z < TILE_Z; ++z) acc[t][z] = fma(a, zr[z], acc[t][z]);
+          for (int z = 0; z < TILE_Z; z += 2) fma2(a, zr[z], zr[z + 1], acc[t][z], acc[t][z + 1]);
         }
       }
     }
