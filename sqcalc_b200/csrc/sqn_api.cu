@@ -748,12 +748,8 @@ int setup_plan(sqn_plan *p, const sqn_plan_desc *d) {
   // the fused path and other grid sizes.
   if (!p->fused && !p->inplace && !(d->flags & SQN_FLAG_CUFFT) && p->nf[0] == 512 &&
       p->nf[1] == 512 && p->nf[2] == 512) {
-    std::vector<double> tw(2 * 512);
-    for (int m = 0; m < 512; ++m) {
-      const double a = -2.0 * M_PI * (double)m / 512.0;
-      tw[2 * m] = std::cos(a);
-      tw[2 * m + 1] = std::sin(a);
-    }
+    std::vector<double> tw;
+    fft512_twiddles(tw);
     char *v;
     if ((st = dalloc(p, &v, tw.size() * rsz))) return st;
     p->d_tw512 = v;

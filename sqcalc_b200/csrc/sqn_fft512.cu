@@ -22,7 +22,10 @@
 //                  (A2 -> G[t][h3][h2][h1]) are the same kernel with other strides.
 // The result is the compact half spectrum that k_bin reads with nf1 = 2 hm1 + 1,
 // nf2 = 2 hm2 + 1 and a row length of H1.
+#include <cmath>
 #include <cstdint>
+#include <vector>
+
 #include <cuda_runtime.h>
 
 #include "sqn_device.cuh"
@@ -117,16 +120,21 @@ template <typename C> __device__ __forceinline__ C shfl_xor16(C v) {
 // n1 = m1 + 2 m2) both touch every 8-byte bank pair exactly twice.
 __device__ __forceinline__ int tslot(int k2, int n1) { return k2 * 32 + ((n1 + k2) & 31); }
 
+// Twiddle table (TW_LEN entries): tw[m] = exp(-2 pi i m / 512) for m < 512,
+// then tw[512 + 32 k2 + n1] = exp(-2 pi i n1 k2 / 512), the per-lane factors
+// laid out so that a warp reads 32 consecutive entries (no bank conflicts).
+constexpr int TW_LEN = 1024;
+
 // Forward 512-point DFT of the line whose element lane + 32 j is v[j].  The
 // scratch line has 512 slots; slot i lives at scr[i * sstride].  On return
-// lane L = k2 + 16 b holds X[k2 + 16 a + 256 b] in v[a].  tw[m] = exp(-2 pi i m
-// / 512).  The caller synchronises the warp before reusing the scratch line.
+// lane L = k2 + 16 b holds X[k2 + 16 a + 256 b] in v[a].  The caller
+// synchronises the warp before reusing the scratch line.
 template <typename C>
 __device__ __forceinline__ void warp_fft512(C (&v)[16], C *scr, int sstride, const C *tw,
                                             int lane) {
   dft16(v);  // v[k2] = Y[n1 = lane][k2]
 #pragma unroll
-  for (int k2 = 1; k2 < 16; ++k2) v[k2] = c_mul(v[k2], tw[lane * k2]);
+  for (int k2 = 1; k2 < 16; ++k2) v[k2] = c_mul(v[k2], tw[512 + 32 * k2 + lane]);
 #pragma unroll
   for (int k2 = 0; k2 < 16; ++k2) scr[tslot(k2, lane) * sstride] = v[k2];
   __syncwarp();
@@ -160,9 +168,9 @@ __global__ void __launch_bounds__(32 * x_warps<R>())
                int64_t pitch, int H1, const typename Cplx<R>::T *__restrict__ tw) {
   using C = typename Cplx<R>::T;
   constexpr int X_WARPS = x_warps<R>();
-  __shared__ C s_tw[512];
+  __shared__ C s_tw[TW_LEN];
   __shared__ C s_line[X_WARPS][512];
-  for (int i = threadIdx.x; i < 512; i += blockDim.x) s_tw[i] = tw[i];
+  for (int i = threadIdx.x; i < TW_LEN; i += blockDim.x) s_tw[i] = tw[i];
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   C *line = s_line[warp];
@@ -225,8 +233,8 @@ __global__ void __launch_bounds__(32 * COLS, sizeof(R) == 4 ? 2 : 1)
   using C = typename Cplx<R>::T;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C *s_tw = reinterpret_cast<C *>(smem_raw);
-  C *tile = s_tw + 512;  // [512][COL_LD]
-  for (int i = threadIdx.x; i < 512; i += blockDim.x) s_tw[i] = tw[i];
+  C *tile = s_tw + TW_LEN;  // [512][COL_LD]
+  for (int i = threadIdx.x; i < TW_LEN; i += blockDim.x) s_tw[i] = tw[i];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nblk = (cp.ncols + COLS - 1) / COLS;
   const int M = 2 * cp.hm + 1;
@@ -278,7 +286,7 @@ __global__ void __launch_bounds__(32 * COLS, sizeof(R) == 4 ? 2 : 1)
 }
 
 template <typename R> size_t cols_smem() {
-  return sizeof(typename Cplx<R>::T) * (512 + 512 * COL_LD);
+  return sizeof(typename Cplx<R>::T) * (TW_LEN + 512 * COL_LD);
 }
 
 }  // namespace
@@ -289,6 +297,17 @@ template <typename R> cudaError_t fft512_set_attributes() {
 }
 template cudaError_t fft512_set_attributes<float>();
 template cudaError_t fft512_set_attributes<double>();
+
+// Twiddle table of the passes (TW_LEN complex values, FP64 on the host).
+void fft512_twiddles(std::vector<double> &tw) {
+  tw.assign(2 * TW_LEN, 0.0);
+  for (int m = 0; m < TW_LEN; ++m) {
+    const int e = m < 512 ? m : ((m - 512) & 31) * ((m - 512) >> 5);  // n1 k2
+    const double a = -2.0 * M_PI * (double)e / 512.0;
+    tw[2 * m] = std::cos(a);
+    tw[2 * m + 1] = std::sin(a);
+  }
+}
 
 // grid [ntr][nf2][nf1][pitch] real -> A1 [ntr][nf2][nf1][H1] -> A2 [ntr][nf2][M2][H1]
 // -> G [ntr][M3][M2][H1] (A2 may share the grid's storage; A1 and G share one buffer).
