@@ -51,41 +51,67 @@ __global__ void k_prep(const double *__restrict__ pos, FrameGeom g, int *__restr
 }
 
 // Exclusive scan of counts[0..n) into starts[0..n], then zero counts for the
-// next frame.  One CTA of 1024 threads, each owning a contiguous run.
+// next frame.  One CTA of 1024 threads walks the array in chunks of 4096
+// (four consecutive counts per thread, vector loads and stores), carrying the
+// running total from chunk to chunk.
 __global__ void __launch_bounds__(1024) k_scan(int *__restrict__ counts, int *__restrict__ starts,
                                                int n) {
   __shared__ int wsum[32];
+  __shared__ int s_carry;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int per = (n + 1023) / 1024;
-  const int lo = min(n, tid * per), hi = min(n, lo + per);
-  int s = 0;
-  for (int i = lo; i < hi; ++i) s += counts[i];
-  int v = s;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    int t = __shfl_up_sync(FULL, v, o);
-    if (lane >= o) v += t;
-  }
-  if (lane == 31) wsum[warp] = v;
+  if (tid == 0) s_carry = 0;
   __syncthreads();
-  if (warp == 0) {
-    int x = wsum[lane];
+  for (int base = 0; base < n; base += 4096) {
+    const int i0 = base + 4 * tid;
+    int c[4] = {0, 0, 0, 0};
+    const bool full = i0 + 3 < n;
+    if (full) {
+      const int4 v = *reinterpret_cast<const int4 *>(counts + i0);
+      c[0] = v.x;
+      c[1] = v.y;
+      c[2] = v.z;
+      c[3] = v.w;
+    } else {
+      for (int k = 0; k < 4; ++k)
+        if (i0 + k < n) c[k] = counts[i0 + k];
+    }
+    const int s = c[0] + c[1] + c[2] + c[3];
+    int v = s;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      int t = __shfl_up_sync(FULL, x, o);
-      if (lane >= o) x += t;
+      const int t = __shfl_up_sync(FULL, v, o);
+      if (lane >= o) v += t;
     }
-    wsum[lane] = x;
+    if (lane == 31) wsum[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+      int x = wsum[lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(FULL, x, o);
+        if (lane >= o) x += t;
+      }
+      wsum[lane] = x;
+    }
+    __syncthreads();
+    const int excl = s_carry + v - s + (warp > 0 ? wsum[warp - 1] : 0);
+    const int o0 = excl, o1 = o0 + c[0], o2 = o1 + c[1], o3 = o2 + c[2];
+    if (full) {
+      *reinterpret_cast<int4 *>(starts + i0) = make_int4(o0, o1, o2, o3);
+      *reinterpret_cast<int4 *>(counts + i0) = make_int4(0, 0, 0, 0);
+    } else {
+      const int o[4] = {o0, o1, o2, o3};
+      for (int k = 0; k < 4; ++k)
+        if (i0 + k < n) {
+          starts[i0 + k] = o[k];
+          counts[i0 + k] = 0;
+        }
+    }
+    __syncthreads();  // every thread has read s_carry and wsum
+    if (tid == 1023) s_carry = excl + s;
+    __syncthreads();
   }
-  __syncthreads();
-  int run = v - s + (warp > 0 ? wsum[warp - 1] : 0);
-  for (int i = lo; i < hi; ++i) {
-    const int c = counts[i];
-    starts[i] = run;
-    run += c;
-    counts[i] = 0;
-  }
-  if (tid == 1023) starts[n] = run;
+  if (tid == 0) starts[n] = s_carry;
 }
 
 template <typename R>
