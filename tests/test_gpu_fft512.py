@@ -49,3 +49,31 @@ def test_pruned_passes_match_cufft(precision, eps, tol, serial, grid):
             assert np.max(np.abs(a[2] - b[2])) / max(1.0, float(np.max(np.abs(b[2])))) < 10 * tol
         # three more kernels per frame than the cuFFT plan
         assert pp.launch_count() - pc.launch_count() == 3 * len(fr)
+
+
+def test_pruned_passes_xray_weights_and_powder_pattern():
+    """q-dependent (x-ray) amplitudes and the two-theta histogram of the powder
+    pattern read from the compact spectrum, against the cuFFT plan."""
+    tid, fr = frames(2)
+    coef = np.array([[2.0, 1.5, 1.0, 0.5, 10.0, 5.0, 1.0, 0.2, 0.3],
+                     [3.0, 2.0, 1.0, 0.4, 12.0, 4.0, 0.8, 0.1, 0.5],
+                     [6.0, 3.0, 2.0, 1.0, 8.0, 3.0, 0.9, 0.3, 1.0]])
+    xrd = dict(lam=1.5406, range=(10.0, 60.0), step=0.5, lp=True)
+
+    def mk(cufft):
+        return _lib.Plan(np.eye(3).reshape(9) * L, np.zeros(3), tid, ntypes=3,
+                         weight=_lib.WEIGHT_XRAY, xray_coef=coef, qmin=0.0, qmax=QMAX, nq=200,
+                         partials=True, precision=_lib.PREC_SINGLE, eps=1e-6,
+                         fused_fft=False if cufft else None, xrd=xrd)
+    with mk(False) as pp, mk(True) as pc:
+        assert pp.info.pruned_fft512 == 1 and pc.info.pruned_fft512 == 0
+        for p in (pp, pc):
+            for f in fr:
+                p.accumulate(f)
+        a, b = pp.finalize(), pc.finalize()
+        for x, y in ((a[0], b[0]), (a[1], b[1])):
+            assert np.max(np.abs(x - y)) / max(1.0, float(np.max(np.abs(y)))) < 2e-6
+        xa, xb = pp.xrd(), pc.xrd()
+        np.testing.assert_array_equal(xa[3], xb[3])
+        for x, y in ((xa[1], xb[1]), (xa[2], xb[2])):
+            assert np.max(np.abs(x - y)) / max(1.0, float(np.max(np.abs(y)))) < 2e-6
