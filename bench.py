@@ -463,7 +463,10 @@ def run_ours(args, rank, world, local_rank):
         import torch.distributed as td
         td.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
     K, W = args.steps, args.warmup
-    types, frames = make_frames(K + W, SEED + 7919 * rank)
+    # distinct frames, cycled through by the steps (each 24 MB, all of them far
+    # larger than L2 together)
+    NFR = min(K + W, 32)
+    types, frames = make_frames(NFR, SEED + 7919 * rank)
     prec = _lib.PREC_SINGLE if args.precision == "single" else _lib.PREC_DOUBLE
     eps = EPS
     # A dedicated (non-default) stream: the plans run on it, so torch CUDA
@@ -484,7 +487,7 @@ def run_ours(args, rank, world, local_rank):
     fbytes = N_ATOMS * 3 * 8
     base = dev.data_ptr()
     for f in range(W):
-        plan.accumulate((base + f * fbytes, 1), where=_lib.DEVICE)
+        plan.accumulate((base + (f % NFR) * fbytes, 1), where=_lib.DEVICE)
     plan.sync()
     if dist:
         td.barrier()
@@ -497,7 +500,7 @@ def run_ours(args, rank, world, local_rank):
         tm0 = time.monotonic()
         ev0.record(stream)
         for f in range(W, W + K):
-            plan.accumulate((base + f * fbytes, 1), where=_lib.DEVICE)
+            plan.accumulate((base + (f % NFR) * fbytes, 1), where=_lib.DEVICE)
         plan.join()  # the last frame's FFT and binning run on the plan's FFT stream
         ev1.record(stream)
         torch.cuda.synchronize()
@@ -515,10 +518,10 @@ def run_ours(args, rank, world, local_rank):
     # --- per-stage device times (CUDA events inside the library) -------------
     tplan = mk(True)
     for f in range(W):
-        tplan.accumulate((base + f * fbytes, 1), where=_lib.DEVICE)
+        tplan.accumulate((base + (f % NFR) * fbytes, 1), where=_lib.DEVICE)
     tplan.reset()
     for f in range(W, W + K):
-        tplan.accumulate((base + f * fbytes, 1), where=_lib.DEVICE)
+        tplan.accumulate((base + (f % NFR) * fbytes, 1), where=_lib.DEVICE)
     st = tplan.stage_times()
     tplan.close()
     nfr = max(st["frames"], 1)
@@ -532,7 +535,7 @@ def run_ours(args, rank, world, local_rank):
     import ctypes
     L = _lib.load()
     for f in range(W):
-        L.sqn_accumulate_frames(e2e_plan.handle, ctypes.c_void_p(hbase + f * fbytes), 1, _lib.HOST)
+        L.sqn_accumulate_frames(e2e_plan.handle, ctypes.c_void_p(hbase + (f % NFR) * fbytes), 1, _lib.HOST)
         e2e_plan.peek_num_async(pnum.data_ptr())
     e2e_plan.sync()
     if dist:
@@ -540,7 +543,7 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize()
     ev0.record(stream)
     for f in range(W, W + K):
-        rc = L.sqn_accumulate_frames(e2e_plan.handle, ctypes.c_void_p(hbase + f * fbytes), 1,
+        rc = L.sqn_accumulate_frames(e2e_plan.handle, ctypes.c_void_p(hbase + (f % NFR) * fbytes), 1,
                                      _lib.HOST)
         _lib.check(rc, "sqn_accumulate_frames")
         e2e_plan.peek_num_async(pnum.data_ptr())
@@ -632,7 +635,7 @@ def run_ours(args, rank, world, local_rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="single", choices=["single", "double"])
