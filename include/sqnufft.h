@@ -73,6 +73,11 @@ enum {
                              kernel (the default, faster on B200 at the benchmark sizes) */
   SQN_FLAG_CUFFT = 8,      /* cuFFT R2C + the bin kernel (instead of the pruned 512-point
                               passes that 512^3 grids use by default) */
+  SQN_FLAG_SPREAD_TC = 32,   /* FP32 plans with 1 to 4 transforms: spread on the tensor
+                                cores (tcgen05, 3xTF32, accumulators in tensor memory)
+                                instead of the CUDA cores.  Off by default: measured
+                                slower on B200 (the per-tile MMAs are small and chained
+                                on one accumulator) */
   SQN_FLAG_PIPELINE = 16   /* keep a second fine grid and run the FFT and binning of
                               frame f on an internal stream while frame f + 1 is sorted
                               and spread on the plan's stream (not with SQN_FLAG_TIMING,

@@ -270,6 +270,9 @@ struct sqn_plan_s {
   }
   int64_t c1pitch = 0;  // complex row pitch of the half spectrum
   // pruned 512-point passes (every axis 512): compact half spectrum in d_G
+  bool spread_tc = false;  // FP32: the tensor-core spread (sqn_spread_tc.cu)
+  int tc_chunk = 0;
+  int *d_err = nullptr;    // set by a kernel whose bounded wait gave up
   bool fft512 = false;
   void *d_tw512 = nullptr;
   BinGeom bg512{};
@@ -743,6 +746,15 @@ int setup_plan(sqn_plan *p, const sqn_plan_desc *d) {
     if (st2 != SQN_OK) return st2;
   }
 
+  // --- tensor-core spread (FP32, opt-in) -------------------------------------------
+  if (!p->fp64 && !p->fused && p->ntr >= 1 && p->ntr <= 4 && (d->flags & SQN_FLAG_SPREAD_TC)) {
+    if ((st = dalloc(p, &p->d_err, 1))) return st;
+    if (cudaMemset(p->d_err, 0, sizeof(int)) != cudaSuccess || spread_tc_set_attributes() != cudaSuccess)
+      return SQN_ERR_CUDA;
+    p->tc_chunk = spread_tc_chunk();
+    p->spread_tc = true;
+  }
+
   // --- pruned 512-point passes -------------------------------------------------
   // cuFFT stays for plans that ask for it, dS/dr plans (in-place spectra),
   // the fused path and other grid sizes.
@@ -987,11 +999,22 @@ int join_fft_stream(sqn_plan *p) {
   return SQN_OK;
 }
 
-// All queued work of the plan finished (both streams).
+// All queued work of the plan finished (both streams); a kernel that gave up
+// a bounded wait since the last check turns into an error here.
 int sync_plan(sqn_plan *p) {
   const int st = join_fft_stream(p);
   if (st != SQN_OK) return st;
-  return cudaStreamSynchronize(p->stream) == cudaSuccess ? SQN_OK : SQN_ERR_CUDA;
+  if (cudaStreamSynchronize(p->stream) != cudaSuccess) return SQN_ERR_CUDA;
+  if (p->d_err) {
+    int h = 0;
+    if (cudaMemcpy(&h, p->d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+      return SQN_ERR_CUDA;
+    if (h != 0) {
+      cudaMemset(p->d_err, 0, sizeof(int));
+      return SQN_ERR_CUDA;
+    }
+  }
+  return SQN_OK;
 }
 
 // The frame plan's forward transform of `in` into `out` on stream s.
@@ -1101,8 +1124,17 @@ template <typename R> int run_frame(sqn_plan *p, const double *dpos, int slot) {
     p->gbuf ^= 1;
     if (cudaStreamWaitEvent(s, p->ev_fftdone[gb], 0) != cudaSuccess) return SQN_ERR_CUDA;
   }
-  e = launch_spread<R>((const R *)p->d_recs, p->d_starts, g, (const R *)p->d_strength,
-                       (R *)grid, s);
+  if constexpr (sizeof(R) == 4) {
+    if (p->spread_tc) {
+      FrameGeom gt = g;
+      gt.chunk = p->tc_chunk;
+      e = launch_spread_tc((const float *)p->d_recs, p->d_starts, gt, (const float *)p->d_strength,
+                           (float *)grid, p->d_err, s);
+    }
+  }
+  if (!p->spread_tc)
+    e = launch_spread<R>((const R *)p->d_recs, p->d_starts, g, (const R *)p->d_strength,
+                         (R *)grid, s);
   if (e != cudaSuccess) return SQN_ERR_CUDA;
   if (p->timing) cudaEventRecord(ev[2], s);
   if (p->fused) {

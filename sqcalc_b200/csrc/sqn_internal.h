@@ -175,6 +175,14 @@ template <typename R>
 cudaError_t launch_fft512(const R *grid, void *A1, void *A2, void *G, int ntr, int64_t pitch,
                           int H1, int hm1, int hm2, const void *tw, int nsm, cudaStream_t s);
 
+// Gather spreading on the tensor cores (sqn_spread_tc.cu, FP32, 1..4
+// transforms); *err is set when an MMA barrier wait gives up.
+int spread_tc_chunk();
+size_t spread_tc_smem(int chunk);
+cudaError_t spread_tc_set_attributes();
+cudaError_t launch_spread_tc(const float *recs, const int *starts, const FrameGeom &g,
+                             const float *strength, float *grid, int *err, cudaStream_t s);
+
 // Density amplitudes of requested lattice points from the half spectra.
 template <typename R>
 cudaError_t launch_gather_modes(const void *G, const BinGeom &b, const int *hkl, int64_t nm,
