@@ -1,5 +1,5 @@
 /*
- * CPU restatement of the NUFFT form of the static S(q) path.  TEST AND BASELINE
+ * CPU restatement of the NUFFT form of the static S(q) path.  TEST AND CPU-BASELINE
  * INFRASTRUCTURE ONLY: it is the timed CPU baseline of the benchmark and a second
  * checker for the tests; the product path never links or calls it.
  *

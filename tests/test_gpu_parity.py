@@ -145,7 +145,7 @@ def test_grid_table_vs_oracle(golden_dir):
 
 
 def test_fp32_form_within_budget(golden_dir):
-    # north_star: FP32 spread/FFT with FP64 accumulation, max |dS| <= 1e-5.
+    # the FP32 precision form (FP32 spread/FFT, FP64 accumulation): max |dS| <= 1e-5.
     _, frames = load_case(golden_dir, "ka_unit_mean")
     scheme = WeightScheme.from_options("neutron", "1:Si,2:O")
     S, Sp, _ = gpu_run(frames, scheme, norm="mean", qmax=6.0, nq=120, eps=1e-6,
