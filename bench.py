@@ -591,6 +591,20 @@ def run_ours(args, rank, world, local_rank):
         kms = stage_ms["spread_ms"] if kern == "spread" else stage_ms["bin_ms"]
         achieved = kb / (kms * 1e-3) / 1e9
         frame_bytes = ntr * (3 * vol * p + (info.nmodes // 2) * 2 * p) + N_ATOMS * (24 + 1)
+        # algorithmic bytes of each stage over its CUDA-event time
+        m = list(info.modes)
+        H1, M2, M3 = (m[0] - 1) // 2 + 1, m[1], m[2]
+        if info.pruned_fft512:
+            fft_bytes = ntr * (vol * p + 2 * nf[2] * nf[1] * H1 * 2 * p
+                               + 2 * nf[2] * M2 * H1 * 2 * p + M3 * M2 * H1 * 2 * p)
+        else:
+            fft_bytes = ntr * (vol * p + vol // nf[0] * c1 * 2 * p)  # one-pass lower bound
+        stage_roofline = {}
+        for name, nbytes, ms in (("spread", spread_bytes, stage_ms["spread_ms"]),
+                                 ("fft", fft_bytes, stage_ms["fft_ms"]),
+                                 ("bin", bin_bytes, stage_ms["bin_ms"])):
+            gbs = nbytes / (ms * 1e-3) / 1e9
+            stage_roofline[name] = {"bytes": int(nbytes), "ms": ms, "gbs": gbs, "frac": gbs / peak}
         frame_ms = 1e3 * elapsed / K
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
@@ -610,7 +624,10 @@ def run_ours(args, rank, world, local_rank):
             "pipeline": {"bytes_per_frame": frame_bytes, "ms_per_frame": frame_ms,
                          "achieved_gbs": frame_bytes / (frame_ms * 1e-3) / 1e9,
                          "frac": frame_bytes / (frame_ms * 1e-3) / 1e9 / peak,
-                         "stage_ms": stage_ms},
+                         "stage_ms": stage_ms, "stage_roofline": stage_roofline,
+                         "stage_roofline_note": "HBM roofline per stage (measured copy "
+                                                "peak); fft = the pruned 512-point passes' "
+                                                "reads and writes"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": fbytes,
                     "d2h_bytes_per_step": NQ * 8},
             "gpu_launches": launches,
