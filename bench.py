@@ -478,7 +478,8 @@ def run_ours(args, rank, world, local_rank):
                                   qmin=0.0, qmax=QMAX, nq=NQ, norm=_lib.NORM_MEAN,
                                   partials=True, precision=prec, eps=eps, device=local_rank,
                                   upsampfac=args.upsampfac, timing=timing,
-                                  stream=stream.cuda_stream, fused_fft=True if args.fused_fft else None)
+                                  stream=stream.cuda_stream, fused_fft=True if args.fused_fft else None,
+                                  spread_tc=args.spread_tc)
 
     # --- device-resident inputs: value --------------------------------------
     dev = torch.from_numpy(frames).to(f"cuda:{local_rank}")
@@ -657,6 +658,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="single", choices=["single", "double"])
     ap.add_argument("--upsampfac", type=float, default=0.0)
+    ap.add_argument("--spread-tc", action="store_true",
+                    help="FP32 spread on the tensor cores (SQN_FLAG_SPREAD_TC)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-grad", action="store_true", help="skip the dS/dr leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-systems leg")

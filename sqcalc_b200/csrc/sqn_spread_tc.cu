@@ -33,6 +33,7 @@ constexpr int B_BYTES = 32 * 8 * 4;       // one K-step of B (32 rows x 8 tf32)
 constexpr int BUF_BYTES = TC_GROUP * 2 * (A_BYTES + B_BYTES);  // one group, hi and lo
 constexpr int OPS_BYTES = 2 * BUF_BYTES;  // two groups: one formed while the other multiplies
 constexpr uint32_t LBO = 128, SBO = 256;  // K-major core-matrix strides (bytes)
+constexpr int FORMER_WARPS = SPREAD_WARPS - 1;  // warp 15 issues the MMAs
 
 // Byte offset of element (row r, k) of a K-major operand step: 8-row groups of
 // 16-byte rows (core matrices), the two K halves LBO apart, groups SBO apart.
@@ -92,6 +93,10 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
   return false;
 }
 
+__device__ __forceinline__ void mbar_arrive(uint32_t mbar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(mbar) : "memory");
+}
+
 __device__ __forceinline__ void tc_fence_before() {
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
 }
@@ -135,7 +140,11 @@ __global__ void __launch_bounds__(SPREAD_THREADS, 2)
   __shared__ int s_wcount[MAX_FAST_T * SPREAD_WARPS];
   __shared__ int s_bl[3][MAX_BINS_DIM];
   __shared__ int s_nbl[3];
-  __shared__ __align__(8) uint64_t s_mbar[2];  // one per operand buffer
+  // per operand buffer: `full` (the formers' arrivals) and `empty` (the MMA commit)
+  __shared__ __align__(8) uint64_t s_full[2], s_empty[2];
+  __shared__ int s_step[64];   // K-step table: transform << 16 | step within it
+  __shared__ int s_tp0[MAX_FAST_T + 1];  // the transforms' point ranges in the chunk
+  __shared__ int s_nsteps;
   __shared__ uint32_t s_tmem;
   __shared__ int s_touched[MAX_FAST_T];
 
@@ -149,7 +158,8 @@ __global__ void __launch_bounds__(SPREAD_THREADS, 2)
   const int ty = min(g.tile[1], g.nf[1] - Y0);
   const int tz = min(g.tile[2], g.nf[2] - Z0);
   const int w = g.w;
-  const uint32_t mbar0 = smem_u32(&s_mbar[0]), mbar1 = smem_u32(&s_mbar[1]);
+  const uint32_t full0 = smem_u32(&s_full[0]), full1 = smem_u32(&s_full[1]);
+  const uint32_t empty0 = smem_u32(&s_empty[0]), empty1 = smem_u32(&s_empty[1]);
 
   // tensor memory for the accumulators, the MMA barrier
   if (warp == 0) {
@@ -160,8 +170,10 @@ __global__ void __launch_bounds__(SPREAD_THREADS, 2)
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar0) : "memory");
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar1) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(full0), "r"(32 * FORMER_WARPS) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(full1), "r"(32 * FORMER_WARPS) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(empty0) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(empty1) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (tid < MAX_FAST_T) s_touched[tid] = 0;
@@ -229,13 +241,10 @@ __global__ void __launch_bounds__(SPREAD_THREADS, 2)
   const float c2 = 4.0f / ((float)w * (float)w);
   const float beta = (float)g.beta;
 
-  // groups committed per operand buffer (each buffer's barrier completes one
-  // phase per commit, and a buffer is refilled only after its last commit)
-  uint32_t ncommit[2] = {0u, 0u};
-  int gcount = 0;  // groups so far: group g uses buffer g & 1
+  int gbase = 0;  // groups so far: group g uses buffer g & 1 for the (g >> 1)-th time
   bool started[NT];
 #pragma unroll
-  for (int t = 0; t < NT; ++t) started[t] = false;  // used by thread 0 only
+  for (int t = 0; t < NT; ++t) started[t] = false;  // used by the issuing thread
 
   for (int base = 0; base < total; base += chunk) {
     // 1. candidates that overlap the tile, counting-sorted by transform
@@ -289,6 +298,22 @@ __global__ void __launch_bounds__(SPREAD_THREADS, 2)
     }
     __syncthreads();
 
+    // K-step table of this chunk (read after the barrier that ends the rows)
+    if (tid == 0) {
+      int ks[NT], kmax = 0, n = 0;
+#pragma unroll
+      for (int t = 0; t < NT; ++t) {
+        ks[t] = (tstart[t + 1] - tstart[t] + 7) / 8;
+        kmax = max(kmax, ks[t]);
+        s_tp0[t] = tstart[t];
+      }
+      s_tp0[NT] = tstart[NT];
+      for (int r = 0; r < kmax; ++r)
+#pragma unroll
+        for (int t = 0; t < NT; ++t)
+          if (r < ks[t] && n < 64) s_step[n++] = (t << 16) | r;
+      s_nsteps = n;
+    }
     // 2. kernel rows shifted onto the tile's cells (x 32, y 16, z 8 times the
     //    strength), zero outside the support or the grid
     for (int e = tid; e < 3 * npts; e += SPREAD_THREADS) {
@@ -312,111 +337,128 @@ __global__ void __launch_bounds__(SPREAD_THREADS, 2)
     }
     __syncthreads();
 
-    // 3. K-steps of eight points of one transform; groups of TC_GROUP steps
-    //    share a barrier and one commit
-    int ksum[NT + 1];
-    ksum[0] = 0;
+    // 3. K-steps of eight points of one transform, interleaved across the
+    //    transforms (consecutive MMAs go to different accumulators), in groups of
+    //    TC_GROUP.  Warps 0..14 form the operands of a group into one of two
+    //    buffers and arrive on its `full` barrier; warp 15 waits for it, issues
+    //    the group's MMAs and commits them to the buffer's `empty` barrier, which
+    //    the formers wait for before they refill that buffer.
+    const int nsteps = s_nsteps;
+    const int ngroups = (nsteps + TC_GROUP - 1) / TC_GROUP;
+    if (warp < FORMER_WARPS) {
+      for (int gi = 0; gi < ngroups; ++gi) {
+        const int gg = gbase + gi, bsel = gg & 1, use = gg >> 1;
+        unsigned char *ops = smem_raw + bsel * BUF_BYTES;
+        if (use > 0) {
+          bool ok = true;
+          if (lane == 0) ok = mbar_wait(bsel ? empty1 : empty0, (uint32_t)(use - 1) & 1u);
+          __syncwarp();
+          if (!ok) atomicExch(err, 1);
+        }
+        if (tid < 128 * TC_GROUP) {
+          // A: thread -> (row m = (y, z), step j)
+          const int m = tid & 127, j = tid >> 7, sidx = gi * TC_GROUP + j;
+          if (sidx < nsteps) {
+            const int st = s_step[sidx], t = st >> 16;
+            const int p0 = s_tp0[t] + 8 * (st & 0xFFFF), pend = s_tp0[t + 1];
+            const int y = m >> 3, z = m & 7;
+            unsigned char *ah = ops + j * A_BYTES;
+            unsigned char *al = ops + TC_GROUP * A_BYTES + j * A_BYTES;
+            float hi[8], lo[8];
 #pragma unroll
-    for (int t = 0; t < NT; ++t) ksum[t + 1] = ksum[t] + (tstart[t + 1] - tstart[t] + 7) / 8;
-    const int nsteps = ksum[NT];
-    for (int g0 = 0; g0 < nsteps; g0 += TC_GROUP, ++gcount) {
-      const int bsel = gcount & 1;
-      const uint32_t mbar = bsel ? mbar1 : mbar0;
-      unsigned char *ops = smem_raw + bsel * BUF_BYTES;
-      // the MMAs of this buffer's previous group have read it
-      if (ncommit[bsel] > 0 && !mbar_wait(mbar, (ncommit[bsel] - 1) & 1u) && tid == 0)
-        atomicExch(err, 1);
-      // A: thread -> (row m = (y, z), step j); B: thread -> (row n = x, step j)
-      if (tid < 128 * TC_GROUP) {
-        const int m = tid & 127, j = tid >> 7, s = g0 + j;
-        if (s < nsteps) {
-          int t = 0;
-#pragma unroll
-          for (int u = 1; u < NT; ++u) t += s >= ksum[u];
-          const int p0 = tstart[t] + 8 * (s - ksum[t]), pend = tstart[t + 1];
-          const int y = m >> 3, z = m & 7;
-          unsigned char *ah = ops + j * A_BYTES;
-          unsigned char *al = ops + TC_GROUP * A_BYTES + j * A_BYTES;
-          float hi[8], lo[8];
-#pragma unroll
-          for (int k = 0; k < 8; ++k) {
-            const int p = p0 + k;
-            float a = 0.0f;
-            if (p < pend) {
-              const float *row = s_rows + (size_t)p * SPREAD_ROW;
-              a = row[TILE_X + y] * row[TILE_X + TILE_Y + z];
+            for (int k = 0; k < 8; ++k) {
+              const int pp = p0 + k;
+              float a = 0.0f;
+              if (pp < pend) {
+                const float *row = s_rows + (size_t)pp * SPREAD_ROW;
+                a = row[TILE_X + y] * row[TILE_X + TILE_Y + z];
+              }
+              hi[k] = to_tf32(a);
+              lo[k] = to_tf32(a - hi[k]);
             }
-            hi[k] = to_tf32(a);
-            lo[k] = to_tf32(a - hi[k]);
+            *reinterpret_cast<float4 *>(ah + kmaj_off(m, 0)) = make_float4(hi[0], hi[1], hi[2], hi[3]);
+            *reinterpret_cast<float4 *>(ah + kmaj_off(m, 4)) = make_float4(hi[4], hi[5], hi[6], hi[7]);
+            *reinterpret_cast<float4 *>(al + kmaj_off(m, 0)) = make_float4(lo[0], lo[1], lo[2], lo[3]);
+            *reinterpret_cast<float4 *>(al + kmaj_off(m, 4)) = make_float4(lo[4], lo[5], lo[6], lo[7]);
           }
-          *reinterpret_cast<float4 *>(ah + kmaj_off(m, 0)) = make_float4(hi[0], hi[1], hi[2], hi[3]);
-          *reinterpret_cast<float4 *>(ah + kmaj_off(m, 4)) = make_float4(hi[4], hi[5], hi[6], hi[7]);
-          *reinterpret_cast<float4 *>(al + kmaj_off(m, 0)) = make_float4(lo[0], lo[1], lo[2], lo[3]);
-          *reinterpret_cast<float4 *>(al + kmaj_off(m, 4)) = make_float4(lo[4], lo[5], lo[6], lo[7]);
-        }
-      } else if (tid < 128 * TC_GROUP + 32 * TC_GROUP) {
-        const int q = tid - 128 * TC_GROUP;
-        const int n = q & 31, j = q >> 5, s = g0 + j;
-        if (s < nsteps) {
-          int t = 0;
+        } else if (tid < 128 * TC_GROUP + 32 * TC_GROUP) {
+          // B: thread -> (row n = x, step j)
+          const int q = tid - 128 * TC_GROUP;
+          const int n = q & 31, j = q >> 5, sidx = gi * TC_GROUP + j;
+          if (sidx < nsteps) {
+            const int st = s_step[sidx], t = st >> 16;
+            const int p0 = s_tp0[t] + 8 * (st & 0xFFFF), pend = s_tp0[t + 1];
+            unsigned char *bh = ops + 2 * TC_GROUP * A_BYTES + j * B_BYTES;
+            unsigned char *bl = ops + 2 * TC_GROUP * A_BYTES + TC_GROUP * B_BYTES + j * B_BYTES;
+            float hi[8], lo[8];
 #pragma unroll
-          for (int u = 1; u < NT; ++u) t += s >= ksum[u];
-          const int p0 = tstart[t] + 8 * (s - ksum[t]), pend = tstart[t + 1];
-          unsigned char *bh = ops + 2 * TC_GROUP * A_BYTES + j * B_BYTES;
-          unsigned char *bl = ops + 2 * TC_GROUP * A_BYTES + TC_GROUP * B_BYTES + j * B_BYTES;
-          float hi[8], lo[8];
-#pragma unroll
-          for (int k = 0; k < 8; ++k) {
-            const int p = p0 + k;
-            const float b = p < pend ? s_rows[(size_t)p * SPREAD_ROW + n] : 0.0f;
-            hi[k] = to_tf32(b);
-            lo[k] = to_tf32(b - hi[k]);
+            for (int k = 0; k < 8; ++k) {
+              const int pp = p0 + k;
+              const float b = pp < pend ? s_rows[(size_t)pp * SPREAD_ROW + n] : 0.0f;
+              hi[k] = to_tf32(b);
+              lo[k] = to_tf32(b - hi[k]);
+            }
+            *reinterpret_cast<float4 *>(bh + kmaj_off(n, 0)) = make_float4(hi[0], hi[1], hi[2], hi[3]);
+            *reinterpret_cast<float4 *>(bh + kmaj_off(n, 4)) = make_float4(hi[4], hi[5], hi[6], hi[7]);
+            *reinterpret_cast<float4 *>(bl + kmaj_off(n, 0)) = make_float4(lo[0], lo[1], lo[2], lo[3]);
+            *reinterpret_cast<float4 *>(bl + kmaj_off(n, 4)) = make_float4(lo[4], lo[5], lo[6], lo[7]);
           }
-          *reinterpret_cast<float4 *>(bh + kmaj_off(n, 0)) = make_float4(hi[0], hi[1], hi[2], hi[3]);
-          *reinterpret_cast<float4 *>(bh + kmaj_off(n, 4)) = make_float4(hi[4], hi[5], hi[6], hi[7]);
-          *reinterpret_cast<float4 *>(bl + kmaj_off(n, 0)) = make_float4(lo[0], lo[1], lo[2], lo[3]);
-          *reinterpret_cast<float4 *>(bl + kmaj_off(n, 4)) = make_float4(lo[4], lo[5], lo[6], lo[7]);
         }
+        // this thread's generic-proxy writes -> the tensor core's reads; then
+        // every former thread arrives on the buffer's `full` barrier
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_arrive(bsel ? full1 : full0);
       }
-      // generic-proxy writes -> the tensor core's reads
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      __syncthreads();
-      if (tid == 0) {
-        tc_fence_after();
-        const uint32_t obase = smem_u32(ops);
-        for (int j = 0; j < TC_GROUP; ++j) {
-          const int s = g0 + j;
-          if (s >= nsteps) break;
-          int t = 0;
+    } else {
+      for (int gi = 0; gi < ngroups; ++gi) {
+        const int gg = gbase + gi, bsel = gg & 1, use = gg >> 1;
+        bool ok = true;
+        if (lane == 0) ok = mbar_wait(bsel ? full1 : full0, (uint32_t)use & 1u);
+        __syncwarp();
+        if (lane == 0) {
+          if (!ok) atomicExch(err, 1);
+          tc_fence_after();
+          const uint32_t obase = smem_u32(smem_raw + bsel * BUF_BYTES);
+          for (int j = 0; j < TC_GROUP; ++j) {
+            const int sidx = gi * TC_GROUP + j;
+            if (sidx >= nsteps) break;
+            const int t = s_step[sidx] >> 16;
+            const uint32_t ah = obase + j * A_BYTES, al = obase + (TC_GROUP + j) * A_BYTES;
+            const uint32_t bh = obase + 2 * TC_GROUP * A_BYTES + j * B_BYTES;
+            const uint32_t bl = bh + TC_GROUP * B_BYTES;
+            const uint32_t d = tmem + 32u * (uint32_t)t;
+            bool stt = false;
 #pragma unroll
-          for (int u = 1; u < NT; ++u) t += s >= ksum[u];
-          const uint32_t ah = obase + j * A_BYTES, al = obase + (TC_GROUP + j) * A_BYTES;
-          const uint32_t bh = obase + 2 * TC_GROUP * A_BYTES + j * B_BYTES;
-          const uint32_t bl = bh + TC_GROUP * B_BYTES;
-          const uint32_t d = tmem + 32u * (uint32_t)t;
-          bool st = false;
+            for (int u = 0; u < NT; ++u)
+              if (u == t) stt = started[u];
+            mma_tf32(d, smem_desc(ah), smem_desc(bh), stt ? 1u : 0u);
+            mma_tf32(d, smem_desc(ah), smem_desc(bl), 1u);
+            mma_tf32(d, smem_desc(al), smem_desc(bh), 1u);
 #pragma unroll
-          for (int u = 0; u < NT; ++u)
-            if (u == t) st = started[u];
-          mma_tf32(d, smem_desc(ah), smem_desc(bh), st ? 1u : 0u);
-          mma_tf32(d, smem_desc(ah), smem_desc(bl), 1u);
-          mma_tf32(d, smem_desc(al), smem_desc(bh), 1u);
-#pragma unroll
-          for (int u = 0; u < NT; ++u)
-            if (u == t) started[u] = true;
-          s_touched[t] = 1;
+            for (int u = 0; u < NT; ++u)
+              if (u == t) started[u] = true;
+            s_touched[t] = 1;
+          }
+          mma_commit(bsel ? empty1 : empty0);
         }
-        mma_commit(mbar);
+        __syncwarp();
       }
-      ++ncommit[bsel];
     }
-    // the next chunk rewrites s_meta, s_off and s_rows, which the MMAs do not read
+    gbase += ngroups;
+    // the next chunk rewrites s_meta, s_off, s_rows and the step table, which
+    // the MMAs do not read
     __syncthreads();
   }
 
-  // 4. the last groups' MMAs done, each row (y, z) of each transform out
-  if (ncommit[0] > 0 && !mbar_wait(mbar0, (ncommit[0] - 1) & 1u) && tid == 0) atomicExch(err, 1);
-  if (ncommit[1] > 0 && !mbar_wait(mbar1, (ncommit[1] - 1) & 1u) && tid == 0) atomicExch(err, 1);
+  // 4. the last groups' MMAs done (the last use of each buffer), each row
+  //    (y, z) of each transform out
+  {
+    const int uses0 = (gbase + 1) / 2, uses1 = gbase / 2;
+    bool ok = true;
+    if (uses0 > 0) ok = mbar_wait(empty0, (uint32_t)(uses0 - 1) & 1u) && ok;
+    if (uses1 > 0) ok = mbar_wait(empty1, (uint32_t)(uses1 - 1) & 1u) && ok;
+    if (!ok && tid == 0) atomicExch(err, 1);
+  }
   tc_fence_after();
   __syncthreads();
   if (warp < 4 * NT) {
