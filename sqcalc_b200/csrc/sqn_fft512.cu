@@ -52,6 +52,48 @@ template <typename C> __device__ __forceinline__ C c_mul(C a, C w) {
   r.y = a.x * w.y + a.y * w.x;
   return r;
 }
+// FP32: one packed instruction (add/sub.rn.f32x2, sm_100) per complex add.
+__device__ __forceinline__ float2 c_add(float2 a, float2 b) {
+  float2 r;
+  asm("{\n\t.reg .b64 pa, pb;\n\t"
+      "mov.b64 pa, {%2, %3};\n\t"
+      "mov.b64 pb, {%4, %5};\n\t"
+      "add.rn.f32x2 pa, pa, pb;\n\t"
+      "mov.b64 {%0, %1}, pa;\n\t}"
+      : "=f"(r.x), "=f"(r.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+}
+__device__ __forceinline__ float2 c_sub(float2 a, float2 b) {
+  float2 r;
+  asm("{\n\t.reg .b64 pa, pb;\n\t"
+      "mov.b64 pa, {%2, %3};\n\t"
+      "mov.b64 pb, {%4, %5};\n\t"
+      "sub.rn.f32x2 pa, pa, pb;\n\t"
+      "mov.b64 {%0, %1}, pa;\n\t}"
+      : "=f"(r.x), "=f"(r.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+}
+// o + s a for s = +-1 (one rounding, as o + a or o - a)
+template <typename C, typename R> __device__ __forceinline__ C c_sfma(R s, C a, C o) {
+  C r;
+  r.x = fma(s, a.x, o.x);
+  r.y = fma(s, a.y, o.y);
+  return r;
+}
+__device__ __forceinline__ float2 c_sfma(float s, float2 a, float2 o) {
+  float2 r;
+  asm("{\n\t.reg .b64 ps, pa, po;\n\t"
+      "mov.b64 ps, {%2, %2};\n\t"
+      "mov.b64 pa, {%3, %4};\n\t"
+      "mov.b64 po, {%5, %6};\n\t"
+      "fma.rn.f32x2 po, ps, pa, po;\n\t"
+      "mov.b64 {%0, %1}, po;\n\t}"
+      : "=f"(r.x), "=f"(r.y)
+      : "f"(s), "f"(a.x), "f"(a.y), "f"(o.x), "f"(o.y));
+  return r;
+}
 // a * exp(-i theta) for cos theta = c, sin theta = s
 template <typename C, typename R> __device__ __forceinline__ C c_rot(C a, R c, R s) {
   C r;
@@ -63,15 +105,14 @@ template <typename C, typename R> __device__ __forceinline__ C c_rot(C a, R c, R
 // 4-point forward DFT in place.
 template <typename C> __device__ __forceinline__ void dft4(C &v0, C &v1, C &v2, C &v3) {
   const C a0 = c_add(v0, v2), a1 = c_sub(v0, v2);
-  const C a2 = c_add(v1, v3);
-  C a3 = c_sub(v1, v3);  // times -i
-  const auto t = a3.x;
-  a3.x = a3.y;
-  a3.y = -t;
+  const C a2 = c_add(v1, v3), a3 = c_sub(v1, v3);
   v0 = c_add(a0, a2);
   v2 = c_sub(a0, a2);
-  v1 = c_add(a1, a3);
-  v3 = c_sub(a1, a3);
+  // v1 = a1 - i a3, v3 = a1 + i a3
+  v1.x = a1.x + a3.y;
+  v1.y = a1.y - a3.x;
+  v3.x = a1.x - a3.y;
+  v3.y = a1.y + a3.x;
 }
 
 // 16-point forward DFT in registers, natural order in and out:
@@ -117,8 +158,10 @@ template <typename C> __device__ __forceinline__ C shfl_xor16(C v) {
 
 // Skewed slot of element (k2, n1) of the transpose (512 slots): the writes
 // (fixed k2, lanes over n1) and the reads (fixed m2, lanes over k2 and m1 with
-// n1 = m1 + 2 m2) both touch every 8-byte bank pair exactly twice.
-__device__ __forceinline__ int tslot(int k2, int n1) { return k2 * 32 + ((n1 + k2) & 31); }
+// n1 = m1 + 2 m2) both touch every 8-byte bank pair exactly twice (slot mod 16
+// is (n1 ^ k2) mod 16, a bijection of n1 mod 16 for fixed k2 and of k2 for
+// fixed n1).
+__device__ __forceinline__ int tslot(int k2, int n1) { return k2 * 32 + (n1 ^ k2); }
 
 // Twiddle table (TW_LEN entries): tw[m] = exp(-2 pi i m / 512) for m < 512,
 // then tw[512 + 32 k2 + n1] = exp(-2 pi i n1 k2 / 512), the per-lane factors
@@ -147,11 +190,11 @@ __device__ __forceinline__ void warp_fft512(C (&v)[16], C *scr, int sstride, con
 #pragma unroll
     for (int a = 1; a < 16; ++a) v[a] = c_mul(v[a], tw[16 * a]);  // exp(-2 pi i a / 32)
   }
+  // lanes m1 = 0 form v + o, lanes m1 = 1 form o - v
+  using R = decltype(v[0].x);
+  const R sg = m1 ? R(-1) : R(1);
 #pragma unroll
-  for (int a = 0; a < 16; ++a) {
-    const C o = shfl_xor16(v[a]);
-    v[a] = m1 ? c_sub(o, v[a]) : c_add(v[a], o);
-  }
+  for (int a = 0; a < 16; ++a) v[a] = c_sfma(sg, v[a], shfl_xor16(v[a]));
 }
 
 // ---------------------------------------------------------------------------
@@ -256,7 +299,10 @@ __global__ void __launch_bounds__(32 * COLS, sizeof(R) == 4 ? 2 : 1)
       for (int k0 = 0; k0 < 512 / 32; k0 += 8) {
         C ld[8];
 #pragma unroll
-        for (int k = 0; k < 8; ++k) ld[k] = src[(k0 + k) * step];
+        for (int k = 0; k < 8; ++k) {
+          ld[k] = src[0];
+          src += step;
+        }
 #pragma unroll
         for (int k = 0; k < 8; ++k) tile[(r0 + 32 * (k0 + k)) * COL_LD + c] = ld[k];
       }
@@ -275,12 +321,16 @@ __global__ void __launch_bounds__(32 * COLS, sizeof(R) == 4 ? 2 : 1)
       for (int a = 0; a < 16; ++a) col[(k2 + 16 * a + 256 * b) * COL_LD] = v[a];
     }
     __syncthreads();
-    for (int e = threadIdx.x; e < M * COLS; e += blockDim.x) {
-      const int hw = e >> 4, c = e & (COLS - 1);
-      if (c < nc) {
-        const int h = hw <= cp.hm ? hw : hw - M;
-        ob[(int64_t)hw * cp.out_r + c] = tile[(h & 511) * COL_LD + c];
-      }
+    // output rows hw = 0 .. hm come from tile rows hw, rows hm + 1 .. M - 1
+    // (h = hw - M < 0) from tile rows 512 + hw - M
+    if (c < nc) {
+      const int64_t ostep = 32 * cp.out_r;
+      C *dst = ob + (int64_t)r0 * cp.out_r + c;
+      const C *tp = tile + r0 * COL_LD + c;
+      int hw = r0;
+      for (; hw <= cp.hm; hw += 32, tp += 32 * COL_LD, dst += ostep) *dst = *tp;
+      tp += (512 - M) * COL_LD;
+      for (; hw < M; hw += 32, tp += 32 * COL_LD, dst += ostep) *dst = *tp;
     }
   }
 }
