@@ -281,12 +281,14 @@ __global__ void __launch_bounds__(32 * COLS, sizeof(R) == 4 ? 2 : 1)
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nblk = (cp.ncols + COLS - 1) / COLS;
   const int M = 2 * cp.hm + 1;
-  const int64_t nsteps = cp.nplanes * nblk;
-  for (int64_t st = blockIdx.x; st < nsteps; st += gridDim.x) {
-    const int64_t plane = st / nblk;
-    const int c0 = (int)(st - plane * nblk) * COLS;
+  // 32-bit step indices (the host keeps nplanes * nblk below 2^31): the
+  // divisions below are then a few instructions, not a 64-bit division routine
+  const unsigned nsteps = (unsigned)cp.nplanes * (unsigned)nblk;
+  for (unsigned st = blockIdx.x; st < nsteps; st += gridDim.x) {
+    const unsigned plane = st / (unsigned)nblk;
+    const int c0 = (int)(st - plane * (unsigned)nblk) * COLS;
     const int nc = min(COLS, cp.ncols - c0);
-    const int64_t t = plane / cp.planes_per_t, p = plane - t * cp.planes_per_t;
+    const unsigned t = plane / (unsigned)cp.planes_per_t, p = plane - t * cp.planes_per_t;
     const C *ib = in + t * cp.in_t + p * cp.in_p + c0;
     C *ob = out + t * cp.out_t + p * cp.out_p + c0;
     // a thread's loads (column c, rows r0 + 32 k) go out eight at a time
@@ -368,6 +370,7 @@ cudaError_t launch_fft512(const R *grid, void *A1, void *A2, void *G, int ntr, i
   const int n = 512;
   const int M2 = 2 * hm1 + 1, M3 = 2 * hm2 + 1;
   const int64_t nrows = (int64_t)ntr * n * n;
+  if ((int64_t)ntr * n * ((H1 + COLS - 1) / COLS) >= ((int64_t)1 << 31)) return cudaErrorInvalidValue;
   k_fft512_x<R><<<nsm * 8, 32 * x_warps<R>(), 0, s>>>(grid, (C *)A1, nrows, pitch, H1,
                                                       (const C *)tw);
   cudaError_t e = cudaGetLastError();
