@@ -78,6 +78,11 @@ enum {
                                 instead of the CUDA cores.  Off by default: measured
                                 slower on B200 (the per-tile MMAs are small and chained
                                 on one accumulator) */
+  SQN_FLAG_FFT_RING = 64,  /* FP32 plans on the pruned 512-point passes (even H1 = hm0 + 1):
+                              the y and z passes in the ring form (a producer warp streams
+                              column tiles into shared memory with bulk copies while two
+                              groups of compute warps transform and store earlier tiles).
+                              Off by default: experimental, not yet measured on B200 */
   SQN_FLAG_PIPELINE = 16   /* keep a second fine grid and run the FFT and binning of
                               frame f on an internal stream while frame f + 1 is sorted
                               and spread on the plan's stream (not with SQN_FLAG_TIMING,
@@ -146,7 +151,9 @@ typedef struct sqn_plan_info {
   int64_t natoms;           /* atoms per frame */
   int32_t xrd_bins;         /* two-theta bins of the powder pattern (0: off) */
   int32_t pruned_fft512;    /* 1: the frame FFT runs as pruned 512-point passes of ours
-                               (every axis 512, no SQN_FLAG_CUFFT) instead of cuFFT */
+                               (every axis 512, no SQN_FLAG_CUFFT) instead of cuFFT;
+                               2: the same with the column passes in the ring form
+                               (SQN_FLAG_FFT_RING) */
   double xrd_step;          /* their width, degrees */
 } sqn_plan_info;
 

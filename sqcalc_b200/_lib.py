@@ -27,6 +27,7 @@ FLAG_FUSED_FFT = 4
 FLAG_CUFFT = 8
 FLAG_PIPELINE = 16
 FLAG_SPREAD_TC = 32
+FLAG_FFT_RING = 64
 
 # Every symbol include/sqnufft.h declares.
 EXPORTS = (
@@ -218,13 +219,14 @@ class Plan:
                  xray_coef=None, qmin=0.0, qmax=20.0, nq=500, norm=NORM_MEAN, partials=True,
                  want_grid=False, precision=PREC_DOUBLE, eps=1e-9, upsampfac=0.0,
                  kernel_width=0, device=0, max_grid_modes=0, timing=False, stream=None,
-                 grad=False, fused_fft=None, xrd=None, pipeline=False, spread_tc=False):
+                 grad=False, fused_fft=None, xrd=None, pipeline=False, spread_tc=False,
+                 fft_ring=False):
         L = load()
         self._L = L
         d = self._describe(cell, origin, type_id, ntypes, weight, amp_const, xray_coef, qmin,
                            qmax, nq, norm, partials, want_grid, precision, eps, upsampfac,
                            kernel_width, device, max_grid_modes, timing, stream, grad, fused_fft,
-                           xrd, pipeline, spread_tc)
+                           xrd, pipeline, spread_tc, fft_ring)
         h = ctypes.c_void_p()
         self.status = check(L.sqn_plan_create(ctypes.byref(d), ctypes.byref(h)), "sqn_plan_create")
         self._attach(h, owned=True)
@@ -233,12 +235,14 @@ class Plan:
                   xray_coef=None, qmin=0.0, qmax=20.0, nq=500, norm=NORM_MEAN, partials=True,
                   want_grid=False, precision=PREC_DOUBLE, eps=1e-9, upsampfac=0.0,
                   kernel_width=0, device=0, max_grid_modes=0, timing=False, stream=None,
-                  grad=False, fused_fft=None, xrd=None, pipeline=False, spread_tc=False):
+                  grad=False, fused_fft=None, xrd=None, pipeline=False, spread_tc=False,
+                  fft_ring=False):
         """Fill an SqnDesc; the arrays it points to are kept on self.  xrd: None, or a
         dict(lam=..., range=(min, max), step=0.0, lp=True) for the powder pattern.
         pipeline: FFT and binning of frame f on a second stream beside the spread of
         frame f + 1 (a second fine grid).  spread_tc: FP32 spread on the tensor cores
-        (tcgen05) instead of the CUDA cores."""
+        (tcgen05) instead of the CUDA cores.  fft_ring: FP32 column passes of the pruned
+        512-point FFT in the ring form (experimental)."""
         L = self._L
         self.type_id = np.ascontiguousarray(type_id, dtype=np.int32)
         self.natoms = int(self.type_id.size)
@@ -272,7 +276,8 @@ class Plan:
         d.flags = ((FLAG_TIMING if timing else 0) | (FLAG_GRAD if grad else 0)
                    | (0 if fused_fft is None else (FLAG_FUSED_FFT if fused_fft else FLAG_CUFFT))
                    | (FLAG_PIPELINE if pipeline else 0)
-                   | (FLAG_SPREAD_TC if spread_tc else 0))
+                   | (FLAG_SPREAD_TC if spread_tc else 0)
+                   | (FLAG_FFT_RING if fft_ring else 0))
         d.eps = float(eps)
         d.upsampfac = float(upsampfac)
         d.kernel_width = int(kernel_width)

@@ -274,6 +274,7 @@ struct sqn_plan_s {
   int tc_chunk = 0;
   int *d_err = nullptr;    // set by a kernel whose bounded wait gave up
   bool fft512 = false;
+  bool fft_ring = false;  // FP32: column passes in the ring form (SQN_FLAG_FFT_RING)
   void *d_tw512 = nullptr;
   BinGeom bg512{};
   // density amplitudes (sqn_density_modes): request buffers, grown on demand
@@ -781,6 +782,14 @@ int setup_plan(sqn_plan *p, const sqn_plan_desc *d) {
     p->bg512.c1 = p->hm[0] + 1;
     p->bg512.vol_cplx = p->bg512.c1 * p->bg512.nf[1] * p->bg512.nf[2];
     p->fft512 = true;
+    if (!p->fp64 && (d->flags & SQN_FLAG_FFT_RING) && (p->hm[0] + 1) % 2 == 0) {
+      if (!p->d_err) {
+        if ((st = dalloc(p, &p->d_err, 1))) return st;
+        if (cudaMemset(p->d_err, 0, sizeof(int)) != cudaSuccess) return SQN_ERR_CUDA;
+      }
+      if (fft512_ring_set_attributes() != cudaSuccess) return SQN_ERR_CUDA;
+      p->fft_ring = true;
+    }
   }
 
   // --- adjoint buffers (dS/dr) -----------------------------------------------
@@ -1159,7 +1168,8 @@ template <typename R> int run_frame(sqn_plan *p, const double *dpos, int slot) {
     if (p->fft512) {
       // x pass into d_G, y pass back into the (consumed) grid, z pass into d_G
       e = launch_fft512<R>((const R *)grid, p->d_G, grid, p->d_G, p->ntr, g.pitch,
-                           p->hm[0] + 1, p->hm[1], p->hm[2], p->d_tw512, p->nsm, fs);
+                           p->hm[0] + 1, p->hm[1], p->hm[2], p->d_tw512, p->nsm, fs,
+                           p->fft_ring ? 1 : 0, p->d_err);
       if (e != cudaSuccess) return SQN_ERR_CUDA;
       p->launches += 3;
     } else if (exec_forward(p, fs, grid, p->d_G) != CUFFT_SUCCESS) {
@@ -1298,7 +1308,7 @@ int sqn_plan_info_get(const sqn_plan *p, sqn_plan_info *info) {
   info->device_bytes = p->device_bytes;
   info->fused_fft = p->fused ? 1 : 0;
   info->pipelined = p->overlap ? 1 : 0;
-  info->pruned_fft512 = p->fft512 ? 1 : 0;
+  info->pruned_fft512 = p->fft512 ? (p->fft_ring ? 2 : 1) : 0;
   info->natoms = p->desc.natoms;
   info->xrd_bins = p->bg.xrd ? p->bg.xbins : 0;
   info->xrd_step = p->bg.xrd ? p->bg.xstep : 0.0;
