@@ -478,8 +478,7 @@ def run_ours(args, rank, world, local_rank):
                                   qmin=0.0, qmax=QMAX, nq=NQ, norm=_lib.NORM_MEAN,
                                   partials=True, precision=prec, eps=eps, device=local_rank,
                                   upsampfac=args.upsampfac, timing=timing,
-                                  stream=stream.cuda_stream, fused_fft=True if args.fused_fft else None,
-                                  spread_tc=args.spread_tc)
+                                  stream=stream.cuda_stream, fft_ring=args.fft_ring)
 
     # --- device-resident inputs: value --------------------------------------
     dev = torch.from_numpy(frames).to(f"cuda:{local_rank}")
@@ -502,7 +501,6 @@ def run_ours(args, rank, world, local_rank):
         ev0.record(stream)
         for f in range(W, W + K):
             plan.accumulate((base + (f % NFR) * fbytes, 1), where=_lib.DEVICE)
-        plan.join()  # the last frame's FFT and binning run on the plan's FFT stream
         ev1.record(stream)
         torch.cuda.synchronize()
         clk.mark(tm0, time.monotonic())
@@ -658,14 +656,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="single", choices=["single", "double"])
     ap.add_argument("--upsampfac", type=float, default=0.0)
-    ap.add_argument("--spread-tc", action="store_true",
-                    help="FP32 spread on the tensor cores (SQN_FLAG_SPREAD_TC)")
+    ap.add_argument("--fft-ring", action="store_true",
+                    help="FP32 column FFT passes in the ring form (SQN_FLAG_FFT_RING)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-grad", action="store_true", help="skip the dS/dr leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-systems leg")
     ap.add_argument("--no-ingest", action="store_true", help="skip the text-dump ingest leg")
-    ap.add_argument("--fused-fft", action="store_true",
-                    help="frame path on the pruned FFT passes fused with the binning")
     ap.add_argument("--scale", type=float, default=1.0,
                     help="shrink the box by this factor at fixed density (profiling only)")
     args = ap.parse_args()

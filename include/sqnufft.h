@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define SQN_ABI_VERSION 1
+#define SQN_ABI_VERSION 2
 
 /* Status codes.  Values shared with FINUFFT keep FINUFFT's numbering
  * (external/finufft/include/finufft_errors.h:5-31). */
@@ -68,27 +68,13 @@ enum { SQN_HOST = 0, SQN_DEVICE = 1 };
 enum {
   SQN_FLAG_TIMING = 1, /* record per-stage CUDA events (sqn_stage_times) */
   SQN_FLAG_GRAD = 2,   /* allocate the adjoint buffers of sqn_sq_grad */
-  SQN_FLAG_FUSED_FFT = 4, /* frame path on the pruned FFT passes fused with the binning
-                             (2,3,5-smooth axes <= 4096) instead of cuFFT R2C + the bin
-                             kernel (the default, faster on B200 at the benchmark sizes) */
   SQN_FLAG_CUFFT = 8,      /* cuFFT R2C + the bin kernel (instead of the pruned 512-point
                               passes that 512^3 grids use by default) */
-  SQN_FLAG_SPREAD_TC = 32,   /* FP32 plans with 1 to 4 transforms: spread on the tensor
-                                cores (tcgen05, 3xTF32, accumulators in tensor memory)
-                                instead of the CUDA cores.  Off by default: measured
-                                slower on B200 (the per-tile MMAs are small and chained
-                                on one accumulator) */
   SQN_FLAG_FFT_RING = 64,  /* FP32 plans on the pruned 512-point passes (even H1 = hm0 + 1):
                               the y and z passes in the ring form (a producer warp streams
                               column tiles into shared memory with bulk copies while two
                               groups of compute warps transform and store earlier tiles).
                               Off by default: experimental, not yet measured on B200 */
-  SQN_FLAG_PIPELINE = 16   /* keep a second fine grid and run the FFT and binning of
-                              frame f on an internal stream while frame f + 1 is sorted
-                              and spread on the plan's stream (not with SQN_FLAG_TIMING,
-                              SQN_FLAG_GRAD or the fused path).  Off by default: on B200
-                              the two halves time-share the SMs, and with the pruned
-                              512-point passes the pipelined plan is slower */
 };
 
 /* Everything sqcalc's configure + gpu_setup know after the first frame
@@ -145,9 +131,6 @@ typedef struct sqn_plan_info {
   int32_t nspecies;         /* type ids that have atoms */
   int64_t device_bytes;     /* device memory the plan holds */
   int64_t tile[3];          /* spread tile in fine-grid cells */
-  int32_t fused_fft;        /* 1: pruned FFT passes fused with the binning; 0: cuFFT + bin kernel */
-  int32_t pipelined;        /* 1: two fine grids, FFT + binning of frame f beside the
-                               spread of frame f + 1 (see SQN_FLAG_PIPELINE) */
   int64_t natoms;           /* atoms per frame */
   int32_t xrd_bins;         /* two-theta bins of the powder pattern (0: off) */
   int32_t pruned_fft512;    /* 1: the frame FFT runs as pruned 512-point passes of ours
@@ -182,17 +165,17 @@ int sqn_plan_info_get(const sqn_plan *plan, sqn_plan_info *info);
  * Replaces one gpu_accumulate per frame (src/sqc_gpu.f90:213-362: host wrap,
  * uploads, cufinufft_setpts / execute, download, host pair sums and binning).
  * The call returns once the positions have been read; the transforms run
- * asynchronously on the plan's stream and its internal FFT stream (device
- * positions are read in the plan's stream order and must stay valid until
- * sqn_sync). */
+ * asynchronously on the plan's stream (device positions are read in the
+ * plan's stream order and must stay valid until sqn_sync). */
 int sqn_accumulate_frames(sqn_plan *plan, const double *pos, int64_t nframes, int32_t where);
 
-/* Make the plan's stream wait for the plan's internal FFT stream, without
- * blocking the host: work queued on the plan's stream after this call (an event,
- * a collective on the accumulators) comes after every queued frame. */
+/* Order everything queued so far before work the caller queues next on the
+ * plan's stream (an event, a collective on the accumulators), without blocking
+ * the host.  Every kernel of a plan runs on its one stream, so this only checks
+ * the plan; it stays for callers written against a plan with several streams. */
 int sqn_join(sqn_plan *plan);
 
-/* Wait for all queued work of the plan (both of its streams). */
+/* Wait for all queued work of the plan. */
 int sqn_sync(sqn_plan *plan);
 
 /* Copy the accumulators out (syncs first).  Any pointer may be NULL.
@@ -384,12 +367,14 @@ int sqn_batch_destroy(sqn_batch *batch);
 /* Wrap, bin-sort and spread one frame onto caller-provided fine grids WITHOUT
  * allocating any device memory.  No counterpart in the reference: it is for
  * callers that cannot call cudaMalloc -- a host framework that owns all device
- * memory through its own pool, a caller in the middle of recording a CUDA graph
- * (allocation is illegal during a global-mode stream capture), a service that
- * must not grow its footprint per request.
+ * memory through its own pool, a plugin inside an application that has already
+ * reserved the device memory, a service that must keep a fixed footprint.
  *   pos       [natoms][3] FP64 Cartesian positions, device memory
- *   species   [natoms] grid index of each atom (0..ntr-1), host memory
+ *   species   [natoms] grid index of each atom (0..ntr-1), host memory; every
+ *             index is checked on the host before anything is queued
+ *   ntr       1 .. 8 grids (more: SQN_ERR_INVALID_ARGUMENT)
  *   strength  [ntr] FP32 strength of the atoms of each grid, host memory
+ *             (species and strength are copied with cudaMemcpyAsync on stream)
  *   cell, origin, nf[3], kernel_width, beta: as sqn_plan_info reports them
  *   grid      [ntr][nf3][nf2][nf1] FP32 output, device memory, x fastest;
  *             every cell is written (no zeroing needed)

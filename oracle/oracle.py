@@ -459,3 +459,85 @@ def direct_xrd(frames, type_id, cell, origin, weights: Weights, lam, tmin, tmax,
     norm = len(frames) * len(type_id)
     cnt = np.bincount(b, minlength=nb)
     return tmin + (np.arange(nb) + 0.5) * step, I / norm, Ip / norm, cnt, qmin, qmax
+
+
+def direct_sq_separable(frames, type_id, cell, origin, weights: Weights, qmin, qmax, nq,
+                        norm=NORM_MEAN, partials=True, ntypes=None, slab_modes=None):
+    """The FP64 direct sum of ``direct_sq`` (direct_accumulate,
+    src/sqc_structure_factor.f90:1398-1515, on the wrapped positions r = A s of
+    :1431-1435) evaluated slab by slab for grids far too large for the per-mode
+    loop: with s the wrapped fractional coordinates, q_h . (A s) = 2 pi h . s, so
+    exp(i q_h . r_j) = E1[h1, j] E2[h2, j] E3[h3, j] with E_d[h, j] = exp(2 pi i h s_jd)
+    and, for one h3 slab, rho_a[h1, h2] = sum_{j of a} E1[h1, j] (E2[h2, j] E3[h3, j])
+    is one complex matrix product per type.  The kept test, |q| and the shell of
+    every mode use the reference's FP64 operation order (:366-399, as
+    ``sqo_enumerate``), so the kept set and the shells are those of ``direct_sq``;
+    den and shell_count follow mode_denominator (:425-451).  Only the evaluation
+    order of the sum over atoms differs from ``direct_sq`` (agreement ~1e-13).
+    Unit and neutron weights (q-independent amplitudes).  Returns (modes, acc)."""
+    if weights.kind == WEIGHT_XRAY:
+        raise ValueError("direct_sq_separable takes unit or neutron weights")
+    L = lib()
+    type_id = _c(type_id, np.int32)
+    natoms = len(type_id)
+    ntypes = int(ntypes or max(int(type_id.max()), 1))
+    flat = _c(np.asarray(cell, dtype=np.float64).reshape(9), np.float64)
+    inv = np.zeros(9)
+    recip = np.zeros(9)
+    L.sqo_cell_setup(flat, inv, recip)
+    modes = np.zeros(3, dtype=np.int32)
+    if L.sqo_modes(flat, float(qmax), modes) != 0:
+        raise ValueError("degenerate simulation cell")
+    hm = (modes.astype(np.int64) - 1) // 2
+    b = recip  # b_j = recip[3 j : 3 j + 3]
+    dq = (qmax - qmin) / float(nq)
+    counts = type_counts_of(type_id, ntypes)
+    amp, _ = weights.padded(ntypes)
+    present = [t for t in range(1, ntypes + 1) if counts[t - 1] > 0]
+    members = {t: np.nonzero(type_id == t)[0] for t in present}
+    # per-mode denominator: q-independent for unit / neutron weights
+    mode_den = _mode_den(norm, weights, counts, natoms, ntypes, 0.0)
+    h1 = np.arange(-hm[0], hm[0] + 1, dtype=np.float64)[:, None]
+    h2 = np.arange(-hm[1], hm[1] + 1, dtype=np.float64)[None, :]
+    num = np.zeros(nq)
+    cnt = np.zeros(nq, dtype=np.int64)
+    pn = np.zeros((ntypes, ntypes, nq))
+    frac_all = []
+    for pos in frames:
+        frac = np.zeros(3 * natoms)
+        L.sqo_wrap(natoms, _c(pos, np.float64).reshape(-1), flat, _c(origin, np.float64), frac)
+        frac_all.append(frac.reshape(natoms, 3))
+    E = [[np.exp(2j * np.pi * np.arange(-hm[d], hm[d] + 1)[:, None] * fr[None, :, d])
+          for d in range(3)] for fr in frac_all]
+    for k3 in range(-int(hm[2]), int(hm[2]) + 1):
+        # |q| in the reference's order: q_r = (b1_r h1 + b2_r h2) + b3_r h3
+        q = [(b[r] * h1 + b[3 + r] * h2) + b[6 + r] * float(k3) for r in range(3)]
+        ql = np.sqrt((q[0] * q[0] + q[1] * q[1]) + q[2] * q[2])
+        keep = (ql <= qmax) & (ql >= qmin)
+        if k3 == 0:
+            keep[hm[0], hm[1]] = False
+        if not keep.any():
+            continue
+        sh = np.clip(((ql[keep] - qmin) / dq).astype(np.int64), 0, nq - 1)
+        cnt += np.bincount(sh, minlength=nq)
+        for f in range(len(frames)):
+            E1, E2, E3 = E[f]
+            rho = {}
+            for t in present:
+                j = members[t]
+                B = E2[:, j] * E3[k3 + hm[2], j][None, :]
+                rho[t] = (E1[:, j] @ B.T)[keep]
+            tot = sum(amp[t - 1] * rho[t] for t in present)
+            num += np.bincount(sh, weights=(tot.real * tot.real + tot.imag * tot.imag),
+                               minlength=nq)
+            if partials:
+                for ia in present:
+                    for ib in present:
+                        if ib < ia:
+                            continue
+                        v = rho[ia].real * rho[ib].real + rho[ia].imag * rho[ib].imag
+                        pn[ia - 1, ib - 1] += np.bincount(sh, weights=v, minlength=nq)
+    den = cnt.astype(np.float64) * mode_den
+    acc = Accumulators(num, den, cnt, pn if partials else None, None, None, len(frames), natoms,
+                       counts)
+    return modes, acc

@@ -15,7 +15,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libsqnufft.so")
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 OK, WARN_EPS_TOO_SMALL = 0, 1
 WEIGHT_UNIT, WEIGHT_NEUTRON, WEIGHT_XRAY = 0, 1, 2
 NORM_MEAN, NORM_SELF, NORM_NATOM = 1, 2, 3
@@ -23,10 +23,7 @@ PREC_DOUBLE, PREC_SINGLE = 0, 1
 HOST, DEVICE = 0, 1
 FLAG_TIMING = 1
 FLAG_GRAD = 2
-FLAG_FUSED_FFT = 4
 FLAG_CUFFT = 8
-FLAG_PIPELINE = 16
-FLAG_SPREAD_TC = 32
 FLAG_FFT_RING = 64
 
 # Every symbol include/sqnufft.h declares.
@@ -98,8 +95,6 @@ class SqnInfo(ctypes.Structure):
         ("nspecies", ctypes.c_int32),
         ("device_bytes", ctypes.c_int64),
         ("tile", ctypes.c_int64 * 3),
-        ("fused_fft", ctypes.c_int32),
-        ("pipelined", ctypes.c_int32),
         ("natoms", ctypes.c_int64),
         ("xrd_bins", ctypes.c_int32),
         ("pruned_fft512", ctypes.c_int32),
@@ -219,14 +214,13 @@ class Plan:
                  xray_coef=None, qmin=0.0, qmax=20.0, nq=500, norm=NORM_MEAN, partials=True,
                  want_grid=False, precision=PREC_DOUBLE, eps=1e-9, upsampfac=0.0,
                  kernel_width=0, device=0, max_grid_modes=0, timing=False, stream=None,
-                 grad=False, fused_fft=None, xrd=None, pipeline=False, spread_tc=False,
-                 fft_ring=False):
+                 grad=False, cufft=False, xrd=None, fft_ring=False):
         L = load()
         self._L = L
         d = self._describe(cell, origin, type_id, ntypes, weight, amp_const, xray_coef, qmin,
                            qmax, nq, norm, partials, want_grid, precision, eps, upsampfac,
-                           kernel_width, device, max_grid_modes, timing, stream, grad, fused_fft,
-                           xrd, pipeline, spread_tc, fft_ring)
+                           kernel_width, device, max_grid_modes, timing, stream, grad, cufft,
+                           xrd, fft_ring)
         h = ctypes.c_void_p()
         self.status = check(L.sqn_plan_create(ctypes.byref(d), ctypes.byref(h)), "sqn_plan_create")
         self._attach(h, owned=True)
@@ -235,14 +229,11 @@ class Plan:
                   xray_coef=None, qmin=0.0, qmax=20.0, nq=500, norm=NORM_MEAN, partials=True,
                   want_grid=False, precision=PREC_DOUBLE, eps=1e-9, upsampfac=0.0,
                   kernel_width=0, device=0, max_grid_modes=0, timing=False, stream=None,
-                  grad=False, fused_fft=None, xrd=None, pipeline=False, spread_tc=False,
-                  fft_ring=False):
+                  grad=False, cufft=False, xrd=None, fft_ring=False):
         """Fill an SqnDesc; the arrays it points to are kept on self.  xrd: None, or a
         dict(lam=..., range=(min, max), step=0.0, lp=True) for the powder pattern.
-        pipeline: FFT and binning of frame f on a second stream beside the spread of
-        frame f + 1 (a second fine grid).  spread_tc: FP32 spread on the tensor cores
-        (tcgen05) instead of the CUDA cores.  fft_ring: FP32 column passes of the pruned
-        512-point FFT in the ring form (experimental)."""
+        cufft: cuFFT R2C instead of the pruned 512-point passes on 512^3 grids.
+        fft_ring: FP32 column passes of the pruned 512-point FFT in the ring form."""
         L = self._L
         self.type_id = np.ascontiguousarray(type_id, dtype=np.int32)
         self.natoms = int(self.type_id.size)
@@ -274,9 +265,7 @@ class Plan:
         d.want_grid = int(bool(want_grid))
         d.precision = int(precision)
         d.flags = ((FLAG_TIMING if timing else 0) | (FLAG_GRAD if grad else 0)
-                   | (0 if fused_fft is None else (FLAG_FUSED_FFT if fused_fft else FLAG_CUFFT))
-                   | (FLAG_PIPELINE if pipeline else 0)
-                   | (FLAG_SPREAD_TC if spread_tc else 0)
+                   | (FLAG_CUFFT if cufft else 0)
                    | (FLAG_FFT_RING if fft_ring else 0))
         d.eps = float(eps)
         d.upsampfac = float(upsampfac)

@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libsqnufft.so")
-SOURCES = ["sqn_api.cu", "sqn_kernels.cu", "sqn_fft.cu", "sqn_fft512.cu", "sqn_spread_tc.cu", "sqn_adjoint.cu", "sqn_type1.cu",
+SOURCES = ["sqn_api.cu", "sqn_kernels.cu", "sqn_fft512.cu", "sqn_adjoint.cu", "sqn_type1.cu",
            "sqn_noalloc.cu", "sqn_dump.cpp"]
 HEADERS = ["sqn_internal.h", "sqn_device.cuh", os.path.join("..", "..", "include", "sqnufft.h")]
 

@@ -262,16 +262,9 @@ struct sqn_plan_s {
   double *d_acc = nullptr, *d_gnum = nullptr, *d_den = nullptr, *d_cnt = nullptr;
   cufftHandle fft = 0;
   bool fft_ok = false;
-  // fused pruned FFT + binning (sqn_fft.cu); cuFFT + k_bin when off
-  bool fused = false;
   bool inplace = false;  // cuFFT R2C in place over padded real rows (dS/dr plans)
-  static bool fused_requested(int32_t flags) {
-    return (flags & SQN_FLAG_FUSED_FFT) && !(flags & SQN_FLAG_CUFFT);
-  }
   int64_t c1pitch = 0;  // complex row pitch of the half spectrum
   // pruned 512-point passes (every axis 512): compact half spectrum in d_G
-  bool spread_tc = false;  // FP32: the tensor-core spread (sqn_spread_tc.cu)
-  int tc_chunk = 0;
   int *d_err = nullptr;    // set by a kernel whose bounded wait gave up
   bool fft512 = false;
   bool fft_ring = false;  // FP32: column passes in the ring form (SQN_FLAG_FFT_RING)
@@ -281,7 +274,6 @@ struct sqn_plan_s {
   int *d_hkl = nullptr;
   double *d_rho = nullptr;
   int64_t modes_cap = 0;
-  FftPlan3 fp{};
   // adjoint (SQN_FLAG_GRAD)
   bool grad_ok = false;
   int32_t *d_orig = nullptr;
@@ -292,16 +284,6 @@ struct sqn_plan_s {
   int64_t gnum_half = 0;
   int64_t nsums = 0;           // shell + powder-pattern sums at the head of d_acc
   double *d_xcnt = nullptr;    // kept modes per two-theta bin
-
-  // Frame pipeline: frame f's FFT and binning run on fft_stream while frame
-  // f + 1 is sorted and spread on the plan's stream into the other fine grid.
-  bool overlap = false;
-  cudaStream_t fft_stream = nullptr;
-  void *d_grid2 = nullptr;
-  int gbuf = 0;
-  cudaEvent_t ev_spread[2] = {nullptr, nullptr}, ev_fftdone[2] = {nullptr, nullptr};
-  cudaEvent_t ev_join = nullptr;
-  bool aux_pending = false;  // work queued on fft_stream since the last join
 
   int64_t nframes = 0;
   int slot_next = 0;
@@ -341,7 +323,6 @@ void free_plan(sqn_plan *p) {
   cudaSetDevice(p->device);
   if (p->stream) cudaStreamSynchronize(p->stream);
   if (p->copy_stream) cudaStreamSynchronize(p->copy_stream);
-  if (p->fft_stream) cudaStreamSynchronize(p->fft_stream);
   if (p->fft_ok) cufftDestroy(p->fft);
   if (p->fft_fwd1_ok) cufftDestroy(p->fft_fwd1);
   if (p->fft_inv3_ok) cufftDestroy(p->fft_inv3);
@@ -352,13 +333,7 @@ void free_plan(sqn_plan *p) {
     if (p->ev_copied[i]) cudaEventDestroy(p->ev_copied[i]);
     if (p->ev_free[i]) cudaEventDestroy(p->ev_free[i]);
   }
-  for (int i = 0; i < 2; ++i) {
-    if (p->ev_spread[i]) cudaEventDestroy(p->ev_spread[i]);
-    if (p->ev_fftdone[i]) cudaEventDestroy(p->ev_fftdone[i]);
-  }
-  if (p->ev_join) cudaEventDestroy(p->ev_join);
   for (cudaEvent_t e : p->tev_pool) cudaEventDestroy(e);
-  if (p->fft_stream) cudaStreamDestroy(p->fft_stream);
   if (p->copy_stream) cudaStreamDestroy(p->copy_stream);
   if (p->own_stream && p->stream) cudaStreamDestroy(p->stream);
   cudaSetDevice(cur);
@@ -396,8 +371,6 @@ std::vector<int4> build_rows(const double *b, const int *hm, double qmax) {
 template <typename R> std::vector<R> to_r(const std::vector<double> &v) {
   return std::vector<R>(v.begin(), v.end());
 }
-
-int setup_fused_fft(sqn_plan *p);
 
 int setup_plan(sqn_plan *p, const sqn_plan_desc *d) {
   p->desc = *d;
@@ -526,8 +499,8 @@ int setup_plan(sqn_plan *p, const sqn_plan_desc *d) {
   // 2 (nf0/2 + 1), the half spectrum overwriting them): measured on B200 that
   // makes the gradient evaluation ~25 % faster, while the S(q) frame path is
   // fastest out of place (dense real rows: aligned spread stores; any row
-  // padding slows cuFFT).  The fused passes always need both buffers.
-  p->inplace = (d->flags & SQN_FLAG_GRAD) && !p->fused_requested(d->flags);
+  // padding slows cuFFT).
+  p->inplace = (d->flags & SQN_FLAG_GRAD) != 0;
   p->c1pitch = p->nf[0] / 2 + 1;
   g.pitch = p->inplace ? 2 * p->c1pitch : p->nf[0];
   g.vol_real = g.pitch * p->nf[1] * p->nf[2];
@@ -740,26 +713,10 @@ int setup_plan(sqn_plan *p, const sqn_plan_desc *d) {
     if (cufftSetStream(p->fft, s) != CUFFT_SUCCESS) return SQN_ERR_CUFFT;
   }
 
-  // --- fused pruned FFT + binning ------------------------------------------
-  const bool want_fused = sqn_plan_s::fused_requested(d->flags);
-  if (want_fused) {
-    const int st2 = setup_fused_fft(p);
-    if (st2 != SQN_OK) return st2;
-  }
-
-  // --- tensor-core spread (FP32, opt-in) -------------------------------------------
-  if (!p->fp64 && !p->fused && p->ntr >= 1 && p->ntr <= 4 && (d->flags & SQN_FLAG_SPREAD_TC)) {
-    if ((st = dalloc(p, &p->d_err, 1))) return st;
-    if (cudaMemset(p->d_err, 0, sizeof(int)) != cudaSuccess || spread_tc_set_attributes() != cudaSuccess)
-      return SQN_ERR_CUDA;
-    p->tc_chunk = spread_tc_chunk();
-    p->spread_tc = true;
-  }
-
   // --- pruned 512-point passes -------------------------------------------------
-  // cuFFT stays for plans that ask for it, dS/dr plans (in-place spectra),
-  // the fused path and other grid sizes.
-  if (!p->fused && !p->inplace && !(d->flags & SQN_FLAG_CUFFT) && p->nf[0] == 512 &&
+  // cuFFT stays for plans that ask for it, dS/dr plans (in-place spectra)
+  // and other grid sizes.
+  if (!p->inplace && !(d->flags & SQN_FLAG_CUFFT) && p->nf[0] == 512 &&
       p->nf[1] == 512 && p->nf[2] == 512) {
     std::vector<double> tw;
     fft512_twiddles(tw);
@@ -836,183 +793,16 @@ int setup_plan(sqn_plan *p, const sqn_plan_desc *d) {
     p->grad_ok = true;
   }
 
-  // --- frame pipeline: a second fine grid and the FFT stream -----------------
-  // Only when the second grid fits; otherwise the plan runs serially.
-  if (!p->fused && !p->inplace && !p->timing && (d->flags & SQN_FLAG_PIPELINE)) {
-    void *v = nullptr;
-    const size_t gbytes = (size_t)p->ntr * g.vol_real * rsz;
-    if (cudaMalloc(&v, gbytes) == cudaSuccess) {
-      p->allocs.push_back(v);
-      p->device_bytes += (int64_t)gbytes;
-      p->d_grid2 = v;
-      // the FFT stream at the higher priority: its blocks are dispatched as the
-      // spread's retire, and the spread fills the rest of the machine
-      int lo_pri = 0, hi_pri = 0;
-      cudaDeviceGetStreamPriorityRange(&lo_pri, &hi_pri);
-      if (cudaStreamCreateWithPriority(&p->fft_stream, cudaStreamNonBlocking, hi_pri) != cudaSuccess ||
-          cudaEventCreateWithFlags(&p->ev_join, cudaEventDisableTiming) != cudaSuccess)
-        return SQN_ERR_CUDA;
-      for (int i = 0; i < 2; ++i)
-        if (cudaEventCreateWithFlags(&p->ev_spread[i], cudaEventDisableTiming) != cudaSuccess ||
-            cudaEventCreateWithFlags(&p->ev_fftdone[i], cudaEventDisableTiming) != cudaSuccess)
-          return SQN_ERR_CUDA;
-      p->overlap = true;
-    } else {
-      cudaGetLastError();
-    }
-  }
   if (cudaStreamSynchronize(s) != cudaSuccess) return SQN_ERR_CUDA;
   return warn;
 }
 
-// Radix stages of an n-point FFT (8s first, then 4 or 2, 3s, 5s); false when
-// n has another prime factor or needs too many stages.
-bool fft_radices(int n, FftAxis &ax) {
-  ax.n = n;
-  ax.nst = 0;
-  int m = n;
-  auto push = [&ax](int r) {
-    if (ax.nst >= FFT_MAX_STAGES) return false;
-    ax.radix[ax.nst++] = r;
-    return true;
-  };
-  while (m % 8 == 0) {
-    if (!push(8)) return false;
-    m /= 8;
-  }
-  if (m % 4 == 0) {
-    if (!push(4)) return false;
-    m /= 4;
-  }
-  if (m % 2 == 0) {
-    if (!push(2)) return false;
-    m /= 2;
-  }
-  while (m % 3 == 0) {
-    if (!push(3)) return false;
-    m /= 3;
-  }
-  while (m % 5 == 0) {
-    if (!push(5)) return false;
-    m /= 5;
-  }
-  if (m != 1 || n < 2) return false;
-  int ns = 1;
-  for (int st = 0; st < ax.nst; ++st) {
-    ax.nr[st] = make_fastdiv((uint32_t)(n / ax.radix[st]));
-    ax.ns[st] = make_fastdiv((uint32_t)ns);
-    ns *= ax.radix[st];
-  }
-  ax.n_div = make_fastdiv((uint32_t)n);
-  return true;
-}
-
-// Decide whether the frame path runs the fused pruned passes (sqn_fft.cu) and
-// prepare them: radix plans, FP64-computed twiddle tables, shared-memory
-// limits.  Returns SQN_OK also when the plan keeps cuFFT + k_bin.
-int setup_fused_fft(sqn_plan *p) {
-  FftPlan3 &f = p->fp;
-  const BinGeom &b = p->bg;
-  if (p->ntr > MAX_FAST_T) return SQN_OK;
-  for (int d = 0; d < 3; ++d)
-    if (p->nf[d] > FFT_MAX_N || !fft_radices((int)p->nf[d], f.ax[d])) return SQN_OK;
-  f.H1 = p->hm[0] + 1;
-  f.M1 = 2 * p->hm[1] + 1;
-  f.M2 = 2 * p->hm[2] + 1;
-  f.H1_div = make_fastdiv((uint32_t)f.H1);
-  f.M2_div = make_fastdiv((uint32_t)f.M2);
-  const size_t rsz = p->fp64 ? 8 : 4;
-  // A2 (ntr x nf2 x M1 x H1 complex) reuses the real grids
-  if ((double)f.M1 * f.H1 * 2.0 > (double)p->nf[1] * p->nf[0]) return SQN_OK;
-  if (p->nf[1] % 2 != 0) return SQN_OK;
-  f.hist_smem = (size_t)hist_len(b) * sizeof(double) <= 48 * 1024;
-  int optin = 0;
-  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, p->device) !=
-      cudaSuccess)
-    return SQN_ERR_CUDA;
-  const size_t limit = (size_t)optin - 8 * 1024;  // static shared memory and slack
-  for (int pass = 0; pass < 3; ++pass)
-    if (fft_pass_smem(f, pass, p->fp64, p->ntr, hist_len(b)) > limit) return SQN_OK;
-  for (int d = 0; d < 3; ++d) {
-    const int n = f.ax[d].n;
-    std::vector<double> tw(2 * (size_t)n);
-    for (int k = 0; k < n; ++k) {
-      const double a = 2.0 * M_PI * (double)k / (double)n;
-      tw[2 * k] = std::cos(a);
-      tw[2 * k + 1] = -std::sin(a);
-    }
-    char *v = nullptr;
-    int st = dalloc(p, &v, 2 * (size_t)n * rsz);
-    if (st) return st;
-    cudaError_t e;
-    if (p->fp64) {
-      e = cudaMemcpy(v, tw.data(), tw.size() * 8, cudaMemcpyHostToDevice);
-    } else {
-      std::vector<float> tf = to_r<float>(tw);
-      e = cudaMemcpy(v, tf.data(), tf.size() * 4, cudaMemcpyHostToDevice);
-    }
-    if (e != cudaSuccess) return SQN_ERR_CUDA;
-    f.tw[d] = v;
-  }
-  // per h1, the rows h2 whose line along b3 comes within qmax of the origin
-  // (the distance of h1 b1 + h2 b2 from that line bounds |q| from below;
-  // the margin keeps the test conservative under rounding)
-  {
-    const double *rb = p->recip;
-    const double bb = rb[6] * rb[6] + rb[7] * rb[7] + rb[8] * rb[8];
-    const double q2 = p->desc.qmax * p->desc.qmax * (1.0 + 1e-9) + 1e-12;
-    std::vector<int2> span((size_t)f.H1);
-    for (int h1 = 0; h1 < f.H1; ++h1) {
-      int lo = f.M1, hi = -1;
-      for (int h2 = -p->hm[1]; h2 <= p->hm[1]; ++h2) {
-        double v[3];
-        for (int k = 0; k < 3; ++k) v[k] = h1 * rb[k] + h2 * rb[3 + k];
-        const double vv = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
-        const double vb = v[0] * rb[6] + v[1] * rb[7] + v[2] * rb[8];
-        if (vv - vb * vb / bb <= q2) {
-          lo = std::min(lo, h2 + p->hm[1]);
-          hi = std::max(hi, h2 + p->hm[1]);
-        }
-      }
-      span[(size_t)h1] = make_int2(lo, hi);
-    }
-    int2 *ds = nullptr;
-    int st = dalloc(p, &ds, span.size());
-    if (st) return st;
-    if (cudaMemcpy(ds, span.data(), span.size() * sizeof(int2), cudaMemcpyHostToDevice) !=
-        cudaSuccess)
-      return SQN_ERR_CUDA;
-    f.h2span = ds;
-  }
-  // persistent z-pass CTAs: as many as fit per SM by shared memory, at most 2
-  const size_t sm3 = fft_pass_smem(f, 2, p->fp64, p->ntr, hist_len(b));
-  int per = (int)((228 * 1024) / (sm3 + 1024));
-  per = std::max(1, std::min(2, per));
-  f.grid3 = p->nsm * per;
-  p->fused = true;
-  return SQN_OK;
-}
-
-// One frame through the weighted forward transform and, with gsh, its adjoint.
 // Kernels of ours that one frame launches.
-int frame_launches(const sqn_plan *p) { return p->fused ? 7 : (p->fft512 ? 8 : 5); }
+int frame_launches(const sqn_plan *p) { return p->fft512 ? 8 : 5; }
 
-// Order the work queued on the FFT stream before what comes next on the
-// plan's stream.
-int join_fft_stream(sqn_plan *p) {
-  if (!p->aux_pending) return SQN_OK;
-  if (cudaEventRecord(p->ev_join, p->fft_stream) != cudaSuccess ||
-      cudaStreamWaitEvent(p->stream, p->ev_join, 0) != cudaSuccess)
-    return SQN_ERR_CUDA;
-  p->aux_pending = false;
-  return SQN_OK;
-}
-
-// All queued work of the plan finished (both streams); a kernel that gave up
-// a bounded wait since the last check turns into an error here.
+// All queued work of the plan finished; a kernel that gave up a bounded wait
+// since the last check turns into an error here.
 int sync_plan(sqn_plan *p) {
-  const int st = join_fft_stream(p);
-  if (st != SQN_OK) return st;
   if (cudaStreamSynchronize(p->stream) != cudaSuccess) return SQN_ERR_CUDA;
   if (p->d_err) {
     int h = 0;
@@ -1125,68 +915,28 @@ template <typename R> int run_frame(sqn_plan *p, const double *dpos, int slot) {
   if (e != cudaSuccess) return SQN_ERR_CUDA;
   if (slot >= 0) cudaEventRecord(p->ev_free[slot], s);
   if (p->timing) cudaEventRecord(ev[1], s);
-  // With the pipeline, frames alternate between the two grids; a grid is
-  // spread again once the FFT of the frame before last has read it.
-  const int gb = p->overlap ? p->gbuf : 0;
-  void *grid = gb ? p->d_grid2 : p->d_grid;
-  if (p->overlap) {
-    p->gbuf ^= 1;
-    if (cudaStreamWaitEvent(s, p->ev_fftdone[gb], 0) != cudaSuccess) return SQN_ERR_CUDA;
-  }
-  if constexpr (sizeof(R) == 4) {
-    if (p->spread_tc) {
-      FrameGeom gt = g;
-      gt.chunk = p->tc_chunk;
-      e = launch_spread_tc((const float *)p->d_recs, p->d_starts, gt, (const float *)p->d_strength,
-                           (float *)grid, p->d_err, s);
-    }
-  }
-  if (!p->spread_tc)
-    e = launch_spread<R>((const R *)p->d_recs, p->d_starts, g, (const R *)p->d_strength,
-                         (R *)grid, s);
+  void *grid = p->d_grid;
+  e = launch_spread<R>((const R *)p->d_recs, p->d_starts, g, (const R *)p->d_strength, (R *)grid,
+                       s);
   if (e != cudaSuccess) return SQN_ERR_CUDA;
   if (p->timing) cudaEventRecord(ev[2], s);
-  if (p->fused) {
-    // x and y passes (the "FFT" stage), then the z pass with the binning
-    e = launch_fft_xy<R>(p->fp, p->d_grid, p->d_G, p->d_grid, p->bg, g.pitch, s);
+  if (p->fft512) {
+    // x pass into d_G, y pass back into the (consumed) grid, z pass into d_G
+    e = launch_fft512<R>((const R *)grid, p->d_G, grid, p->d_G, p->ntr, g.pitch, p->hm[0] + 1,
+                         p->hm[1], p->hm[2], p->d_tw512, p->nsm, s, p->fft_ring ? 1 : 0,
+                         p->d_err);
     if (e != cudaSuccess) return SQN_ERR_CUDA;
-    if (p->timing) cudaEventRecord(ev[3], s);
-    e = launch_fft_z_bin<R>(p->fp, p->d_grid, p->bg, (const R *)p->d_inv[0],
-                            (const R *)p->d_inv[1], (const R *)p->d_inv[2], p->d_amp,
-                            p->d_xcoef, p->d_acc, p->d_gnum, s);
-    if (e != cudaSuccess) return SQN_ERR_CUDA;
-    if (p->timing) cudaEventRecord(ev[4], s);
-    p->launches += 7;
-  } else {
-    cudaStream_t fs = s;
-    if (p->overlap) {
-      fs = p->fft_stream;
-      if (cudaEventRecord(p->ev_spread[gb], s) != cudaSuccess ||
-          cudaStreamWaitEvent(fs, p->ev_spread[gb], 0) != cudaSuccess)
-        return SQN_ERR_CUDA;
-    }
-    if (p->fft512) {
-      // x pass into d_G, y pass back into the (consumed) grid, z pass into d_G
-      e = launch_fft512<R>((const R *)grid, p->d_G, grid, p->d_G, p->ntr, g.pitch,
-                           p->hm[0] + 1, p->hm[1], p->hm[2], p->d_tw512, p->nsm, fs,
-                           p->fft_ring ? 1 : 0, p->d_err);
-      if (e != cudaSuccess) return SQN_ERR_CUDA;
-      p->launches += 3;
-    } else if (exec_forward(p, fs, grid, p->d_G) != CUFFT_SUCCESS) {
-      return SQN_ERR_CUFFT;
-    }
-    if (p->overlap) {
-      if (cudaEventRecord(p->ev_fftdone[gb], fs) != cudaSuccess) return SQN_ERR_CUDA;
-      p->aux_pending = true;
-    }
-    if (p->timing) cudaEventRecord(ev[3], s);
-    e = launch_bin<R>(p->d_rows, p->nrows, p->d_G, p->fft512 ? p->bg512 : p->bg,
-                      (const R *)p->d_inv[0], (const R *)p->d_inv[1], (const R *)p->d_inv[2],
-                      p->d_amp, p->d_xcoef, p->d_acc, p->d_gnum, p->nsm, fs);
-    if (e != cudaSuccess) return SQN_ERR_CUDA;
-    if (p->timing) cudaEventRecord(ev[4], s);
-    p->launches += 5;
+    p->launches += 3;
+  } else if (exec_forward(p, s, grid, p->d_G) != CUFFT_SUCCESS) {
+    return SQN_ERR_CUFFT;
   }
+  if (p->timing) cudaEventRecord(ev[3], s);
+  e = launch_bin<R>(p->d_rows, p->nrows, p->d_G, p->fft512 ? p->bg512 : p->bg,
+                    (const R *)p->d_inv[0], (const R *)p->d_inv[1], (const R *)p->d_inv[2],
+                    p->d_amp, p->d_xcoef, p->d_acc, p->d_gnum, p->nsm, s);
+  if (e != cudaSuccess) return SQN_ERR_CUDA;
+  if (p->timing) cudaEventRecord(ev[4], s);
+  p->launches += 5;
   p->nframes++;
   return SQN_OK;
 }
@@ -1306,8 +1056,6 @@ int sqn_plan_info_get(const sqn_plan *p, sqn_plan_info *info) {
   info->ntransforms = p->ntr;
   info->nspecies = p->nspecies;
   info->device_bytes = p->device_bytes;
-  info->fused_fft = p->fused ? 1 : 0;
-  info->pipelined = p->overlap ? 1 : 0;
   info->pruned_fft512 = p->fft512 ? (p->fft_ring ? 2 : 1) : 0;
   info->natoms = p->desc.natoms;
   info->xrd_bins = p->bg.xrd ? p->bg.xbins : 0;
@@ -1354,7 +1102,7 @@ int sqn_accumulate_frames(sqn_plan *p, const double *pos, int64_t nframes, int32
 int sqn_join(sqn_plan *p) {
   if (!p) return SQN_ERR_PLAN_NOTVALID;
   DeviceGuard guard(p->device);
-  return join_fft_stream(p);
+  return SQN_OK;  // every kernel of the plan runs on its one stream
 }
 
 int sqn_sync(sqn_plan *p) {
@@ -1368,7 +1116,7 @@ int sqn_peek_num_async(sqn_plan *p, double *num_host) {
   if (!num_host) return SQN_ERR_INVALID_ARGUMENT;
   DeviceGuard guard(p->device);
   // after the binning of the queued frames, on the stream that runs it
-  cudaStream_t s = p->aux_pending ? p->fft_stream : p->stream;
+  cudaStream_t s = p->stream;
   return cuda_status(cudaMemcpyAsync(num_host, p->d_acc, sizeof(double) * p->desc.nq,
                                      cudaMemcpyDeviceToHost, s));
 }
@@ -1497,7 +1245,7 @@ int sqn_density_modes(sqn_plan *p, const double *pos, int32_t where, const int32
   if (!pos || !hkl || !rho || nmodes < 1 || (where != SQN_HOST && where != SQN_DEVICE))
     return SQN_ERR_INVALID_ARGUMENT;
   // unit-strength transform per species, on the cuFFT spectrum
-  if (p->fused || p->ntr != p->nspecies || !(p->desc.partials || p->bg.xray))
+  if (p->ntr != p->nspecies || !(p->desc.partials || p->bg.xray))
     return SQN_ERR_NOT_SUPPORTED;
   DeviceGuard guard(p->device);
   cudaStream_t s = p->stream;
@@ -1628,7 +1376,6 @@ int sqn_sq_grad(sqn_plan *p, const double *pos, int32_t where, const double *dLd
   const int64_t N = p->desc.natoms;
   const int nq = p->desc.nq;
   const double *dpos = pos;
-  if (join_fft_stream(p) != SQN_OK) return SQN_ERR_CUDA;
   if (where == SQN_HOST) {
     // the copy stream may still be filling this slot for an earlier call
     if (cudaStreamSynchronize(p->copy_stream) != cudaSuccess ||
@@ -1773,7 +1520,6 @@ int sqn_batch_create(const sqn_plan_desc *descs, int32_t nsystems, void *stream,
     sqn_plan_desc d = descs[k];
     d.stream = nullptr;
     d.flags &= ~(uint32_t)SQN_FLAG_TIMING;
-    d.flags &= ~(uint32_t)SQN_FLAG_PIPELINE;  // one stream per system inside the graph
     sqn_plan *p = nullptr;
     const int ps = sqn_plan_create(&d, &p);
     if (ps > SQN_WARN_EPS_TOO_SMALL) {

@@ -348,8 +348,11 @@ __global__ void __launch_bounds__(32 * COLS, sizeof(R) == 4 ? 2 : 1)
 // buffer, issues the copies of the tile three steps on into it.  The loads of
 // the next tiles thus overlap the transforms and stores of the current ones,
 // which the barrier-phased kernel above cannot do.  Needs H1 even (16-byte
-// aligned rows and copy sizes).  Every wait is bounded; a give-up is recorded
-// in *err and ends that group's loop (the group leaves together).
+// aligned rows and copy sizes).  Every wait is bounded by elapsed time (the
+// globaltimer): a give-up is recorded in *err and in a shared abort word that
+// every wait of the CTA polls, so both groups leave at once; before the CTA
+// ends it waits (again with a deadline) until each buffer's last bulk copy has
+// landed.
 // ---------------------------------------------------------------------------
 constexpr int RING_NB = 3;
 constexpr int RING_LD = 18;  // buffer row pitch (complex): 144 bytes, rows 16-byte aligned
@@ -360,15 +363,24 @@ constexpr size_t RING_BUF = (size_t)512 * RING_LD;  // complex per buffer
 
 __host__ __device__ constexpr size_t ring_smem() {
   return sizeof(float2) * (TW_LEN + RING_NB * RING_BUF) + sizeof(uint64_t) * RING_NB +
-         sizeof(unsigned) * RING_NB;
+         sizeof(unsigned) * RING_NB + sizeof(int);
 }
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) {
   return (uint32_t)__cvta_generic_to_shared(p);
 }
-// Wait for phase `parity` of the barrier, at most ~2^22 polls.
-__device__ __forceinline__ bool ring_wait(uint32_t mbar, uint32_t parity) {
-  for (int i = 0; i < (1 << 22); ++i) {
+__device__ __forceinline__ uint64_t now_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+// Longest wait of one step (a tile normally lands within microseconds).
+constexpr uint64_t RING_WAIT_NS = 2000000000ull;
+// Wait for phase `parity` of the barrier until the deadline or, when abort is
+// given, until another group has raised it.
+__device__ __forceinline__ bool ring_wait(uint32_t mbar, uint32_t parity, uint64_t deadline,
+                                          const volatile int *abort) {
+  for (;;) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -378,8 +390,8 @@ __device__ __forceinline__ bool ring_wait(uint32_t mbar, uint32_t parity) {
         : "r"(mbar), "r"(parity)
         : "memory");
     if (ok) return true;
+    if ((abort && *abort) || now_ns() > deadline) return false;
   }
-  return false;
 }
 __device__ __forceinline__ void ring_expect_tx(uint32_t mbar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes)
@@ -484,6 +496,8 @@ __global__ void __launch_bounds__(RING_THREADS, 1)
   // of buffer b only once it has been issued, so that the buffer's barrier is
   // then in step k's phase or just past it and its parity wait is unambiguous
   volatile unsigned *issued = reinterpret_cast<volatile unsigned *>(full + RING_NB);
+  // raised by a group that gave up a wait: every other wait of the CTA ends too
+  volatile int *s_abort = reinterpret_cast<volatile int *>(issued + RING_NB);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nblk = (cp.ncols + COLS - 1) / COLS;
   const int M = 2 * cp.hm + 1;
@@ -496,6 +510,7 @@ __global__ void __launch_bounds__(RING_THREADS, 1)
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(full + b)) : "memory");
       issued[b] = (unsigned)b < nloc ? 1u : 0u;  // warp 0 issues them below
     }
+    *s_abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
@@ -513,17 +528,21 @@ __global__ void __launch_bounds__(RING_THREADS, 1)
   for (unsigned k = g; k < nloc; k += RING_GROUPS) {
     const unsigned st = blockIdx.x + k * gridDim.x;
     const int b = (int)(k % RING_NB);
+    const uint64_t deadline = now_ns() + RING_WAIT_NS;
     bool ok = true;
-    for (int it = 0; issued[b] < k / RING_NB + 1; ++it) {
-      if (it == (1 << 22)) {
+    while (issued[b] < k / RING_NB + 1) {
+      if (*s_abort || now_ns() > deadline) {
         ok = false;
         break;
       }
       __nanosleep(32);
     }
-    ok = ok && ring_wait(smem_addr(full + b), (k / RING_NB) & 1u);
+    ok = ok && ring_wait(smem_addr(full + b), (k / RING_NB) & 1u, deadline, s_abort);
     if (group_any(bar_id, !ok)) {
-      if (gt == 0) atomicExch(err, 3);
+      if (gt == 0) {
+        *s_abort = 1;
+        atomicExch(err, 3);
+      }
       break;
     }
     const unsigned plane = st / (unsigned)nblk;
@@ -578,14 +597,18 @@ __global__ void __launch_bounds__(RING_THREADS, 1)
       }
     }
   }
-  // before the CTA ends, the copies issued into each buffer have landed (they
+  // Before the CTA ends, the copies issued into each buffer have landed (they
   // all have unless a group gave up a wait): a buffer's earlier tiles were
-  // consumed before its last one was issued, so only that one can be in flight
+  // waited for before its last one was issued, so only that one can be in
+  // flight.  Bulk copies from global memory complete on their own, so this
+  // wait ends long before its deadline; the abort word does not cut it short.
   __syncthreads();
   if (tid == 0) {
+    const uint64_t deadline = now_ns() + RING_WAIT_NS;
     for (int b = 0; b < RING_NB; ++b) {
       const unsigned n = issued[b];
-      if (n > 0 && !ring_wait(smem_addr(full + b), (n - 1) & 1u)) atomicExch(err, 3);
+      if (n > 0 && !ring_wait(smem_addr(full + b), (n - 1) & 1u, deadline, nullptr))
+        atomicExch(err, 3);
     }
   }
 }

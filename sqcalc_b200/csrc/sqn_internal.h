@@ -27,6 +27,23 @@ constexpr int MAX_W = 16;
 constexpr int MAX_BINS_DIM = 4;                // bins per dim a tile may need (w <= 16)
 constexpr int MAX_NB = 64;                     // neighbour bins of a tile
 constexpr int MAX_FAST_T = 8;                  // species held in registers
+// Shape facts k_spread hard-codes (lane -> cell map, patch masks, 8-wide z rows):
+// four 8 x 4 patches across x (warp & 3, lane & 7, lane >> 3), the y patches'
+// mask bits above bit 3, 16-byte aligned staged rows.  A bin is one tile, so a
+// tile's start cells X0 - (w - 1) .. X0 + T - 1 touch at most ceil((w - 1) / T) + 1
+// bins per dimension; the bin lists hold MAX_BINS_DIM per dimension and would
+// silently drop the rest.
+static_assert(TILE_X / PATCH_X == 4 && PATCH_X == 8 && PATCH_Y == 4,
+              "k_spread maps warp & 3 / lane & 7 / lane >> 3 onto the patches");
+static_assert(4 + TILE_Y / PATCH_Y <= 32, "patch mask bits");
+static_assert(TILE_Z == 8, "load_zrow and the packed z FMAs take 8 z cells");
+static_assert((TILE_X + TILE_Y) % 4 == 0 && SPREAD_ROW % 4 == 0,
+              "staged rows and their z part are 16-byte aligned");
+static_assert((MAX_W - 2) / TILE_X + 2 <= MAX_BINS_DIM &&
+                  (MAX_W - 2) / TILE_Y + 2 <= MAX_BINS_DIM &&
+                  (MAX_W - 2) / TILE_Z + 2 <= MAX_BINS_DIM,
+              "a tile's bin list per dimension fits MAX_BINS_DIM for every w <= MAX_W");
+static_assert(MAX_BINS_DIM * MAX_BINS_DIM * MAX_BINS_DIM <= MAX_NB, "neighbour bins");
 
 // Point records written by the bin sort and read by the spread and
 // interpolation kernels: four R-sized slots per atom,
@@ -111,51 +128,6 @@ size_t spread_smem_bytes(int chunk, bool fp64);
 int spread_chunk(bool fp64, int ntr);
 cudaError_t spread_set_attributes();
 
-// Pruned three-pass FFT fused with the binning (sqn_fft.cu).
-constexpr int FFT_MAX_STAGES = 16;
-constexpr int FFT_MAX_N = 4096;   // longest axis the fused passes take
-constexpr int FFT_Z_THREADS = 512;
-// Exact x / d for x * d < 2^32 by one multiply-high: m = ceil(2^32 / d), d > 1
-// (Granlund and Montgomery, PLDI 1994); d == 1 is passed through.
-struct FastDiv {
-  uint32_t d, m;
-};
-inline FastDiv make_fastdiv(uint32_t d) {
-  FastDiv f;
-  f.d = d;
-  f.m = d > 1 ? (uint32_t)((((uint64_t)1 << 32) + d - 1) / d) : 0u;
-  return f;
-}
-struct FftAxis {
-  int n;                          // transform length (2, 3, 5-smooth)
-  int nst;                        // radix stages
-  int radix[FFT_MAX_STAGES];      // 8, 4, 2, 3 or 5 each
-  FastDiv nr[FFT_MAX_STAGES];     // n / radix of each stage
-  FastDiv ns[FFT_MAX_STAGES];     // product of the earlier radices
-  FastDiv n_div;                  // n
-};
-struct FftPlan3 {
-  FftAxis ax[3];
-  const void *tw[3];              // exp(-2 pi i k / n_d), k < n_d, complex R
-  int H1;                         // hm0 + 1 kept x modes (h1 >= 0)
-  int M1, M2;                     // 2 hm1 + 1, 2 hm2 + 1
-  FastDiv H1_div, M2_div;
-  const int2 *h2span;             // per h1: [lo, hi] of h2 + hm1 whose line along b3
-                                  // reaches |q| <= qmax (lo > hi: none)
-  int grid3;                      // persistent CTAs of the z pass
-  bool hist_smem;                 // shell histograms in shared memory
-};
-int fft_columns_per_cta(bool fp64);
-int fft_z_columns_per_cta(bool fp64);
-size_t fft_pass_smem(const FftPlan3 &f, int pass, bool fp64, int ntr, int nhist);
-template <typename R>
-cudaError_t launch_fft_xy(const FftPlan3 &f, const void *grid, void *A1, void *A2,
-                          const BinGeom &b, int64_t pitch, cudaStream_t s);
-template <typename R>
-cudaError_t launch_fft_z_bin(const FftPlan3 &f, const void *A2, const BinGeom &b, const R *inv1,
-                             const R *inv2, const R *inv3, const double *amp,
-                             const double *xcoef, double *acc, double *gnum, cudaStream_t s);
-
 // Host math (sqn_api.cu).
 namespace hostmath {
 int64_t next235even(int64_t n);
@@ -178,14 +150,6 @@ template <typename R>
 cudaError_t launch_fft512(const R *grid, void *A1, void *A2, void *G, int ntr, int64_t pitch,
                           int H1, int hm1, int hm2, const void *tw, int nsm, cudaStream_t s,
                           int ring, int *err);
-
-// Gather spreading on the tensor cores (sqn_spread_tc.cu, FP32, 1..4
-// transforms); *err is set when an MMA barrier wait gives up.
-int spread_tc_chunk();
-size_t spread_tc_smem(int chunk);
-cudaError_t spread_tc_set_attributes();
-cudaError_t launch_spread_tc(const float *recs, const int *starts, const FrameGeom &g,
-                             const float *strength, float *grid, int *err, cudaStream_t s);
 
 // Density amplitudes of requested lattice points from the half spectra.
 template <typename R>

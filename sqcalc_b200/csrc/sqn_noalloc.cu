@@ -3,13 +3,14 @@
 //
 // Who needs it: code that runs where cudaMalloc is not an option -- a host
 // framework that owns all device memory through its own pool and forbids
-// side allocations (XLA / PyTorch custom operators), a caller in the middle of
-// recording a CUDA graph (allocation calls are illegal inside a global-mode
-// stream capture), or a long-running service that must not grow its footprint
-// per request.  Such a caller brings its own positions and output grids; the
-// scratch this stage needs (bin counts, bin starts, per-atom keys and slots,
-// sorted point records, species and strengths) lives in one file-scope
-// __device__ array of fixed size instead of being allocated.
+// side allocations (custom operators of ML frameworks, plugins inside a host
+// application that has already reserved the device memory), or a
+// long-running service that must keep a fixed footprint and cannot risk an
+// allocation failing in the middle of a request.  Such a caller brings its
+// own positions and output grids; the scratch this stage needs (bin counts,
+// bin starts, per-atom keys and slots, sorted point records, species and
+// strengths) lives in one file-scope __device__ array of fixed size instead of
+// being allocated.
 //
 // Contract (see include/sqnufft.h):
 //   * The array is SQN_NOALLOC_SCRATCH_BYTES (32 MiB) per GPU.  Every GPU that
@@ -22,7 +23,10 @@
 //     overlaps on the GPU (different streams, or different host threads on the
 //     same device) race on the array and must be serialised by the caller.
 //   * Requests whose scratch would not fit are rejected with
-//     SQN_ERR_SCRATCH_LIMIT before anything is launched.
+//     SQN_ERR_SCRATCH_LIMIT, and more than MAX_FAST_T (8) grids with
+//     SQN_ERR_INVALID_ARGUMENT, before anything is queued.
+//   * species and strength are host arrays: the call checks every species
+//     index on the host and copies both with cudaMemcpyAsync on `stream`.
 //   * No cudaMalloc, cudaFree or allocating library routine is called.
 #include <cuda_runtime.h>
 
@@ -81,7 +85,7 @@ extern "C" int sqn_spread_frame_noalloc(const double *pos, int64_t natoms,
   if (!pos || !species || !strength || !cell || !origin || !nf || !grid)
     return SQN_ERR_INVALID_ARGUMENT;
   if (natoms < 1 || natoms > (int64_t)INT32_MAX / 2) return SQN_ERR_NUM_NU_PTS_INVALID;
-  if (ntr < 1 || ntr > 255) return SQN_ERR_INVALID_ARGUMENT;
+  if (ntr < 1 || ntr > MAX_FAST_T) return SQN_ERR_INVALID_ARGUMENT;
   const int w = kernel_width;
   if (w < 2 || w > MAX_W || !(beta > 0.0)) return SQN_ERR_INVALID_ARGUMENT;
   for (int d = 0; d < 3; ++d)

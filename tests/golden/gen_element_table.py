@@ -4,10 +4,12 @@
 The scattering data (IT92 / Cromer-Mann x-ray coefficients and bound coherent
 neutron lengths) are physical constants that must be identical to the ones the
 reference uses, so they are taken from thatstar/sqcalc's generated module
-src/sqc_element_data.f90 rather than retyped.  Run once, in a checkout that has
-the reference next to it:
+src/sqc_element_data.f90 rather than retyped.  Run from the repository root,
+given the reference's element module:
 
-    python sqcalc_b200/data/gen_element_table.py /path/to/sqcalc/src/sqc_element_data.f90
+    python tests/golden/gen_element_table.py /path/to/sqcalc/src/sqc_element_data.f90
+
+It writes sqcalc_b200/data/elements.json.
 """
 import json
 import os
@@ -35,7 +37,9 @@ def parse(path):
 
 
 def main():
-    src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src/sqc_element_data.f90"
+    if len(sys.argv) != 2:
+        sys.exit("usage: gen_element_table.py <sqcalc>/src/sqc_element_data.f90")
+    src = sys.argv[1]
     a = parse(src)
     ns = len(a["species_label"])
     xa = a["species_xray_a"]
@@ -52,7 +56,8 @@ def main():
                          for i in range(ns)],
         "species_alias": dict(zip(a["species_alias_from"], a["species_alias_to"])),
     }
-    out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "elements.json")
+    root = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    out = os.path.join(root, "sqcalc_b200", "data", "elements.json")
     with open(out, "w") as fh:
         json.dump(table, fh, separators=(",", ":"))
     print("wrote", out, "species", ns, "elements", len(a["element_symbol"]))

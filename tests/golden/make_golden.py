@@ -7,7 +7,7 @@ sections 1, 2, 2b, 5, 9b), and the S(q) tables by the reference's own numpy
 direct sum (test/ref_sq.py).  Both scripts run here unchanged; this file only
 drives them.  Run from the repository root with the reference checked out:
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <path of the sqcalc checkout>
 
 It rewrites tests/golden/*.dump, *.dat and cases.json.
 """
@@ -41,7 +41,9 @@ CASES = [
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <path of the sqcalc checkout>")
+    ref = sys.argv[1]
     gen = os.path.join(ref, "test", "gen_dump.py")
     refsq = os.path.join(ref, "test", "ref_sq.py")
     for name, kw in DUMPS.items():

@@ -1,6 +1,6 @@
 """Pruned 512-point FFT passes (k_fft512_x, k_fft512_cols) on 512^3 fine grids:
 S(q), the partials and the per-mode grid against the same plan on cuFFT R2C
-(SQN_FLAG_CUFFT), FP32 and FP64, serial and pipelined."""
+(SQN_FLAG_CUFFT), FP32 and FP64."""
 import numpy as np
 import pytest
 
@@ -23,18 +23,18 @@ def plan(tid, precision, eps, cufft, **kw):
     return _lib.Plan(np.eye(3).reshape(9) * L, np.zeros(3), tid, ntypes=3,
                      weight=_lib.WEIGHT_NEUTRON, amp_const=np.array([4.149, 5.803, 9.45]),
                      qmin=0.0, qmax=QMAX, nq=300, partials=True, precision=precision, eps=eps,
-                     fused_fft=False if cufft else None, **kw)
+                     cufft=cufft, **kw)
 
 
-@pytest.mark.parametrize("precision,eps,tol,serial,grid", [
-    (_lib.PREC_SINGLE, 1e-6, 2e-6, False, False),
-    (_lib.PREC_SINGLE, 1e-6, 2e-6, True, True),
-    (_lib.PREC_DOUBLE, 1e-6, 1e-12, False, False),
+@pytest.mark.parametrize("precision,eps,tol,grid", [
+    (_lib.PREC_SINGLE, 1e-6, 2e-6, False),
+    (_lib.PREC_SINGLE, 1e-6, 2e-6, True),
+    (_lib.PREC_DOUBLE, 1e-6, 1e-12, False),
 ])
-def test_pruned_passes_match_cufft(precision, eps, tol, serial, grid):
+def test_pruned_passes_match_cufft(precision, eps, tol, grid):
     tid, fr = frames()
-    with plan(tid, precision, eps, False, pipeline=not serial, want_grid=grid) as pp, \
-            plan(tid, precision, eps, True, pipeline=not serial, want_grid=grid) as pc:
+    with plan(tid, precision, eps, False, want_grid=grid) as pp, \
+            plan(tid, precision, eps, True, want_grid=grid) as pc:
         assert list(pp.info.nf) == [512, 512, 512]
         assert pp.info.pruned_fft512 == 1 and pc.info.pruned_fft512 == 0
         for p in (pp, pc):
@@ -64,7 +64,7 @@ def test_pruned_passes_xray_weights_and_powder_pattern():
         return _lib.Plan(np.eye(3).reshape(9) * L, np.zeros(3), tid, ntypes=3,
                          weight=_lib.WEIGHT_XRAY, xray_coef=coef, qmin=0.0, qmax=QMAX, nq=200,
                          partials=True, precision=_lib.PREC_SINGLE, eps=1e-6,
-                         fused_fft=False if cufft else None, xrd=xrd)
+                         cufft=cufft, xrd=xrd)
     with mk(False) as pp, mk(True) as pc:
         assert pp.info.pruned_fft512 == 1 and pc.info.pruned_fft512 == 0
         for p in (pp, pc):
@@ -77,3 +77,44 @@ def test_pruned_passes_xray_weights_and_powder_pattern():
         np.testing.assert_array_equal(xa[3], xb[3])
         for x, y in ((xa[1], xb[1]), (xa[2], xb[2])):
             assert np.max(np.abs(x - y)) / max(1.0, float(np.max(np.abs(y)))) < 2e-6
+
+
+def test_default_512_path_against_direct_sum():
+    """The benchmark's frame path itself -- L = 220 A, q_max 6 (423^3 modes), a
+    512^3 fine grid, the pruned passes -- against the FP64 direct sum of the
+    reference's --method direct (oracle.direct_sq_separable, pinned to
+    oracle.direct_sq by tests/test_oracle.py) on a few hundred atoms: FP64
+    within 1e-7 relative (shells and partials; the reference's own NUFFT-vs-direct
+    bar is 1e-6, test/test_sqcalc.py:389-396), FP32 within max |dS| 1e-5."""
+    from oracle import oracle as O
+
+    rng = np.random.default_rng(11)
+    box, n = 220.0, 500
+    tid = rng.choice(np.array([1, 2, 3], dtype=np.int32), n, p=[0.5, 0.3, 0.2])
+    base = rng.random((n, 3)) * box
+    fr = [base + rng.normal(0, 0.3, (n, 3)) for _ in range(2)]
+    b = np.array([4.149, 5.803, 9.45])
+    w = O.Weights(kind=O.WEIGHT_NEUTRON, amp_const=b)
+    modes, acc = O.direct_sq_separable(fr, tid, np.eye(3) * box, np.zeros(3), w, 0.0, 6.0, 500)
+    assert list(modes) == [423, 423, 423]
+    ref = acc.shell_value()
+    refp = [acc.partial_value(a, c) for a in (1, 2, 3) for c in (1, 2, 3) if c >= a]
+    for prec, eps in ((_lib.PREC_DOUBLE, 1e-9), (_lib.PREC_SINGLE, 1e-6)):
+        with _lib.Plan(np.eye(3).reshape(9) * box, np.zeros(3), tid, ntypes=3,
+                       weight=_lib.WEIGHT_NEUTRON, amp_const=b, qmin=0.0, qmax=6.0, nq=500,
+                       partials=True, precision=prec, eps=eps) as p:
+            assert list(p.info.nf) == [512, 512, 512] and p.info.pruned_fft512 == 1
+            for f in fr:
+                p.accumulate(f)
+            counts = p.accumulators()["shell_count"]
+            S, Sp, _, nfr = p.finalize()
+        assert nfr == 2
+        np.testing.assert_array_equal(counts, acc.shell_count)
+        got = [Sp[a - 1, c - 1] for a in (1, 2, 3) for c in (1, 2, 3) if c >= a]
+        dS = float(np.max(np.abs(S - ref)))
+        rel = dS / max(1.0, float(np.max(np.abs(ref))))
+        dP = max(float(np.max(np.abs(x - y))) for x, y in zip(got, refp))
+        if prec == _lib.PREC_DOUBLE:
+            assert rel < 1e-7 and dP < 1e-7, (rel, dP)
+        else:
+            assert dS < 1e-5 and dP < 1e-5, (dS, dP)

@@ -1,9 +1,10 @@
 """sqn_spread_frame_noalloc: the allocation-free spread entry point.
 
 It serves callers that cannot call cudaMalloc (a framework that owns every
-device byte through its own pool, a caller recording a CUDA graph, a service
-that must not grow per request): they pass device positions and device output
-grids, and the sort scratch comes from a fixed static device array.
+device byte through its own pool, a plugin inside an application that has
+already reserved the device memory, a service that must keep a fixed
+footprint): they pass device positions and device output grids, and the sort
+scratch comes from a fixed static device array.
 
 The check: two calls in a row through the C ABI; each call's grids are carried
 through the rest of the pipeline on the test side (FFT, the oracle's
