@@ -426,6 +426,7 @@ def grad_leg(W, K, stream, dist, local_rank):
                                   "uniform, loss over q in [0.5,8], S_target from a copy "
                                   "displaced by N(0,0.2^2)", "nq": GRAD_NQ}}
     k = min(K, 20)
+    grads = {}
     for name, prec, eps in (("f32+f64acc", _lib.PREC_SINGLE, 1e-6), ("f64", _lib.PREC_DOUBLE, 1e-10)):
         with _lib.Plan(np.eye(3).reshape(9) * GRAD_BOX, np.zeros(3), types, qmin=GRAD_QMIN,
                        qmax=GRAD_QMAX, nq=GRAD_NQ, partials=False, precision=prec, eps=eps,
@@ -440,15 +441,24 @@ def grad_leg(W, K, stream, dist, local_rank):
             ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             ev0.record(stream)
             for _ in range(k):
-                p.sq_grad(d, dLdS)
+                _, g = p.sq_grad(d, dLdS)
             ev1.record(stream)
             torch.cuda.synchronize()
             t = _max_over_ranks(ev0.elapsed_time(ev1) * 1e-3, dist, local_rank)
+            grads[name] = g.cpu().numpy()
             out[name] = {"value": k / t, "ms_per_eval": 1e3 * t / k, "eps": eps, "steps": k,
                          "modes": list(p.modes), "fine_grid": list(p.info.nf),
                          "kernel_width": p.info.kernel_width,
                          "gpu_launches_per_eval": (p.launch_count() - l0) / k}
-    out["value"] = out["f32+f64acc"]["value"]
+    # The headline is the FP64 adjoint: within 1e-6 relative of the FP64
+    # direct-sum gradient (tests/test_gpu_grad.py measures ~1e-13).  The FP32
+    # form is reported beside it with its measured deviation from FP64 on the
+    # same positions and dL/dS (max |g32 - g64| / max |g64|).
+    g64 = grads["f64"]
+    out["f32+f64acc"]["max_rel_dev_vs_f64"] = float(
+        np.max(np.abs(grads["f32+f64acc"] - g64)) / np.max(np.abs(g64)))
+    out["value"] = out["f64"]["value"]
+    out["value_form"] = "f64 (eps 1e-10), the form that meets 1e-6 of the FP64 direct-sum gradient"
     return out
 
 

@@ -9,7 +9,7 @@ from sqcalc_b200 import _lib
 pytestmark = pytest.mark.gpu
 
 L, N = 100.0, 60000
-QMAX = 211.4 * 2 * np.pi / L  # 423 modes per axis: a 512^3 fine grid at sigma ~1.21
+QMAX = 211.4 * 2 * np.pi / L  # 425 modes per axis: a 512^3 fine grid at sigma ~1.2
 
 
 def frames(nframes=3, seed=8):
@@ -19,10 +19,10 @@ def frames(nframes=3, seed=8):
     return tid, [base + rng.normal(0, 0.3, (N, 3)) for _ in range(nframes)]
 
 
-def plan(tid, precision, eps, cufft, **kw):
+def plan(tid, precision, eps, cufft, qmax=QMAX, **kw):
     return _lib.Plan(np.eye(3).reshape(9) * L, np.zeros(3), tid, ntypes=3,
                      weight=_lib.WEIGHT_NEUTRON, amp_const=np.array([4.149, 5.803, 9.45]),
-                     qmin=0.0, qmax=QMAX, nq=300, partials=True, precision=precision, eps=eps,
+                     qmin=0.0, qmax=qmax, nq=300, partials=True, precision=precision, eps=eps,
                      cufft=cufft, **kw)
 
 
@@ -118,3 +118,24 @@ def test_default_512_path_against_direct_sum():
             assert rel < 1e-7 and dP < 1e-7, (rel, dP)
         else:
             assert dS < 1e-5 and dP < 1e-5, (dS, dP)
+
+
+def test_ring_form_matches_default_passes():
+    """The FP32 column passes in the ring form (SQN_FLAG_FFT_RING: bulk-copy tile
+    ring, two compute groups, time-bounded mbarrier waits) against the default
+    barrier-phased passes on the same frames; sqn_sync must report no wait that
+    gave up.  q_max gives 423 modes per axis (H1 = 212 kept h1 >= 0, even, as the
+    ring's 16-byte bulk copies need)."""
+    tid, fr = frames(2)
+    qmax = 210.5 * 2 * np.pi / L
+    with plan(tid, _lib.PREC_SINGLE, 1e-6, False, fft_ring=True, qmax=qmax) as pr, \
+            plan(tid, _lib.PREC_SINGLE, 1e-6, False, qmax=qmax) as pd:
+        assert list(pr.modes) == [423, 423, 423]
+        assert pr.info.pruned_fft512 == 2 and pd.info.pruned_fft512 == 1
+        for p in (pr, pd):
+            for f in fr:
+                p.accumulate(f)
+        pr.sync()
+        a, b = pr.finalize(), pd.finalize()
+        for x, y in ((a[0], b[0]), (a[1], b[1])):
+            assert np.max(np.abs(x - y)) / max(1.0, float(np.max(np.abs(y)))) < 1e-6

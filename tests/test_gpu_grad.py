@@ -63,13 +63,16 @@ def test_grad_vs_direct_sum_fp64(weight):
 
 
 def test_grad_fp32_vs_direct_sum():
+    """FP32 spread / FFT / interpolation (eps 1e-6) with FP64 accumulation: within
+    1e-5 relative of the FP64 direct-sum gradient (measured ~4.5e-6: FP32 does
+    not meet the 1e-6 bar, the FP64 adjoint above does)."""
     pos, types, cell = system(n=1500, seed=5)
     with make_plan(types, 30.0, precision=_lib.PREC_SINGLE, eps=1e-6) as plan:
         dLdS = np.random.default_rng(9).standard_normal(plan.nq)
         _, g = plan.sq_grad(pos, dLdS)
         ref = reference_grad(pos, types, cell, plan, dLdS, np.ones(len(types)))
     err = np.max(np.abs(g - ref)) / np.max(np.abs(ref))
-    assert err < 2e-4, err
+    assert err < 1e-5, err
 
 
 def test_grad_vs_central_differences():
