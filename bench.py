@@ -240,8 +240,9 @@ def _max_over_ranks(x, dist, local_rank):
 
 
 def precision_leg(types, dev, base, fbytes, W, K, stream, dist, world, local_rank):
-    """The plain FP64 path (same tolerance) on the same device-resident frames,
-    and max |dS| of the FP32 path against FP64 at eps 1e-12 on two frames."""
+    """The plain FP64 path on the same device-resident frames, at the benchmark's
+    eps 1e-6 and at sqcalc's default eps 1e-9 (src/sqc_options.f90:87), and max
+    |dS| of the FP32 path against FP64 at eps 1e-12 on two frames."""
     import torch
     from sqcalc_b200 import _lib
 
@@ -251,27 +252,31 @@ def precision_leg(types, dev, base, fbytes, W, K, stream, dist, world, local_ran
                          qmax=QMAX, nq=NQ, norm=_lib.NORM_MEAN, partials=True, precision=prec,
                          eps=eps, device=local_rank, stream=stream.cuda_stream)
 
-    k = min(K, 10)
-    p = plan(_lib.PREC_DOUBLE, EPS)
-    for f in range(W):
-        p.accumulate((base + f * fbytes, 1), where=_lib.DEVICE)
-    p.sync()
-    if dist:
-        import torch.distributed as td
-        td.barrier()
-    torch.cuda.synchronize()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    for f in range(W, W + k):
-        p.accumulate((base + f * fbytes, 1), where=_lib.DEVICE)
-    p.join()
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    t = _max_over_ranks(ev0.elapsed_time(ev1) * 1e-3, dist, local_rank)
-    fp64 = {"value": k * world / t, "unit": UNIT, "steps": k, "ms_per_step": 1e3 * t / k,
-            "eps": EPS, "upsampfac": p.info.upsampfac, "kernel_width": p.info.kernel_width,
-            "fine_grid": list(p.info.nf)}
-    p.close()
+    def timed(eps):
+        k = min(K, 10)
+        p = plan(_lib.PREC_DOUBLE, eps)
+        for f in range(W):
+            p.accumulate((base + f * fbytes, 1), where=_lib.DEVICE)
+        p.sync()
+        if dist:
+            import torch.distributed as td
+            td.barrier()
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for f in range(W, W + k):
+            p.accumulate((base + f * fbytes, 1), where=_lib.DEVICE)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        t = _max_over_ranks(ev0.elapsed_time(ev1) * 1e-3, dist, local_rank)
+        out = {"value": k * world / t, "unit": UNIT, "steps": k, "ms_per_step": 1e3 * t / k,
+               "eps": eps, "upsampfac": p.info.upsampfac, "kernel_width": p.info.kernel_width,
+               "fine_grid": list(p.info.nf)}
+        p.close()
+        return out
+
+    fp64 = timed(EPS)
+    fp64["sqcalc_default_eps"] = timed(1e-9)
     res = {}
     for name, prec, eps in (("fp32", _lib.PREC_SINGLE, EPS), ("fp64_ref", _lib.PREC_DOUBLE, 1e-12)):
         q = plan(prec, eps)
@@ -284,6 +289,83 @@ def precision_leg(types, dev, base, fbytes, W, K, stream, dist, world, local_ran
     fp64["max_abs_dS_partials_fp32"] = float(np.max(np.abs(res["fp32"][1] - res["fp64_ref"][1])))
     fp64["dS_reference"] = "FP64 NUFFT at eps 1e-12 on the same 2 frames"
     return fp64
+
+
+def reference_gpu_baseline(types, dev, W, K, stream, local_rank):
+    """The reference's own GPU kernel on this GPU: cuFINUFFT built from the
+    reference's vendored sources (external/finufft/src/cuda) for sm_100a by
+    oracle/cufinufft.mk, called with sqcalc's options (src/sqc_gpu.f90:185-204:
+    default opts, modeord 0, type 1, iflag +1, one transform per species) on the
+    benchmark's frames: coordinates 2 pi s - pi of the wrapped fractional
+    positions (:230-236) and one-hot species strengths, already on the device.
+    Timed per frame: setpts + execute, the device part of the reference's frame
+    (it then downloads the 3 x 423^3 mode cube and bins on the host).  FP32 at
+    eps 1e-6 and FP64 at sqcalc's default eps 1e-9.  Beside each: this
+    library's cuFINUFFT-shaped type-1 entry points (sqn_type1_*) on the same
+    points and strengths, transform for transform."""
+    import torch
+    from oracle import cufinufft_ref as REF
+    from sqcalc_b200 import _lib
+    if not REF.available():
+        return {"unavailable": "oracle/_ref/libcufinufft.so was not built"}
+    modes = (423, 423, 423)
+    species = sorted(set(int(t) for t in np.unique(types)))
+    T = len(species)
+    k = min(K, 5)
+    nfr = min(dev.shape[0], 4)
+    out = {"note": "device-only setpts + execute per frame, CUDA events on the launching "
+                   "stream; sqcalc's options (type 1, iflag +1, modeord 0, ntransf 3, default "
+                   "method); the same points and strengths for sqn_type1",
+           "modes": list(modes), "ntransf": T, "steps": k}
+    for fp64, eps in ((False, 1e-6), (True, 1e-9)):
+        rdt = torch.float64 if fp64 else torch.float32
+        cdt = torch.complex128 if fp64 else torch.complex64
+        tid = torch.from_numpy(types.astype(np.int64)).cuda()
+        c = torch.zeros((T, N_ATOMS), dtype=cdt, device="cuda")
+        for a, t in enumerate(species):
+            c[a][tid == t] = 1.0
+        xyz = []
+        for f in range(nfr):
+            sfrac = torch.remainder(dev[f] / BOX, 1.0)
+            xyz.append([(2 * np.pi * sfrac[:, d] - np.pi).to(rdt).contiguous() for d in range(3)])
+        fk = torch.empty((T, modes[2], modes[1], modes[0]), dtype=cdt, device="cuda")
+        torch.cuda.synchronize()
+        res = {}
+        with REF.Type1Plan(modes, T, eps, fp64, device=local_rank,
+                           stream=stream.cuda_stream) as rp:
+            def ref_frame(f):
+                x = xyz[f % nfr]
+                rp.setpts(N_ATOMS, x[0].data_ptr(), x[1].data_ptr(), x[2].data_ptr())
+                rp.execute(c.data_ptr(), fk.data_ptr())
+            res["cufinufft"] = _event_time(ref_frame, W, k, stream)
+        with _lib.Type1Plan(modes, iflag=1, ntransf=T, eps=eps,
+                            precision=_lib.PREC_DOUBLE if fp64 else _lib.PREC_SINGLE,
+                            device=local_rank, stream=stream.cuda_stream) as op:
+            def our_frame(f):
+                op.setpts(*xyz[f % nfr])
+                op.execute(c)
+            res["sqn_type1"] = _event_time(our_frame, W, k, stream)
+        del fk, c, xyz
+        torch.cuda.empty_cache()
+        name = "f64" if fp64 else "f32"
+        for key, ms in res.items():
+            out["%s_%s" % (key, name)] = {"frames_per_s": 1e3 / ms, "ms_per_frame": ms, "eps": eps}
+    return out
+
+
+def _event_time(step, W, k, stream):
+    """ms per step of step(f) over k steps after W warm-up steps (CUDA events)."""
+    import torch
+    for f in range(W):
+        step(f)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for f in range(W, W + k):
+        step(f)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    return ev0.elapsed_time(ev1) / k
 
 
 BATCH_SYSTEMS, BATCH_QMAX, BATCH_NQ, BATCH_FRAMES = 64, 8.0, 400, 20
@@ -570,6 +652,11 @@ def run_ours(args, rank, world, local_rank):
     # --- the plain FP64 path on the same frames, and max |dS| of FP32 ----------
     fp64 = precision_leg(types, dev, base, fbytes, W, K, stream, dist, world, local_rank)
 
+    # --- the reference's own cuFINUFFT on this GPU (baseline) --------------------
+    ref_gpu = None
+    if world == 1 and not args.no_reference_gpu:
+        ref_gpu = reference_gpu_baseline(types, dev, W, K, stream, local_rank)
+
     # --- dS/dr evaluations (differentiation form) -------------------------------
     grad = None if args.no_grad else grad_leg(W, K, stream, dist, local_rank)
 
@@ -644,6 +731,14 @@ def run_ours(args, rank, world, local_rank):
                                  "three pruned 512-point FFT passes (512^3 grids; cuFFT "
                                  "kernels, not counted, otherwise) and bin",
             "fp64": fp64,
+            "reference_gpu_baseline": ref_gpu,
+            "fp32_over_fp64": {
+                "vs_own_fp64_eps1e-6": value / fp64["value"],
+                "vs_own_fp64_sqcalc_eps1e-9": value / fp64["sqcalc_default_eps"]["value"],
+                "vs_reference_cufinufft_fp64_eps1e-9": (
+                    value / ref_gpu["cufinufft_f64"]["frames_per_s"]
+                    if ref_gpu and "cufinufft_f64" in ref_gpu else None),
+                "target": 10.0},
             "grad": grad,
             "batched": batched,
             "ingest": ingest,
@@ -670,6 +765,8 @@ def main():
                     help="FP32 column FFT passes in the ring form (SQN_FLAG_FFT_RING)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-grad", action="store_true", help="skip the dS/dr leg")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip timing the reference's cuFINUFFT (oracle/_ref) on the GPU")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-systems leg")
     ap.add_argument("--no-ingest", action="store_true", help="skip the text-dump ingest leg")
     ap.add_argument("--scale", type=float, default=1.0,

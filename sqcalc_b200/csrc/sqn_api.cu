@@ -506,9 +506,9 @@ int setup_plan(sqn_plan *p, const sqn_plan_desc *d) {
   g.vol_real = g.pitch * p->nf[1] * p->nf[2];
   g.natoms = d->natoms;
   g.rec_stride = rec_stride(w, p->fp64);
-  g.chunk = spread_chunk(p->fp64, p->ntr);
+  g.chunk = spread_chunk(p->fp64);
   if ((int64_t)g.ntiles * p->ntr >= INT32_MAX) return SQN_ERR_NOT_SUPPORTED;
-  p->nkeys = g.ntiles;  // one bin per tile; records carry their species
+  p->nkeys = (int)spread_nkeys(g);  // one bin per (transform, tile)
 
   BinGeom &b = p->bg;
   std::memcpy(b.recip, p->recip, sizeof(b.recip));
@@ -828,7 +828,7 @@ template <typename R> int grad_frame(sqn_plan *p, const double *dpos, bool want_
   cudaStream_t s = p->stream;
   FrameGeom g = p->fg;
   g.ntr = 1;  // the total T(h) = sum_j c_j exp(i q.r_j): one weighted transform
-  g.chunk = spread_chunk(p->fp64, 1);
+  g.chunk = spread_chunk(p->fp64);
   BinGeom b = p->bg;
   b.ntr = 1;
   b.partials = 0;

@@ -10,40 +10,42 @@
 namespace sqn {
 
 // Spread tile in fine-grid cells (x fastest).  A CTA of 16 warps owns one
-// 32 x 16 x 8 tile; warp k owns the 8 x 4 (x, y) patch ((k % 4) * 8, (k / 4) * 4)
-// of it and each lane keeps the 8 z-cells of its (x, y) column in registers.
+// 32 x 16 x 16 tile of ONE transform (grid y index = transform); warp k owns
+// the 8 x 4 (x, y) patch ((k % 4) * 8, (k / 4) * 4) of it and each lane keeps
+// the 16 z-cells of its (x, y) column in registers.  The bin sort keys points
+// by (transform, tile), so a CTA reads only the bins of its own transform.
 constexpr int TILE_X = 32;
 constexpr int TILE_Y = 16;
-constexpr int TILE_Z = 8;
+constexpr int TILE_Z = 16;
 constexpr int PATCH_X = 8;
 constexpr int PATCH_Y = 4;
 constexpr int SPREAD_WARPS = (TILE_X / PATCH_X) * (TILE_Y / PATCH_Y);  // 16
 constexpr int SPREAD_THREADS = 32 * SPREAD_WARPS;                       // 512
-constexpr int SPREAD_ROW = TILE_X + TILE_Y + TILE_Z;                    // staged values per point
+// staged values per point: x row, y row, z row, 4 of padding (row pitch 68
+// values: consecutive rows start 4 banks apart)
+constexpr int SPREAD_ROW = TILE_X + TILE_Y + TILE_Z + 4;
 static_assert((TILE_X & (TILE_X - 1)) == 0 && (TILE_Y & (TILE_Y - 1)) == 0 &&
                   (TILE_Z & (TILE_Z - 1)) == 0,
               "tile extents are powers of two");
 constexpr int MAX_W = 16;
-constexpr int MAX_BINS_DIM = 4;                // bins per dim a tile may need (w <= 16)
-constexpr int MAX_NB = 64;                     // neighbour bins of a tile
-constexpr int MAX_FAST_T = 8;                  // species held in registers
-// Shape facts k_spread hard-codes (lane -> cell map, patch masks, 8-wide z rows):
-// four 8 x 4 patches across x (warp & 3, lane & 7, lane >> 3), the y patches'
-// mask bits above bit 3, 16-byte aligned staged rows.  A bin is one tile, so a
-// tile's start cells X0 - (w - 1) .. X0 + T - 1 touch at most ceil((w - 1) / T) + 1
-// bins per dimension; the bin lists hold MAX_BINS_DIM per dimension and would
-// silently drop the rest.
+// A bin is one tile, so a tile's start cells X0 - (w - 1) .. X0 + T - 1 (cyclic)
+// span fewer than 2T cells for w - 1 < T: its own bin, the one before and, when
+// the axis ends in a tile shorter than w - 1 that the range wraps across, the
+// one before that -- at most 3 bins per dimension.
+constexpr int MAX_BINS_DIM = 3;
+constexpr int MAX_NB = MAX_BINS_DIM * MAX_BINS_DIM * MAX_BINS_DIM;  // neighbour bins of a tile
+constexpr int MAX_FAST_T = 8;                  // species held in registers (k_bin)
+// Shape facts k_spread hard-codes (lane -> cell map, patch masks, 8-wide z
+// halves, 16-byte aligned staged rows).
 static_assert(TILE_X / PATCH_X == 4 && PATCH_X == 8 && PATCH_Y == 4,
               "k_spread maps warp & 3 / lane & 7 / lane >> 3 onto the patches");
-static_assert(4 + TILE_Y / PATCH_Y <= 32, "patch mask bits");
-static_assert(TILE_Z == 8, "load_zrow and the packed z FMAs take 8 z cells");
+static_assert(4 + TILE_Y / PATCH_Y <= 8, "patch mask bits 0-7, z-half bits 8-9");
+static_assert(TILE_Z == 16, "two 8-cell z halves per lane");
 static_assert((TILE_X + TILE_Y) % 4 == 0 && SPREAD_ROW % 4 == 0,
               "staged rows and their z part are 16-byte aligned");
-static_assert((MAX_W - 2) / TILE_X + 2 <= MAX_BINS_DIM &&
-                  (MAX_W - 2) / TILE_Y + 2 <= MAX_BINS_DIM &&
-                  (MAX_W - 2) / TILE_Z + 2 <= MAX_BINS_DIM,
+static_assert(MAX_W - 1 < TILE_X && MAX_W - 1 < TILE_Y && MAX_W - 1 < TILE_Z,
               "a tile's bin list per dimension fits MAX_BINS_DIM for every w <= MAX_W");
-static_assert(MAX_BINS_DIM * MAX_BINS_DIM * MAX_BINS_DIM <= MAX_NB, "neighbour bins");
+static_assert(MAX_NB <= 32, "one bin per lane in the bin-list prefix");
 
 // Point records written by the bin sort and read by the spread and
 // interpolation kernels: four R-sized slots per atom,
@@ -66,7 +68,7 @@ struct FrameGeom {
   int ntile[3];       // tiles per dim
   int w;              // ES kernel width
   double beta;        // ES shape
-  int ntr;            // fine grids per frame
+  int ntr;            // fine grids per frame (bins are keyed by transform when > 1)
   int ntiles;         // ntile[0]*ntile[1]*ntile[2]
   int rec_stride;     // R-sized slots per point record
   int chunk;          // points the spread stages in shared memory per pass
@@ -125,7 +127,7 @@ cudaError_t launch_norms(const int4 *rows, int nrows, const BinGeom &b, const do
                          const double *xcoef, const double *counts_t, double *den,
                          double *cnt, double *xcnt, int nsm, cudaStream_t s);
 size_t spread_smem_bytes(int chunk, bool fp64);
-int spread_chunk(bool fp64, int ntr);
+int spread_chunk(bool fp64);
 cudaError_t spread_set_attributes();
 
 // Host math (sqn_api.cu).
@@ -157,11 +159,16 @@ cudaError_t launch_gather_modes(const void *G, const BinGeom &b, const int *hkl,
                                 const R *inv1, const R *inv2, const R *inv3,
                                 const double *origin, double *rho, cudaStream_t s);
 
-// Spread with a weight per point instead of per species (one grid; the
-// weights are in bin-sorted record order).
+// Spread with a weight per point instead of per species (g.ntr == 1): grid k
+// of the ngrids takes the weights wsorted[k * natoms ..] (bin-sorted record
+// order) and is written at grid + k * vol_real.
 template <typename R>
 cudaError_t launch_spread_pw(const R *recs, const int *starts, const FrameGeom &g,
-                             const R *wsorted, R *grid, cudaStream_t s);
+                             const R *wsorted, R *grid, int ngrids, cudaStream_t s);
+// Bin keys of a frame geometry: one per (transform, tile).
+inline int64_t spread_nkeys(const FrameGeom &g) {
+  return (int64_t)g.ntiles * (g.ntr > 1 ? g.ntr : 1);
+}
 
 // Adjoint (sqn_adjoint.cu).
 struct Recip {

@@ -3,15 +3,15 @@
 // Per frame:
 //   k_prep     wrap each atom into the cell, find the first cell of its ES
 //              kernel support on the fine grid and its home tile; count the
-//              tile's bin                                        [HBM: positions]
+//              bin of (transform, tile)                          [HBM: positions]
 //   k_scan     exclusive scan of the bin counts (one CTA) and reset the counts
 //   k_scatter  write each atom's 16-byte record into its bin slot: packed start
 //              cell + species and its three offsets from the support centre
-//   k_spread   gather spreading: one CTA owns one 32 x 16 x 8 fine-grid tile
-//              for every transform, stages the ES kernel values of the points
-//              of the bins that can reach it, already shifted onto the tile's
-//              cells, in shared memory, and each warp accumulates its 8 x 4
-//              patch (8 z-cells per lane, per transform) in registers from the
+//   k_spread   gather spreading: one CTA owns one 32 x 16 x 16 fine-grid tile
+//              of one transform, stages the ES kernel values of the points of
+//              that transform's bins that can reach it, already shifted onto
+//              the tile's cells, in shared memory, and each warp accumulates
+//              its 8 x 4 patch (16 z-cells per lane) in registers from the
 //              points that reach the patch; every cell is written exactly
 //              once, so the grid needs no zeroing and no atomics
 //                                                              [HBM: grid write]
@@ -37,14 +37,17 @@ namespace {
 
 using namespace dev;
 
-__global__ void k_prep(const double *__restrict__ pos, FrameGeom g, int *__restrict__ counts,
-                       uint32_t *__restrict__ key, uint32_t *__restrict__ slot) {
+__global__ void k_prep(const double *__restrict__ pos, const uint8_t *__restrict__ species,
+                       FrameGeom g, int *__restrict__ counts, uint32_t *__restrict__ key,
+                       uint32_t *__restrict__ slot) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < g.natoms;
        i += (int64_t)gridDim.x * blockDim.x) {
     AtomCell c;
     atom_cell(pos, i, g, c);
     int l0, l1, l2;
-    const uint32_t k = home_key(c, g, l0, l1, l2);
+    // bins of transform t follow those of transform t - 1 (one transform per species)
+    const uint32_t k = home_key(c, g, l0, l1, l2) +
+                       (g.ntr > 1 ? (uint32_t)species[i] * (uint32_t)g.ntiles : 0u);
     key[i] = k;
     slot[i] = (uint32_t)atomicAdd(&counts[k], 1);
   }
@@ -135,16 +138,16 @@ __global__ void k_scatter(const double *__restrict__ pos, const uint8_t *__restr
   }
 }
 
-// The 8 z values of a staged row (16-byte aligned) with vector loads.
-__device__ __forceinline__ void load_zrow(const float *src, float (&z)[TILE_Z]) {
+// Eight z values of a staged row (16-byte aligned) with vector loads.
+__device__ __forceinline__ void load_z8(const float *src, float (&z)[8]) {
   const float4 a = reinterpret_cast<const float4 *>(src)[0];
   const float4 b = reinterpret_cast<const float4 *>(src)[1];
   z[0] = a.x; z[1] = a.y; z[2] = a.z; z[3] = a.w;
   z[4] = b.x; z[5] = b.y; z[6] = b.z; z[7] = b.w;
 }
-__device__ __forceinline__ void load_zrow(const double *src, double (&z)[TILE_Z]) {
+__device__ __forceinline__ void load_z8(const double *src, double (&z)[8]) {
 #pragma unroll
-  for (int k = 0; k < TILE_Z / 2; ++k) {
+  for (int k = 0; k < 4; ++k) {
     const double2 v = reinterpret_cast<const double2 *>(src)[k];
     z[2 * k] = v.x;
     z[2 * k + 1] = v.y;
@@ -168,32 +171,44 @@ __device__ __forceinline__ void fma2(double a, double z0, double z1, double &c0,
   c1 = fma(a, z1, c1);
 }
 
-// Does the cyclic support [r, r+w) (mod n) meet the cells [b, b+len)?
-__device__ __forceinline__ bool cyc_meet(int r, int w, int b, int len, int n) {
-  if (len <= 0) return false;
-  int d1 = b - r;
-  if (d1 < 0) d1 += n;
-  int d2 = r - b;
-  if (d2 < 0) d2 += n;
-  return d1 < w || d2 < len;
+// Bits lo .. hi of a mask (0 <= lo <= hi < 32).
+__device__ __forceinline__ unsigned bit_range(int lo, int hi) {
+  return (0xffffffffu >> (31 - hi)) & (0xffffffffu << lo);
+}
+// Which P-cell groups of the tile cells [0, len) the cyclic support
+// [r, r + w) (mod n, 0 <= r < n) reaches: bit k for cells [k P, k P + P).  The
+// support meets the tile in [r, min(r + w, n, len)) when r < len, and in its
+// wrapped part [0, min(r + w - n, len)) when r + w > n.
+template <int P>
+__device__ __forceinline__ unsigned group_mask(int r, int w, int len, int n) {
+  unsigned m = 0u;
+  if (r < len) m = bit_range(r / P, (min(min(r + w, n), len) - 1) / P);
+  const int e = min(r + w - n, len);
+  if (e > 0) m |= bit_range(0, (e - 1) / P);
+  return m;
 }
 
 // ---------------------------------------------------------------------------
-// Gather spreading, one CTA per 32 x 16 x 8 tile for all transforms.
-// NT > 0: exactly NT transforms; NT == 0: any ntr <= MAX_FAST_T.
-// Shared memory per staged point: its kernel values already shifted onto the
-// tile's cells (32 x, 16 y, 8 z with the strength folded in; zero where the
-// support does not reach), its three support offsets, (rx, ry, rz, species)
-// relative to the tile and the mask of the 8 x 4 patches it reaches.  A warp's visit
-// of a point is then two scalar loads, a multiply, two vector loads and eight
-// FMAs per lane.
+// Gather spreading, one CTA per (32 x 16 x 16 tile, transform).
+// The CTA lists the bins of its transform that can reach the tile (at most 3
+// per dimension), loads their point records, keeps the points whose support
+// meets the tile (compacted with one shared atomic per warp) and stages for
+// each its kernel values already shifted onto the tile's cells (32 x, 16 y,
+// 16 z with the strength folded in; zero where the support does not reach),
+// with a mask of the 8 x 4 patches and the two 8-cell z halves it reaches.  A
+// warp's visit of a point is then two scalar loads, a multiply, and per z half
+// that the point reaches two vector loads and four packed FMAs per lane.
+// Every cell of the tile is written exactly once: no zeroing, no atomics.
+// ptw != nullptr (one grid per y index, g.ntr == 1): the weight of a point is
+// ptw[y * natoms + record index] instead of strength[species].
 // ---------------------------------------------------------------------------
-template <typename R, int NT>
-__global__ void __launch_bounds__(SPREAD_THREADS, (sizeof(R) == 4 || NT == 1) ? 2 : 1)
+constexpr unsigned ZLO = 1u << 8, ZHI = 1u << 9;
+
+template <typename R>
+__global__ void __launch_bounds__(SPREAD_THREADS, sizeof(R) == 4 ? 2 : 1)
     k_spread(const R *__restrict__ recs, const int *__restrict__ starts, FrameGeom g,
              const R *__restrict__ strength, R *__restrict__ grid,
              const R *__restrict__ ptw = nullptr) {
-  constexpr int TM = NT > 0 ? NT : MAX_FAST_T;
   const int chunk = g.chunk;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R *s_rows = reinterpret_cast<R *>(smem_raw);                        // [chunk][SPREAD_ROW]
@@ -203,15 +218,14 @@ __global__ void __launch_bounds__(SPREAD_THREADS, (sizeof(R) == 4 || NT == 1) ? 
   __shared__ int s_bstart[MAX_NB];
   __shared__ int s_bpref[MAX_NB + 1];
   __shared__ int s_borg[MAX_NB][3];
-  __shared__ int s_wcount[MAX_FAST_T * SPREAD_WARPS];
   __shared__ int s_bl[3][MAX_BINS_DIM];
   __shared__ int s_nbl[3];
+  __shared__ int s_nkept;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int cx = (warp & 3) * PATCH_X + (lane & 7);   // this lane's x cell in the tile
   const int cy = (warp >> 2) * PATCH_Y + (lane >> 3);  // and its y cell
-  const int tile = blockIdx.x;
-  const int ntr = NT > 0 ? NT : g.ntr;
+  const int tile = blockIdx.x, tr = blockIdx.y;
   const int t0 = tile % g.ntile[0];
   const int t1 = (tile / g.ntile[0]) % g.ntile[1];
   const int t2 = tile / (g.ntile[0] * g.ntile[1]);
@@ -220,6 +234,10 @@ __global__ void __launch_bounds__(SPREAD_THREADS, (sizeof(R) == 4 || NT == 1) ? 
   const int ty = min(g.tile[1], g.nf[1] - Y0);
   const int tz = min(g.tile[2], g.nf[2] - Z0);
   const int w = g.w;
+  // bins of transform tr (keys tr * ntiles + tile) when the transforms are
+  // binned apart; per-point weights use one set of bins for every grid
+  const int key0 = ptw ? 0 : tr * g.ntiles;
+  if (ptw) ptw += (int64_t)tr * g.natoms;
 
   // Bins whose points can reach this tile, per dimension: a support starting
   // at cell c covers c .. c+w-1, so the start cells that matter are
@@ -247,122 +265,90 @@ __global__ void __launch_bounds__(SPREAD_THREADS, (sizeof(R) == 4 || NT == 1) ? 
   const int nb0 = s_nbl[0], nb1 = s_nbl[1];
   const int nb = nb0 * nb1 * s_nbl[2];
   if (warp == 0) {
-    // two bins per lane (nb <= MAX_NB = 64), inclusive prefix by shuffles
-    int cnt2[2];
-    int sum = 0;
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int b = 2 * lane + h;
-      cnt2[h] = 0;
-      if (b < nb) {
-        const int bx = s_bl[0][b % nb0], by = s_bl[1][(b / nb0) % nb1],
-                  bz = s_bl[2][b / (nb0 * nb1)];
-        const int key = (bz * g.ntile[1] + by) * g.ntile[0] + bx;
-        const int st = starts[key];
-        cnt2[h] = starts[key + 1] - st;
-        s_bstart[b] = st;
-        s_borg[b][0] = bx * g.tile[0];
-        s_borg[b][1] = by * g.tile[1];
-        s_borg[b][2] = bz * g.tile[2];
-      }
-      sum += cnt2[h];
+    // one bin per lane (nb <= MAX_NB <= 32), inclusive prefix by shuffles
+    int cnt = 0;
+    if (lane < nb) {
+      const int bx = s_bl[0][lane % nb0], by = s_bl[1][(lane / nb0) % nb1],
+                bz = s_bl[2][lane / (nb0 * nb1)];
+      const int key = key0 + (bz * g.ntile[1] + by) * g.ntile[0] + bx;
+      const int st = starts[key];
+      cnt = starts[key + 1] - st;
+      s_bstart[lane] = st;
+      s_borg[lane][0] = bx * g.tile[0];
+      s_borg[lane][1] = by * g.tile[1];
+      s_borg[lane][2] = bz * g.tile[2];
     }
-    int incl = sum;
+    int incl = cnt;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       const int t = __shfl_up_sync(FULL, incl, o);
       if (lane >= o) incl += t;
     }
-    const int excl = incl - sum;
-    if (2 * lane < nb + 1) s_bpref[2 * lane] = excl;
-    if (2 * lane + 1 < nb + 1) s_bpref[2 * lane + 1] = excl + cnt2[0];
-    if (lane == 31 && nb == MAX_NB) s_bpref[MAX_NB] = incl;
+    if (lane < nb) s_bpref[lane + 1] = incl;
+    if (lane == 0) s_bpref[0] = 0;
   }
   __syncthreads();
   const int total = s_bpref[nb];
 
-  R acc[TM][TILE_Z];
+  R acc[TILE_Z];
 #pragma unroll
-  for (int t = 0; t < TM; ++t)
-#pragma unroll
-    for (int z = 0; z < TILE_Z; ++z) acc[t][z] = R(0);
+  for (int z = 0; z < TILE_Z; ++z) acc[z] = R(0);
   const unsigned xbit = 1u << (warp & 3), ybit = 1u << (4 + (warp >> 2));
   const R halfw = R(0.5) * (R)w - R(0.5);
   const R c2 = R(4) / ((R)w * (R)w);
   const R beta = (R)g.beta;
 
   for (int base = 0; base < total; base += chunk) {
-    // 1. candidates that overlap the tile, compacted (order kept)
+    if (tid == 0) s_nkept = 0;
+    __syncthreads();  // the previous pass's visits have read the rows
+    // 1. candidates whose support meets the tile, compacted
     const int i = base + tid;
     bool keep = false;
     int4 meta = make_int4(0, 0, 0, 0);
+    unsigned mask = 0u;
     R rec[REC_SLOTS];
     if (tid < chunk && i < total) {
-      int b = 0;
-      while (i >= s_bpref[b + 1]) ++b;
-      const int ridx = s_bstart[b] + (i - s_bpref[b]);
+      // bin of candidate i: s_bpref[b] <= i < s_bpref[b + 1]
+      int lo = 0, hi = nb;
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (s_bpref[mid] <= i) lo = mid; else hi = mid;
+      }
+      const int ridx = s_bstart[lo] + (i - s_bpref[lo]);
       load_rec(recs + (int64_t)ridx * REC_SLOTS, rec);
       const uint32_t packed = unpack_rec<R>(rec[0]);
-      int rx = s_borg[b][0] + (int)(packed & 255u) - X0;
-      int ry = s_borg[b][1] + (int)((packed >> 8) & 255u) - Y0;
-      int rz = s_borg[b][2] + (int)((packed >> 16) & 255u) - Z0;
+      int rx = s_borg[lo][0] + (int)(packed & 255u) - X0;
+      int ry = s_borg[lo][1] + (int)((packed >> 8) & 255u) - Y0;
+      int rz = s_borg[lo][2] + (int)((packed >> 16) & 255u) - Z0;
       if (rx < 0) rx += g.nf[0];
       if (ry < 0) ry += g.nf[1];
       if (rz < 0) rz += g.nf[2];
       keep = (rx < tx || rx + w > g.nf[0]) && (ry < ty || ry + w > g.nf[1]) &&
              (rz < tz || rz + w > g.nf[2]);
-      // with per-point weights (one grid) the slot carries the record index
-      meta = make_int4(rx, ry, rz, ptw ? ridx : (int)(packed >> 24));
-    }
-    // Counting sort of the kept points by transform (order kept within one),
-    // so that each transform's points form one contiguous range.
-    const int my_t = ntr > 1 ? meta.w : 0;
-    unsigned my_bal = 0u;
-#pragma unroll
-    for (int t = 0; t < TM; ++t) {
-      if (t < ntr) {
-        const unsigned bt = __ballot_sync(FULL, keep && my_t == t);
-        if (lane == 0) s_wcount[t * SPREAD_WARPS + warp] = __popc(bt);
-        if (t == my_t) my_bal = bt;
+      if (keep) {
+        mask = group_mask<PATCH_X>(rx, w, tx, g.nf[0]) |
+               (group_mask<PATCH_Y>(ry, w, ty, g.nf[1]) << 4) |
+               (group_mask<8>(rz, w, tz, g.nf[2]) << 8);
+        // with per-point weights the slot carries the record index
+        meta = make_int4(rx, ry, rz, ptw ? ridx : (int)(packed >> 24));
       }
     }
-    __syncthreads();
-    int tstart[TM + 1];
-    tstart[0] = 0;
-#pragma unroll
-    for (int t = 0; t < TM; ++t) {
-      int tot = 0;
-      if (t < ntr)
-#pragma unroll
-        for (int k = 0; k < SPREAD_WARPS; ++k) tot += s_wcount[t * SPREAD_WARPS + k];
-      tstart[t + 1] = tstart[t] + tot;
-    }
-    const int npts = tstart[TM];
+    const unsigned bal = __ballot_sync(FULL, keep);
+    int wbase = 0;
+    if (lane == 0 && bal) wbase = atomicAdd(&s_nkept, __popc(bal));
+    wbase = __shfl_sync(FULL, wbase, 0);
     if (keep) {
-      int p = __popc(my_bal & ((1u << lane) - 1u));
-#pragma unroll
-      for (int t = 0; t < TM; ++t)
-        if (t == my_t) p += tstart[t];
-      for (int k = 0; k < warp; ++k) p += s_wcount[my_t * SPREAD_WARPS + k];
-      // the 8 x 4 patches of the tile this point reaches
-      unsigned mask = 0u;
-#pragma unroll
-      for (int k = 0; k < TILE_X / PATCH_X; ++k)
-        if (cyc_meet(meta.x, w, k * PATCH_X, min(PATCH_X, tx - k * PATCH_X), g.nf[0]))
-          mask |= 1u << k;
-#pragma unroll
-      for (int k = 0; k < TILE_Y / PATCH_Y; ++k)
-        if (cyc_meet(meta.y, w, k * PATCH_Y, min(PATCH_Y, ty - k * PATCH_Y), g.nf[1]))
-          mask |= 1u << (4 + k);
+      const int p = wbase + __popc(bal & ((1u << lane) - 1u));
       s_meta[p] = meta;
       s_mask[p] = mask;
       store_rec(s_off + (size_t)p * 4, R(0), rec[1], rec[2], rec[3]);
     }
     __syncthreads();
+    const int npts = s_nkept;
 
     // 2. kernel values shifted onto the tile's cells: row c of point p holds
-    //    phi at tile cell c (x: c < 32, y: next 16, z: last 8, times the
-    //    strength), zero outside the support or the grid.  One thread per
+    //    phi at tile cell c (x: c < 32, y: next 16, z: next 16, times the
+    //    weight), zero outside the support or the grid.  One thread per
     //    (point, axis) clears its row and writes the w support values that
     //    fall in the tile (the same thread, so no barrier between the two).
     for (int e = tid; e < 3 * npts; e += SPREAD_THREADS) {
@@ -381,52 +367,47 @@ __global__ void __launch_bounds__(SPREAD_THREADS, (sizeof(R) == 4 || NT == 1) ? 
       for (int k = 0; k < w; ++k) {
         int cell = rel + k;
         if (cell >= n) cell -= n;
-        const R v = es_at(k, off, halfw, c2, beta) * sc;
-        if (cell < lim) row[cell] = v;
+        if (cell < lim) row[cell] = es_at(k, off, halfw, c2, beta) * sc;
       }
     }
     __syncthreads();
 
-    // 3. each warp walks only the points that reach its patch, transform by
-    //    transform (static accumulator indices)
+    // 3. each warp walks only the points that reach its patch
+    for (int pb = 0; pb < npts; pb += 32) {
+      const int p = pb + lane;
+      unsigned m = 0u;
+      if (p < npts) m = s_mask[p];
+      unsigned am = __ballot_sync(FULL, (m & xbit) && (m & ybit));
+      while (am) {
+        const int src = __ffs(am) - 1;
+        am &= am - 1u;
+        const unsigned zm = __shfl_sync(FULL, m, src);
+        const R *row = s_rows + (size_t)(pb + src) * SPREAD_ROW;
+        const R a = row[cx] * row[TILE_X + cy];
+        const R *zr = row + TILE_X + TILE_Y;
+        if (zm & ZLO) {
+          R z[8];
+          load_z8(zr, z);
 #pragma unroll
-    for (int t = 0; t < TM; ++t) {
-      if (t >= ntr) break;
-      const int tend = tstart[t + 1];
-      for (int pb = tstart[t]; pb < tend; pb += 32) {
-        const int p = pb + lane;
-        bool act = false;
-        if (p < tend) {
-          const unsigned m = s_mask[p];
-          act = (m & xbit) && (m & ybit);
+          for (int k = 0; k < 8; k += 2) fma2(a, z[k], z[k + 1], acc[k], acc[k + 1]);
         }
-        unsigned am = __ballot_sync(FULL, act);
-        while (am) {
-          const int q = pb + __ffs(am) - 1;
-          am &= am - 1u;
-          const R *row = s_rows + q * SPREAD_ROW;
-          const R a = row[cx] * row[TILE_X + cy];
-          R zr[TILE_Z];
-          load_zrow(row + TILE_X + TILE_Y, zr);
+        if (zm & ZHI) {
+          R z[8];
+          load_z8(zr + 8, z);
 #pragma unroll
-          for (int z = 0; z < TILE_Z; z += 2) fma2(a, zr[z], zr[z + 1], acc[t][z], acc[t][z + 1]);
+          for (int k = 0; k < 8; k += 2) fma2(a, z[k], z[k + 1], acc[8 + k], acc[9 + k]);
         }
       }
     }
-    __syncthreads();
   }
 
   if (cx < tx && cy < ty) {
     const int64_t zs = (int64_t)g.nf[1] * g.pitch;
-    R *out = grid + ((int64_t)Z0 * g.nf[1] + (Y0 + cy)) * g.pitch + X0 + cx;
+    R *out = grid + (int64_t)tr * g.vol_real + ((int64_t)Z0 * g.nf[1] + (Y0 + cy)) * g.pitch +
+             X0 + cx;
 #pragma unroll
-    for (int t = 0; t < TM; ++t) {
-      if (t < ntr) {
-#pragma unroll
-        for (int z = 0; z < TILE_Z; ++z)
-          if (z < tz) out[(int64_t)t * g.vol_real + z * zs] = acc[t][z];
-      }
-    }
+    for (int z = 0; z < TILE_Z; ++z)
+      if (z < tz) out[z * zs] = acc[z];
   }
 }
 
@@ -632,8 +613,7 @@ static int grid_for(int64_t n, int threads) {
 template <typename R>
 cudaError_t launch_prep(const double *pos, const uint8_t *species, const FrameGeom &g,
                         int *counts, uint32_t *key, uint32_t *slot, cudaStream_t s) {
-  (void)species;
-  k_prep<<<grid_for(g.natoms, 256), 256, 0, s>>>(pos, g, counts, key, slot);
+  k_prep<<<grid_for(g.natoms, 256), 256, 0, s>>>(pos, species, g, counts, key, slot);
   return cudaGetLastError();
 }
 
@@ -660,10 +640,9 @@ size_t spread_smem_bytes(int chunk, bool fp64) {
   return (size_t)chunk * spread_point_bytes(fp64);
 }
 
-int spread_chunk(bool fp64, int ntr) {
-  // Two CTAs per SM (FP32, or one transform) share ~216 KB of shared memory;
-  // the FP64 multi-transform kernel runs one CTA per SM.
-  const size_t budget = (fp64 && ntr != 1) ? 216 * 1024 : 106 * 1024;
+int spread_chunk(bool fp64) {
+  // Two FP32 CTAs per SM share ~216 KB of shared memory; an FP64 CTA has it alone.
+  const size_t budget = fp64 ? 216 * 1024 : 106 * 1024;
   int c = (int)(budget / spread_point_bytes(fp64));
   c = c > SPREAD_THREADS ? SPREAD_THREADS : c;
   return c / 32 * 32;
@@ -679,49 +658,34 @@ template <typename K> static cudaError_t smem_optin(K kernel, int optin) {
                               optin - (int)fa.sharedSizeBytes);
 }
 
-template <typename R> static cudaError_t spread_attr(int optin) {
-  cudaError_t e = smem_optin(k_spread<R, 1>, optin);
-  if (e == cudaSuccess) e = smem_optin(k_spread<R, 2>, optin);
-  if (e == cudaSuccess) e = smem_optin(k_spread<R, 3>, optin);
-  if (e == cudaSuccess) e = smem_optin(k_spread<R, 4>, optin);
-  if (e == cudaSuccess) e = smem_optin(k_spread<R, 0>, optin);
-  return e;
-}
-
 cudaError_t spread_set_attributes() {
   int dev = 0, optin = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e == cudaSuccess)
     e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  if (e == cudaSuccess) e = spread_attr<float>(optin);
-  if (e == cudaSuccess) e = spread_attr<double>(optin);
+  if (e == cudaSuccess) e = smem_optin(k_spread<float>, optin);
+  if (e == cudaSuccess) e = smem_optin(k_spread<double>, optin);
   return e;
 }
 
+// One CTA per (tile, transform): grid (ntiles, ntr).
 template <typename R>
 cudaError_t launch_spread(const R *recs, const int *starts, const FrameGeom &g,
                           const R *strength, R *grid, cudaStream_t s) {
-  const dim3 grd((unsigned)g.ntiles);
+  if (g.ntr < 1 || g.ntr > MAX_FAST_T) return cudaErrorInvalidValue;
+  const dim3 grd((unsigned)g.ntiles, (unsigned)g.ntr);
   const size_t sm = spread_smem_bytes(g.chunk, sizeof(R) == 8);
-  switch (g.ntr) {
-    case 1: k_spread<R, 1><<<grd, SPREAD_THREADS, sm, s>>>(recs, starts, g, strength, grid); break;
-    case 2: k_spread<R, 2><<<grd, SPREAD_THREADS, sm, s>>>(recs, starts, g, strength, grid); break;
-    case 3: k_spread<R, 3><<<grd, SPREAD_THREADS, sm, s>>>(recs, starts, g, strength, grid); break;
-    case 4: k_spread<R, 4><<<grd, SPREAD_THREADS, sm, s>>>(recs, starts, g, strength, grid); break;
-    default:
-      if (g.ntr > MAX_FAST_T) return cudaErrorInvalidValue;
-      k_spread<R, 0><<<grd, SPREAD_THREADS, sm, s>>>(recs, starts, g, strength, grid);
-  }
+  k_spread<R><<<grd, SPREAD_THREADS, sm, s>>>(recs, starts, g, strength, grid);
   return cudaGetLastError();
 }
 
 template <typename R>
 cudaError_t launch_spread_pw(const R *recs, const int *starts, const FrameGeom &g,
-                             const R *wsorted, R *grid, cudaStream_t s) {
-  if (g.ntr != 1 || !wsorted) return cudaErrorInvalidValue;
+                             const R *wsorted, R *grid, int ngrids, cudaStream_t s) {
+  if (g.ntr != 1 || !wsorted || ngrids < 1 || ngrids > 65535) return cudaErrorInvalidValue;
   const size_t sm = spread_smem_bytes(g.chunk, sizeof(R) == 8);
-  k_spread<R, 1><<<(unsigned)g.ntiles, SPREAD_THREADS, sm, s>>>(recs, starts, g, nullptr, grid,
-                                                                wsorted);
+  const dim3 grd((unsigned)g.ntiles, (unsigned)ngrids);
+  k_spread<R><<<grd, SPREAD_THREADS, sm, s>>>(recs, starts, g, nullptr, grid, wsorted);
   return cudaGetLastError();
 }
 
@@ -807,9 +771,9 @@ template cudaError_t launch_spread<float>(const float *, const int *, const Fram
 template cudaError_t launch_spread<double>(const double *, const int *, const FrameGeom &,
                                            const double *, double *, cudaStream_t);
 template cudaError_t launch_spread_pw<float>(const float *, const int *, const FrameGeom &,
-                                             const float *, float *, cudaStream_t);
+                                             const float *, float *, int, cudaStream_t);
 template cudaError_t launch_spread_pw<double>(const double *, const int *, const FrameGeom &,
-                                              const double *, double *, cudaStream_t);
+                                              const double *, double *, int, cudaStream_t);
 template cudaError_t launch_bin<float>(const int4 *, int, const void *, const BinGeom &,
                                        const float *, const float *, const float *,
                                        const double *, const double *, double *, double *, int,

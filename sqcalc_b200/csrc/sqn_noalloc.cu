@@ -130,8 +130,8 @@ extern "C" int sqn_spread_frame_noalloc(const double *pos, int64_t natoms,
   g.vol_real = nf[0] * nf[1] * nf[2];
   g.natoms = natoms;
   g.rec_stride = rec_stride(w, false);
-  g.chunk = spread_chunk(false, ntr);
-  const int64_t nkeys = (int64_t)g.ntiles;  // one bin per tile
+  g.chunk = spread_chunk(false);
+  const int64_t nkeys = spread_nkeys(g);  // one bin per (grid, tile)
   if (nkeys >= INT32_MAX) return SQN_ERR_SCRATCH_LIMIT;
 
   // Scratch layout inside the static array, each section 256-byte aligned.

@@ -250,7 +250,7 @@ int make_type1(int type, int dim, const int64_t *n_modes, int iflag, int ntransf
   g.pitch = p->nf[0];
   g.vol_real = p->nf[0] * p->nf[1] * p->nf[2];
   g.rec_stride = REC_SLOTS;
-  g.chunk = spread_chunk(fp64, 1);
+  g.chunk = spread_chunk(fp64);
   g.natoms = 0;
   const size_t rsz = fp64 ? 8 : 4;
   const int ngrid = 2 * p->ntr;
@@ -346,9 +346,8 @@ template <typename R> int execute_type1(sqn_type1_plan *p, const R *c, R *fk) {
   R *grid = (R *)p->d_grid;
   k_sorted_weights<R><<<grid1d(M), 256, 0, s>>>(c, p->d_orig, M, p->ntr, w);
   cudaError_t e = cudaGetLastError();
-  for (int gi = 0; gi < 2 * p->ntr && e == cudaSuccess; ++gi)
-    e = launch_spread_pw<R>((const R *)p->d_recs, p->d_starts, p->g, w + (int64_t)gi * M,
-                            grid + (int64_t)gi * p->g.vol_real, s);
+  if (e == cudaSuccess)
+    e = launch_spread_pw<R>((const R *)p->d_recs, p->d_starts, p->g, w, grid, 2 * p->ntr, s);
   if (e != cudaSuccess) return SQN_ERR_CUDA;
   cufftResult fr = p->fp64 ? cufftExecD2Z(p->fft, (cufftDoubleReal *)p->d_grid,
                                           (cufftDoubleComplex *)p->d_G)
