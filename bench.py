@@ -368,6 +368,98 @@ def _event_time(step, W, k, stream):
     return ev0.elapsed_time(ev1) / k
 
 
+def small_fp64_leg(W, K, stream, local_rank):
+    """The CPU-runnable configuration (plain FP64 static S(q)): cubic L = 20 A,
+    N = 8000, 2 types 2667 / 5333, i.i.d. uniform frames, unit weights, norm
+    mean, partials, NUFFT tolerance 1e-9 (sqcalc's default), q_max 10 (65^3
+    modes), nq 500.  The plan in FP64 and in FP32 with FP64 accumulation, frames
+    device-resident; beside them the reference's cuFINUFFT (FP64, eps 1e-9) on
+    the same frames (setpts + execute only, see reference_gpu_baseline)."""
+    import torch
+    from sqcalc_b200 import _lib
+    rng = np.random.default_rng(SEED + 11)
+    n, box, nfr = 8000, 20.0, 10
+    types = np.repeat(np.array([1, 2], dtype=np.int32), [2667, n - 2667])
+    rng.shuffle(types)
+    frames = torch.from_numpy(rng.random((nfr, n, 3)) * box).cuda()
+    k = max(K, 20)
+    out = {"workload": "plain FP64 form: cubic L=20 A, N=8000, 2 types 2667/5333, uniform, "
+                       "unit weights, norm mean, partials, eps 1e-9, qmax 10 (65^3 modes), nq 500",
+           "steps": k}
+    for name, prec in (("f64", _lib.PREC_DOUBLE), ("f32+f64acc", _lib.PREC_SINGLE)):
+        with _lib.Plan(np.eye(3).reshape(9) * box, np.zeros(3), types, qmin=0.0, qmax=10.0,
+                       nq=500, norm=_lib.NORM_MEAN, partials=True, precision=prec, eps=1e-9,
+                       device=local_rank, stream=stream.cuda_stream) as p:
+            fb = n * 3 * 8
+            step = lambda f: p.accumulate((frames.data_ptr() + (f % nfr) * fb, 1),  # noqa: E731
+                                          where=_lib.DEVICE)
+            ms = _event_time(step, W, k, stream)
+            out[name] = {"frames_per_s": 1e3 / ms, "ms_per_frame": ms,
+                         "fine_grid": list(p.info.nf), "kernel_width": p.info.kernel_width,
+                         "eps_used": p.info.eps_used}
+    from oracle import cufinufft_ref as REF
+    if REF.available():
+        T = 2
+        c = torch.zeros((T, n), dtype=torch.complex128, device="cuda")
+        tid = torch.from_numpy(types.astype(np.int64)).cuda()
+        for a in range(T):
+            c[a][tid == a + 1] = 1.0
+        xyz = [[(2 * np.pi * torch.remainder(frames[f][:, d] / box, 1.0) - np.pi).contiguous()
+                for d in range(3)] for f in range(nfr)]
+        fk = torch.empty((T, 65, 65, 65), dtype=torch.complex128, device="cuda")
+        with REF.Type1Plan((65, 65, 65), T, 1e-9, True, device=local_rank,
+                           stream=stream.cuda_stream) as rp:
+            def ref_frame(f):
+                x = xyz[f % nfr]
+                rp.setpts(n, x[0].data_ptr(), x[1].data_ptr(), x[2].data_ptr())
+                rp.execute(c.data_ptr(), fk.data_ptr())
+            ms = _event_time(ref_frame, W, k, stream)
+        out["reference_cufinufft_f64_device_only"] = {"frames_per_s": 1e3 / ms, "ms_per_frame": ms}
+    return out
+
+
+def solid_leg(W, K, stream, local_rank):
+    """The structured-solid configuration: triclinic FCC crystal, a = 4 A,
+    64^3 cells (N = 1,048,576), tilts xy = 5, xz = 3, 2 types alternating on the
+    sublattices, Gaussian thermal displacement sigma 0.1 A, IT92 x-ray weights
+    (Cu / Au), q_max 10 (817^3 modes: above the reference's 4e8 mode cap, which
+    refuses this run), nq 500, FP32 spread / FFT with FP64 accumulation, eps
+    1e-6, partials.  Frames device-resident."""
+    import torch
+    from sqcalc_b200 import _lib
+    from sqcalc_b200.synthetic import fcc_solid
+    from sqcalc_b200.weights import WeightScheme
+    pos0, types, cell = fcc_solid(64)
+    rng = torch.Generator(device="cuda").manual_seed(SEED + 13)
+    base = torch.from_numpy(pos0).cuda()
+    nfr = 4
+    frames = torch.stack([base + 0.1 * torch.randn(base.shape, generator=rng, device="cuda",
+                                                   dtype=torch.float64) for _ in range(nfr)])
+    scheme = WeightScheme.from_options("xray", "1:Cu,2:Au")
+    k = min(K, 10)
+    with _lib.Plan(cell.reshape(9), np.zeros(3), types, ntypes=2, weight=_lib.WEIGHT_XRAY,
+                   xray_coef=scheme.xray_rows(2), qmin=0.0, qmax=10.0, nq=500,
+                   norm=_lib.NORM_MEAN, partials=True, precision=_lib.PREC_SINGLE, eps=1e-6,
+                   max_grid_modes=-1, device=local_rank, stream=stream.cuda_stream) as p:
+        fb = len(types) * 3 * 8
+        step = lambda f: p.accumulate((frames.data_ptr() + (f % nfr) * fb, 1),  # noqa: E731
+                                      where=_lib.DEVICE)
+        ms = _event_time(step, W, k, stream)
+        info = p.info
+        out = {"workload": "structured solid: triclinic FCC a=4 A, 64^3 cells (N=1048576), "
+                           "tilts xy=5 xz=3, 2 types on sublattices, thermal sigma 0.1 A, "
+                           "IT92 x-ray (Cu/Au), qmax 10 (817^3 modes), nq 500, FP32+FP64acc, "
+                           "eps 1e-6, partials",
+               "frames_per_s": 1e3 / ms, "ms_per_frame": ms, "steps": k,
+               "modes": list(info.modes), "fine_grid": list(info.nf),
+               "kernel_width": info.kernel_width,
+               "reference": "refuses this grid (817^3 modes above its 4e8 cap, "
+                            "src/sqc_structure_factor.f90:340-345)"}
+    del frames
+    torch.cuda.empty_cache()
+    return out
+
+
 BATCH_SYSTEMS, BATCH_QMAX, BATCH_NQ, BATCH_FRAMES = 64, 8.0, 400, 20
 
 
@@ -657,6 +749,12 @@ def run_ours(args, rank, world, local_rank):
     if world == 1 and not args.no_reference_gpu:
         ref_gpu = reference_gpu_baseline(types, dev, W, K, stream, local_rank)
 
+    # --- the CPU-runnable FP64 configuration and the structured solid ----------
+    small = solid = None
+    if world == 1 and not args.no_configs:
+        small = small_fp64_leg(W, K, stream, local_rank)
+        solid = solid_leg(W, K, stream, local_rank)
+
     # --- dS/dr evaluations (differentiation form) -------------------------------
     grad = None if args.no_grad else grad_leg(W, K, stream, dist, local_rank)
 
@@ -732,6 +830,8 @@ def run_ours(args, rank, world, local_rank):
                                  "kernels, not counted, otherwise) and bin",
             "fp64": fp64,
             "reference_gpu_baseline": ref_gpu,
+            "plain_fp64_config": small,
+            "solid_config": solid,
             "fp32_over_fp64": {
                 "vs_own_fp64_eps1e-6": value / fp64["value"],
                 "vs_own_fp64_sqcalc_eps1e-9": value / fp64["sqcalc_default_eps"]["value"],
@@ -765,6 +865,8 @@ def main():
                     help="FP32 column FFT passes in the ring form (SQN_FLAG_FFT_RING)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-grad", action="store_true", help="skip the dS/dr leg")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the plain-FP64 (L=20, N=8000) and structured-solid legs")
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip timing the reference's cuFINUFFT (oracle/_ref) on the GPU")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-systems leg")

@@ -75,6 +75,13 @@ enum {
                               column tiles into shared memory with bulk copies while two
                               groups of compute warps transform and store earlier tiles).
                               Off by default: experimental, not yet measured on B200 */
+  SQN_FLAG_AUTOTUNE = 128  /* choose the fine grid and kernel width by timing: the plan
+                              builds the candidate (sigma, w) pairs that reach eps (the
+                              smallest upsampling for each width up to the precision's
+                              cap), runs a few frames of uniform synthetic positions of
+                              its own shape through each, and keeps the fastest; results
+                              are cached per shape for the life of the process.  Ignored
+                              when upsampfac or kernel_width is given */
 };
 
 /* Everything sqcalc's configure + gpu_setup know after the first frame
@@ -138,6 +145,9 @@ typedef struct sqn_plan_info {
                                2: the same with the column passes in the ring form
                                (SQN_FLAG_FFT_RING) */
   double xrd_step;          /* their width, degrees */
+  int32_t autotuned;        /* 1: fine grid and width chosen by timing (SQN_FLAG_AUTOTUNE) */
+  int32_t tune_candidates;  /* (sigma, w) pairs timed (0 when the choice came from the cache) */
+  double tune_ms;           /* measured milliseconds per frame of the chosen pair */
 } sqn_plan_info;
 
 typedef struct sqn_plan_s sqn_plan;

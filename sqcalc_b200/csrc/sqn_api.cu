@@ -14,7 +14,11 @@
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <new>
+#include <random>
+#include <string>
 #include <vector>
 
 #include "../../include/sqnufft.h"
@@ -285,6 +289,10 @@ struct sqn_plan_s {
   int64_t nsums = 0;           // shell + powder-pattern sums at the head of d_acc
   double *d_xcnt = nullptr;    // kept modes per two-theta bin
 
+  // SQN_FLAG_AUTOTUNE: fine grid and width chosen by timing
+  int autotuned = 0, tune_candidates = 0;
+  double tune_ms = 0.0;
+
   int64_t nframes = 0;
   int slot_next = 0;
   cudaEvent_t ev_copied[2] = {nullptr, nullptr}, ev_free[2] = {nullptr, nullptr};
@@ -370,6 +378,121 @@ std::vector<int4> build_rows(const double *b, const int *hm, double qmax) {
 
 template <typename R> std::vector<R> to_r(const std::vector<double> &v) {
   return std::vector<R>(v.begin(), v.end());
+}
+
+// ---------------------------------------------------------------------------
+// Autotuner (SQN_FLAG_AUTOTUNE): candidate (sigma, w) pairs that reach eps --
+// for each kernel width up to the precision's cap the smallest 2,3,5-smooth
+// upsampling of the largest mode count that reaches it, plus the cost model's
+// own choice -- each timed on the plan's shape (same cell, atoms, types, q
+// range, precision and flags) over a few frames of uniform positions; the
+// fastest is kept and cached per shape for the life of the process.
+// ---------------------------------------------------------------------------
+struct TuneResult {
+  double sigma;  // 0: the cost model's grid
+  int w;
+  int ncand;
+  double ms;
+};
+std::mutex g_tune_mutex;
+std::map<std::string, TuneResult> g_tune_cache;
+
+std::string tune_key(const sqn_plan *p, const sqn_plan_desc *d, double eps) {
+  char buf[256];
+  std::snprintf(buf, sizeof(buf), "%d/%d/%d|%.17g|%d|%lld|%d|%d|%d|%d|%d|%.17g|%.17g|%d|%x",
+                p->modes[0], p->modes[1], p->modes[2], eps, (int)p->fp64,
+                (long long)d->natoms, p->ntr, d->partials, d->weight, d->want_grid, d->device,
+                d->qmin, d->qmax, d->nq, (unsigned)(d->flags & ~SQN_FLAG_AUTOTUNE));
+  return std::string(buf);
+}
+
+int autotune_grid(sqn_plan *p, const sqn_plan_desc *d, double eps, TuneResult *out) {
+  const std::string key = tune_key(p, d, eps);
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      *out = it->second;
+      out->ncand = 0;
+      return SQN_OK;
+    }
+  }
+  const int m = std::max(p->modes[0], std::max(p->modes[1], p->modes[2]));
+  const int wcap = p->fp64 ? MAX_W : 12;
+  std::vector<std::pair<double, int>> cand;
+  cand.push_back({0.0, 0});  // the cost model's choice
+  int last_w = 1 << 30;
+  for (int64_t n = next235even((int64_t)std::ceil(1.2 * m)); n <= (int64_t)(2.05 * m) + 2;
+       n = next235even(n + 2)) {
+    const double s = (double)n / m;
+    const int w = es_width(eps, s);
+    if (w > wcap || n < 2 * w || w >= last_w) continue;
+    cand.push_back({s, w});
+    last_w = w;
+  }
+  // uniform positions in the cell, one frame, device resident
+  const int64_t N = d->natoms;
+  std::vector<double> pos((size_t)N * 3);
+  std::mt19937_64 rng(12345);
+  std::uniform_real_distribution<double> U(0.0, 1.0);
+  for (int64_t i = 0; i < N; ++i) {
+    const double f0 = U(rng), f1 = U(rng), f2 = U(rng);
+    for (int r = 0; r < 3; ++r)
+      pos[3 * i + r] = d->origin[r] + f0 * d->cell[r] + f1 * d->cell[3 + r] + f2 * d->cell[6 + r];
+  }
+  double *dpos = nullptr;
+  if (cudaMalloc(&dpos, pos.size() * sizeof(double)) != cudaSuccess) {
+    cudaGetLastError();
+    return SQN_ERR_ALLOC;
+  }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  int st = cudaMemcpy(dpos, pos.data(), pos.size() * sizeof(double), cudaMemcpyHostToDevice) ==
+                   cudaSuccess
+               ? SQN_OK
+               : SQN_ERR_CUDA;
+  TuneResult best{0.0, 0, 0, 1e300};
+  constexpr int kFrames = 3;
+  for (size_t c = 0; c < cand.size() && st == SQN_OK; ++c) {
+    sqn_plan_desc sd = *d;
+    sd.flags &= ~(SQN_FLAG_AUTOTUNE | SQN_FLAG_TIMING);
+    sd.upsampfac = cand[c].first;
+    sd.kernel_width = cand[c].second;
+    sqn_plan *sp = nullptr;
+    if (sqn_plan_create(&sd, &sp) > SQN_WARN_EPS_TOO_SMALL || !sp) continue;  // e.g. no memory
+    int rc = sqn_accumulate_frames(sp, dpos, 1, SQN_DEVICE);
+    if (rc == SQN_OK) rc = sqn_sync(sp);
+    float ms = 0.f;
+    if (rc == SQN_OK && cudaEventRecord(e0, sp->stream) == cudaSuccess) {
+      for (int f = 0; f < kFrames && rc == SQN_OK; ++f)
+        rc = sqn_accumulate_frames(sp, dpos, 1, SQN_DEVICE);
+      if (rc == SQN_OK && (cudaEventRecord(e1, sp->stream) != cudaSuccess ||
+                           cudaEventSynchronize(e1) != cudaSuccess ||
+                           cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
+        rc = SQN_ERR_CUDA;
+    }
+    sqn_plan_destroy(sp);
+    if (rc != SQN_OK) {
+      st = rc;
+      break;
+    }
+    ms /= kFrames;
+    if (ms < best.ms) best = {cand[c].first, cand[c].second, 0, ms};
+    best.ncand = (int)c + 1;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(dpos);
+  if (st != SQN_OK) return st;
+  if (best.ms >= 1e300) return SQN_ERR_ALLOC;
+  best.ncand = (int)cand.size();
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    g_tune_cache[key] = best;
+  }
+  *out = best;
+  return SQN_OK;
 }
 
 int setup_plan(sqn_plan *p, const sqn_plan_desc *d) {
@@ -472,8 +595,21 @@ int setup_plan(sqn_plan *p, const sqn_plan_desc *d) {
   if (d->upsampfac != 0.0 && d->upsampfac <= 1.0) return SQN_ERR_UPSAMPFAC_TOO_SMALL;
   int w = 0;
   double sigma = 0.0;
-  if (!choose_fine_grid(p->modes, eps, d->upsampfac, d->kernel_width, p->fp64 ? MAX_W : 12,
-                        p->nf, &w, &sigma)) {
+  double sigma_req = d->upsampfac;
+  int w_req = d->kernel_width;
+  if ((d->flags & SQN_FLAG_AUTOTUNE) && sigma_req == 0.0 && w_req == 0) {
+    TuneResult tr{};
+    const int ts = autotune_grid(p, d, eps, &tr);
+    if (ts != SQN_OK) return ts;
+    sigma_req = tr.sigma;
+    w_req = tr.w;
+    p->autotuned = 1;
+    p->tune_candidates = tr.ncand;
+    p->tune_ms = tr.ms;
+    if (cudaSetDevice(p->device) != cudaSuccess) return SQN_ERR_CUDA;
+  }
+  if (!choose_fine_grid(p->modes, eps, sigma_req, w_req, p->fp64 ? MAX_W : 12, p->nf, &w,
+                        &sigma)) {
     w = MAX_W;
     warn = SQN_WARN_EPS_TOO_SMALL;
   }
@@ -1060,6 +1196,9 @@ int sqn_plan_info_get(const sqn_plan *p, sqn_plan_info *info) {
   info->natoms = p->desc.natoms;
   info->xrd_bins = p->bg.xrd ? p->bg.xbins : 0;
   info->xrd_step = p->bg.xrd ? p->bg.xstep : 0.0;
+  info->autotuned = p->autotuned;
+  info->tune_candidates = p->tune_candidates;
+  info->tune_ms = p->tune_ms;
   return SQN_OK;
 }
 
