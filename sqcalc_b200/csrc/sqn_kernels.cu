@@ -471,143 +471,6 @@ __global__ void __launch_bounds__(256, 2)
   }
 }
 
-// ---------------------------------------------------------------------------
-// The same pass with warp-private histograms (NT = 1..4 transforms, no powder
-// pattern, nquant * nq sums per warp in shared memory).  A warp owns its sums,
-// so its lanes add with plain shared loads and stores instead of FP64 shared
-// atomics: a warp whose kept modes all fall in one shell adds one warp sum;
-// otherwise lanes whose shells differ write in parallel, lanes sharing a shell
-// take turns (__match_any_sync picks the lowest lane of each shell per round,
-// at most BINW_ROUNDS rounds, shared atomics for what is left).  Each warp
-// loads the next 32 modes of its row before binning the current ones.  At the
-// end the CTA sums its warps' histograms and flushes them with one global
-// atomic per nonzero sum.
-// ---------------------------------------------------------------------------
-constexpr int BINW_WARPS = 4;
-constexpr int BINW_ROUNDS = 3;
-
-template <typename R, int NT, bool XR>
-__global__ void __launch_bounds__(32 * BINW_WARPS, 2)
-    k_bin_w(const int4 *__restrict__ rows, int nrows, const typename Cplx<R>::T *__restrict__ G,
-            BinGeom b, const R *__restrict__ inv1, const R *__restrict__ inv2,
-            const R *__restrict__ inv3, const double *__restrict__ amp,
-            const double *__restrict__ xcoef, double *__restrict__ acc,
-            double *__restrict__ gnum) {
-  using C = typename Cplx<R>::T;
-  constexpr int NPAIR = NT * (NT + 1) / 2;
-  extern __shared__ double s_hist[];  // [BINW_WARPS][nquant * nq]
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int nq = b.nq;
-  const int nhist = b.nquant * nq;
-  double *hist = s_hist + (size_t)warp * nhist;
-  for (int i = tid; i < BINW_WARPS * nhist; i += blockDim.x) s_hist[i] = 0.0;
-  __syncthreads();
-  double am[NT];
-#pragma unroll
-  for (int t = 0; t < NT; ++t) am[t] = XR ? 0.0 : amp[t];
-
-  for (int r = blockIdx.x * BINW_WARPS + warp; r < nrows; r += gridDim.x * BINW_WARPS) {
-    const int4 row = rows[r];
-    const int h2 = row.x, h3 = row.y, lo = row.z, hi = row.w;
-    const int64_t ky = h2 >= 0 ? h2 : b.nf[1] + h2;
-    const int64_t kz = h3 >= 0 ? h3 : b.nf[2] + h3;
-    const int64_t rowbase = (kz * b.nf[1] + ky) * b.c1;
-    const R dyz = inv2[abs(h2)] * inv3[abs(h3)];
-    const int64_t gbase =
-        ((int64_t)(h3 + b.hm[2]) * b.m2 + (int64_t)(h2 + b.hm[1])) * (int64_t)(b.hm[0] + 1);
-    double crow[3];
-    row_const(b, h2, h3, crow);
-    C vn[NT];
-    {
-      const bool in = lo + lane <= hi;
-#pragma unroll
-      for (int t = 0; t < NT; ++t)
-        if (in) vn[t] = G[(int64_t)t * b.vol_cplx + rowbase + lo + lane];
-    }
-    for (int h1b = lo; h1b <= hi; h1b += 32) {
-      const int h1 = h1b + lane;
-      const bool inrow = h1 <= hi;
-      C v[NT];
-#pragma unroll
-      for (int t = 0; t < NT; ++t) v[t] = vn[t];
-      {  // the next 32 modes of the row, in flight while these are binned
-        const bool in = h1 + 32 <= hi;
-#pragma unroll
-        for (int t = 0; t < NT; ++t)
-          if (in) vn[t] = G[(int64_t)t * b.vol_cplx + rowbase + h1 + 32];
-      }
-      double ql = 0.0;
-      int s = 0;
-      const bool keep = inrow && classify_mode(b, crow, h1, h2, h3, s, ql);
-      const unsigned act = __ballot_sync(FULL, keep);
-      if (act == 0u) continue;
-      const R dec = inrow ? inv1[h1] * dyz : R(0);
-      const double mult = h1 > 0 ? 2.0 : 1.0;
-      double re[NT], im[NT];
-      double tre = 0.0, tim = 0.0;
-#pragma unroll
-      for (int t = 0; t < NT; ++t) {
-        re[t] = keep ? (double)(v[t].x * dec) : 0.0;
-        im[t] = keep ? (double)(v[t].y * dec) : 0.0;
-        const double a = XR ? (keep ? xray_f(xcoef + 9 * t, ql) : 0.0) : am[t];
-        tre += a * re[t];
-        tim += a * im[t];
-      }
-      double val[1 + NPAIR];
-      val[0] = mult * (tre * tre + tim * tim);
-      if (b.want_grid && keep) gnum[gbase + h1] += val[0] / mult;
-      {
-        int p = 1;
-#pragma unroll
-        for (int a = 0; a < NT; ++a)
-#pragma unroll
-          for (int c = a; c < NT; ++c) val[p++] = mult * (re[a] * re[c] + im[a] * im[c]);
-      }
-      const int nv = b.partials ? 1 + NPAIR : 1;
-      const int s0 = __shfl_sync(FULL, s, __ffs(act) - 1);
-      if (__all_sync(FULL, !keep || s == s0)) {
-#pragma unroll
-        for (int q = 0; q < 1 + NPAIR; ++q) {
-          if (q < nv) {
-            const double sum = warp_sum(keep ? val[q] : 0.0);
-            if (lane == 0) hist[q * nq + s0] += sum;
-          }
-        }
-      } else {
-        unsigned todo = act;
-        for (int round = 0; round < BINW_ROUNDS && todo; ++round) {
-          const bool mine = (todo >> lane) & 1u;
-          bool lead = false;
-          if (mine) {
-            const unsigned peers = __match_any_sync(todo, s);
-            lead = (peers & ((1u << lane) - 1u)) == 0u;  // lowest lane of its shell
-          }
-          if (lead) {
-#pragma unroll
-            for (int q = 0; q < 1 + NPAIR; ++q)
-              if (q < nv) hist[q * nq + s] += val[q];
-          }
-          todo &= ~__ballot_sync(FULL, lead);
-          __syncwarp();  // this round's stores before the next round's loads
-        }
-        if ((todo >> lane) & 1u) {
-#pragma unroll
-          for (int q = 0; q < 1 + NPAIR; ++q)
-            if (q < nv) atomicAdd(&hist[q * nq + s], val[q]);
-        }
-      }
-      __syncwarp();
-    }
-  }
-  __syncthreads();
-  for (int i = tid; i < nhist; i += blockDim.x) {
-    double v = 0.0;
-#pragma unroll
-    for (int w = 0; w < BINW_WARPS; ++w) v += s_hist[(size_t)w * nhist + i];
-    if (v != 0.0) atomicAdd(&acc[i], v);
-  }
-}
-
 // den(shell) and shell_count(shell) over all kept modes (both halves),
 // mode_denominator of src/sqc_structure_factor.f90:425-451.
 __global__ void __launch_bounds__(256)
@@ -867,43 +730,10 @@ static cudaError_t bin_dispatch_smem(const int4 *rows, int nrows, const void *G,
   return bin_dispatch_xr<R, NT, false>(rows, nrows, G, b, i1, i2, i3, amp, xc, acc, gnum, nsm, s);
 }
 
-template <typename R, int NT>
-static cudaError_t bin_w(const int4 *rows, int nrows, const void *G, const BinGeom &b,
-                         const R *i1, const R *i2, const R *i3, const double *amp,
-                         const double *xc, double *acc, double *gnum, int nsm, cudaStream_t s) {
-  using C = typename Cplx<R>::T;
-  const size_t sm = (size_t)BINW_WARPS * hist_len(b) * sizeof(double);
-  cudaError_t e;
-  if (b.xray) {
-    e = cudaFuncSetAttribute(k_bin_w<R, NT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)sm);
-    if (e == cudaSuccess)
-      k_bin_w<R, NT, true><<<nsm * 2, 32 * BINW_WARPS, sm, s>>>(rows, nrows, (const C *)G, b, i1,
-                                                                i2, i3, amp, xc, acc, gnum);
-  } else {
-    e = cudaFuncSetAttribute(k_bin_w<R, NT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)sm);
-    if (e == cudaSuccess)
-      k_bin_w<R, NT, false><<<nsm * 2, 32 * BINW_WARPS, sm, s>>>(rows, nrows, (const C *)G, b, i1,
-                                                                 i2, i3, amp, xc, acc, gnum);
-  }
-  return e == cudaSuccess ? cudaGetLastError() : e;
-}
-
 template <typename R>
 cudaError_t launch_bin(const int4 *rows, int nrows, const void *G, const BinGeom &b,
                        const R *inv1, const R *inv2, const R *inv3, const double *amp,
                        const double *xcoef, double *acc, double *gnum, int nsm, cudaStream_t s) {
-  // warp-private histograms when four of them fit two CTAs per SM
-  if (!b.xrd && b.ntr >= 1 && b.ntr <= 4 &&
-      (size_t)BINW_WARPS * hist_len(b) * sizeof(double) <= 112 * 1024) {
-    switch (b.ntr) {
-      case 1: return bin_w<R, 1>(rows, nrows, G, b, inv1, inv2, inv3, amp, xcoef, acc, gnum, nsm, s);
-      case 2: return bin_w<R, 2>(rows, nrows, G, b, inv1, inv2, inv3, amp, xcoef, acc, gnum, nsm, s);
-      case 3: return bin_w<R, 3>(rows, nrows, G, b, inv1, inv2, inv3, amp, xcoef, acc, gnum, nsm, s);
-      case 4: return bin_w<R, 4>(rows, nrows, G, b, inv1, inv2, inv3, amp, xcoef, acc, gnum, nsm, s);
-    }
-  }
   switch (b.ntr) {
     case 1: return bin_dispatch_smem<R, 1>(rows, nrows, G, b, inv1, inv2, inv3, amp, xcoef, acc, gnum, nsm, s);
     case 2: return bin_dispatch_smem<R, 2>(rows, nrows, G, b, inv1, inv2, inv3, amp, xcoef, acc, gnum, nsm, s);
