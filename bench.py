@@ -662,7 +662,7 @@ def run_ours(args, rank, world, local_rank):
                                   qmin=0.0, qmax=QMAX, nq=NQ, norm=_lib.NORM_MEAN,
                                   partials=True, precision=prec, eps=eps, device=local_rank,
                                   upsampfac=args.upsampfac, timing=timing,
-                                  stream=stream.cuda_stream, fft_ring=args.fft_ring)
+                                  stream=stream.cuda_stream)
 
     # --- device-resident inputs: value --------------------------------------
     dev = torch.from_numpy(frames).to(f"cuda:{local_rank}")
@@ -861,8 +861,6 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="single", choices=["single", "double"])
     ap.add_argument("--upsampfac", type=float, default=0.0)
-    ap.add_argument("--fft-ring", action="store_true",
-                    help="FP32 column FFT passes in the ring form (SQN_FLAG_FFT_RING)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-grad", action="store_true", help="skip the dS/dr leg")
     ap.add_argument("--no-configs", action="store_true",

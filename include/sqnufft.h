@@ -70,11 +70,6 @@ enum {
   SQN_FLAG_GRAD = 2,   /* allocate the adjoint buffers of sqn_sq_grad */
   SQN_FLAG_CUFFT = 8,      /* cuFFT R2C + the bin kernel (instead of the pruned 512-point
                               passes that 512^3 grids use by default) */
-  SQN_FLAG_FFT_RING = 64,  /* FP32 plans on the pruned 512-point passes (even H1 = hm0 + 1):
-                              the y and z passes in the ring form (a producer warp streams
-                              column tiles into shared memory with bulk copies while two
-                              groups of compute warps transform and store earlier tiles).
-                              Off by default: experimental, not yet measured on B200 */
   SQN_FLAG_AUTOTUNE = 128  /* choose the fine grid and kernel width by timing: the plan
                               builds the candidate (sigma, w) pairs that reach eps (the
                               smallest upsampling for each width up to the precision's
@@ -141,9 +136,7 @@ typedef struct sqn_plan_info {
   int64_t natoms;           /* atoms per frame */
   int32_t xrd_bins;         /* two-theta bins of the powder pattern (0: off) */
   int32_t pruned_fft512;    /* 1: the frame FFT runs as pruned 512-point passes of ours
-                               (every axis 512, no SQN_FLAG_CUFFT) instead of cuFFT;
-                               2: the same with the column passes in the ring form
-                               (SQN_FLAG_FFT_RING) */
+                               (every axis 512, no SQN_FLAG_CUFFT) instead of cuFFT */
   double xrd_step;          /* their width, degrees */
   int32_t autotuned;        /* 1: fine grid and width chosen by timing (SQN_FLAG_AUTOTUNE) */
   int32_t tune_candidates;  /* (sigma, w) pairs timed (0 when the choice came from the cache) */

@@ -24,7 +24,6 @@ HOST, DEVICE = 0, 1
 FLAG_TIMING = 1
 FLAG_GRAD = 2
 FLAG_CUFFT = 8
-FLAG_FFT_RING = 64
 FLAG_AUTOTUNE = 128
 
 # Every symbol include/sqnufft.h declares.
@@ -218,13 +217,13 @@ class Plan:
                  xray_coef=None, qmin=0.0, qmax=20.0, nq=500, norm=NORM_MEAN, partials=True,
                  want_grid=False, precision=PREC_DOUBLE, eps=1e-9, upsampfac=0.0,
                  kernel_width=0, device=0, max_grid_modes=0, timing=False, stream=None,
-                 grad=False, cufft=False, xrd=None, fft_ring=False, autotune=False):
+                 grad=False, cufft=False, xrd=None, autotune=False):
         L = load()
         self._L = L
         d = self._describe(cell, origin, type_id, ntypes, weight, amp_const, xray_coef, qmin,
                            qmax, nq, norm, partials, want_grid, precision, eps, upsampfac,
                            kernel_width, device, max_grid_modes, timing, stream, grad, cufft,
-                           xrd, fft_ring, autotune)
+                           xrd, autotune)
         h = ctypes.c_void_p()
         self.status = check(L.sqn_plan_create(ctypes.byref(d), ctypes.byref(h)), "sqn_plan_create")
         self._attach(h, owned=True)
@@ -233,11 +232,10 @@ class Plan:
                   xray_coef=None, qmin=0.0, qmax=20.0, nq=500, norm=NORM_MEAN, partials=True,
                   want_grid=False, precision=PREC_DOUBLE, eps=1e-9, upsampfac=0.0,
                   kernel_width=0, device=0, max_grid_modes=0, timing=False, stream=None,
-                  grad=False, cufft=False, xrd=None, fft_ring=False, autotune=False):
+                  grad=False, cufft=False, xrd=None, autotune=False):
         """Fill an SqnDesc; the arrays it points to are kept on self.  xrd: None, or a
         dict(lam=..., range=(min, max), step=0.0, lp=True) for the powder pattern.
         cufft: cuFFT R2C instead of the pruned 512-point passes on 512^3 grids.
-        fft_ring: FP32 column passes of the pruned 512-point FFT in the ring form.
         autotune: fine grid and kernel width chosen by timing (SQN_FLAG_AUTOTUNE)."""
         L = self._L
         self.type_id = np.ascontiguousarray(type_id, dtype=np.int32)
@@ -271,7 +269,6 @@ class Plan:
         d.precision = int(precision)
         d.flags = ((FLAG_TIMING if timing else 0) | (FLAG_GRAD if grad else 0)
                    | (FLAG_CUFFT if cufft else 0)
-                   | (FLAG_FFT_RING if fft_ring else 0)
                    | (FLAG_AUTOTUNE if autotune else 0))
         d.eps = float(eps)
         d.upsampfac = float(upsampfac)

@@ -269,9 +269,7 @@ struct sqn_plan_s {
   bool inplace = false;  // cuFFT R2C in place over padded real rows (dS/dr plans)
   int64_t c1pitch = 0;  // complex row pitch of the half spectrum
   // pruned 512-point passes (every axis 512): compact half spectrum in d_G
-  int *d_err = nullptr;    // set by a kernel whose bounded wait gave up
   bool fft512 = false;
-  bool fft_ring = false;  // FP32: column passes in the ring form (SQN_FLAG_FFT_RING)
   void *d_tw512 = nullptr;
   BinGeom bg512{};
   // density amplitudes (sqn_density_modes): request buffers, grown on demand
@@ -875,14 +873,6 @@ int setup_plan(sqn_plan *p, const sqn_plan_desc *d) {
     p->bg512.c1 = p->hm[0] + 1;
     p->bg512.vol_cplx = p->bg512.c1 * p->bg512.nf[1] * p->bg512.nf[2];
     p->fft512 = true;
-    if (!p->fp64 && (d->flags & SQN_FLAG_FFT_RING) && (p->hm[0] + 1) % 2 == 0) {
-      if (!p->d_err) {
-        if ((st = dalloc(p, &p->d_err, 1))) return st;
-        if (cudaMemset(p->d_err, 0, sizeof(int)) != cudaSuccess) return SQN_ERR_CUDA;
-      }
-      if (fft512_ring_set_attributes() != cudaSuccess) return SQN_ERR_CUDA;
-      p->fft_ring = true;
-    }
   }
 
   // --- adjoint buffers (dS/dr) -----------------------------------------------
@@ -936,19 +926,9 @@ int setup_plan(sqn_plan *p, const sqn_plan_desc *d) {
 // Kernels of ours that one frame launches.
 int frame_launches(const sqn_plan *p) { return p->fft512 ? 8 : 5; }
 
-// All queued work of the plan finished; a kernel that gave up a bounded wait
-// since the last check turns into an error here.
+// All queued work of the plan finished.
 int sync_plan(sqn_plan *p) {
   if (cudaStreamSynchronize(p->stream) != cudaSuccess) return SQN_ERR_CUDA;
-  if (p->d_err) {
-    int h = 0;
-    if (cudaMemcpy(&h, p->d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
-      return SQN_ERR_CUDA;
-    if (h != 0) {
-      cudaMemset(p->d_err, 0, sizeof(int));
-      return SQN_ERR_CUDA;
-    }
-  }
   return SQN_OK;
 }
 
@@ -1059,8 +1039,7 @@ template <typename R> int run_frame(sqn_plan *p, const double *dpos, int slot) {
   if (p->fft512) {
     // x pass into d_G, y pass back into the (consumed) grid, z pass into d_G
     e = launch_fft512<R>((const R *)grid, p->d_G, grid, p->d_G, p->ntr, g.pitch, p->hm[0] + 1,
-                         p->hm[1], p->hm[2], p->d_tw512, p->nsm, s, p->fft_ring ? 1 : 0,
-                         p->d_err);
+                         p->hm[1], p->hm[2], p->d_tw512, p->nsm, s);
     if (e != cudaSuccess) return SQN_ERR_CUDA;
     p->launches += 3;
   } else if (exec_forward(p, s, grid, p->d_G) != CUFFT_SUCCESS) {
@@ -1192,7 +1171,7 @@ int sqn_plan_info_get(const sqn_plan *p, sqn_plan_info *info) {
   info->ntransforms = p->ntr;
   info->nspecies = p->nspecies;
   info->device_bytes = p->device_bytes;
-  info->pruned_fft512 = p->fft512 ? (p->fft_ring ? 2 : 1) : 0;
+  info->pruned_fft512 = p->fft512 ? 1 : 0;
   info->natoms = p->desc.natoms;
   info->xrd_bins = p->bg.xrd ? p->bg.xbins : 0;
   info->xrd_step = p->bg.xrd ? p->bg.xstep : 0.0;

@@ -337,282 +337,6 @@ __global__ void __launch_bounds__(32 * COLS, sizeof(R) == 4 ? 2 : 1)
   }
 }
 
-// ---------------------------------------------------------------------------
-// Column passes, ring form (FP32, opt-in): one persistent CTA per SM with a
-// ring of three shared-memory tile buffers.  Tiles (16 columns x 512 rows)
-// arrive by bulk copies (cp.async.bulk, one row segment per copy, completion
-// counted on the buffer's `full` mbarrier); two groups of eight warps take
-// alternate tiles, each warp transforming two adjacent columns with 16-byte
-// shared accesses (the column pair is its own scratch line); the group then
-// stores the kept band with coalesced row stores and, having released the
-// buffer, issues the copies of the tile three steps on into it.  The loads of
-// the next tiles thus overlap the transforms and stores of the current ones,
-// which the barrier-phased kernel above cannot do.  Needs H1 even (16-byte
-// aligned rows and copy sizes).  Every wait is bounded by elapsed time (the
-// globaltimer): a give-up is recorded in *err and in a shared abort word that
-// every wait of the CTA polls, so both groups leave at once; before the CTA
-// ends it waits (again with a deadline) until each buffer's last bulk copy has
-// landed.
-// ---------------------------------------------------------------------------
-constexpr int RING_NB = 3;
-constexpr int RING_LD = 18;  // buffer row pitch (complex): 144 bytes, rows 16-byte aligned
-constexpr int RING_GROUPS = 2;
-constexpr int RING_GW = 8;  // compute warps per group, two columns each
-constexpr int RING_THREADS = 32 * RING_GROUPS * RING_GW;
-constexpr size_t RING_BUF = (size_t)512 * RING_LD;  // complex per buffer
-
-__host__ __device__ constexpr size_t ring_smem() {
-  return sizeof(float2) * (TW_LEN + RING_NB * RING_BUF) + sizeof(uint64_t) * RING_NB +
-         sizeof(unsigned) * RING_NB + sizeof(int);
-}
-
-__device__ __forceinline__ uint32_t smem_addr(const void *p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ uint64_t now_ns() {
-  uint64_t t;
-  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
-  return t;
-}
-// Longest wait of one step (a tile normally lands within microseconds).
-constexpr uint64_t RING_WAIT_NS = 2000000000ull;
-// Wait for phase `parity` of the barrier until the deadline or, when abort is
-// given, until another group has raised it.
-__device__ __forceinline__ bool ring_wait(uint32_t mbar, uint32_t parity, uint64_t deadline,
-                                          const volatile int *abort) {
-  for (;;) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.b32 %0, 1, 0, p;\n\t}\n"
-        : "=r"(ok)
-        : "r"(mbar), "r"(parity)
-        : "memory");
-    if (ok) return true;
-    if ((abort && *abort) || now_ns() > deadline) return false;
-  }
-}
-__device__ __forceinline__ void ring_expect_tx(uint32_t mbar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes)
-               : "memory");
-}
-// global -> shared bulk copy (16-byte aligned addresses, size a multiple of 16)
-__device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_t bytes,
-                                          uint32_t mbar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-          dst),
-      "l"(src), "r"(bytes), "r"(mbar)
-      : "memory");
-}
-// Named barrier of one compute group; group_any also ORs a predicate over it.
-__device__ __forceinline__ void group_sync(int id) {
-  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(32 * RING_GW) : "memory");
-}
-__device__ __forceinline__ bool group_any(int id, bool q) {
-  uint32_t r;
-  asm volatile(
-      "{\n\t.reg .pred pq, pr;\n\t"
-      "setp.ne.u32 pq, %1, 0;\n\t"
-      "bar.red.or.pred pr, %2, %3, pq;\n\t"
-      "selp.u32 %0, 1, 0, pr;\n\t}"
-      : "=r"(r)
-      : "r"((uint32_t)q), "r"(id), "r"(32 * RING_GW)
-      : "memory");
-  return r != 0;
-}
-
-// warp_fft512 on two lines at once (same operations per line); the scratch
-// line holds both lines' slot i as one float4 at scr[i * sstride].
-__device__ __forceinline__ void warp_fft512_pair(float2 (&a)[16], float2 (&b)[16], float4 *scr,
-                                                 int sstride, const float2 *tw, int lane) {
-  dft16(a);
-  dft16(b);
-#pragma unroll
-  for (int k2 = 1; k2 < 16; ++k2) {
-    const float2 w = tw[512 + 32 * k2 + lane];
-    a[k2] = c_mul(a[k2], w);
-    b[k2] = c_mul(b[k2], w);
-  }
-#pragma unroll
-  for (int k2 = 0; k2 < 16; ++k2)
-    scr[tslot(k2, lane) * sstride] = make_float4(a[k2].x, a[k2].y, b[k2].x, b[k2].y);
-  __syncwarp();
-  const int k2 = lane & 15, m1 = lane >> 4;
-#pragma unroll
-  for (int m2 = 0; m2 < 16; ++m2) {
-    const float4 q = scr[tslot(k2, m1 + 2 * m2) * sstride];
-    a[m2] = make_float2(q.x, q.y);
-    b[m2] = make_float2(q.z, q.w);
-  }
-  __syncwarp();
-  dft16(a);
-  dft16(b);
-  if (m1) {
-#pragma unroll
-    for (int i = 1; i < 16; ++i) {
-      const float2 w = tw[16 * i];
-      a[i] = c_mul(a[i], w);
-      b[i] = c_mul(b[i], w);
-    }
-  }
-  const float sg = m1 ? -1.f : 1.f;
-#pragma unroll
-  for (int i = 0; i < 16; ++i) {
-    a[i] = c_sfma(sg, a[i], shfl_xor16(a[i]));
-    b[i] = c_sfma(sg, b[i], shfl_xor16(b[i]));
-  }
-}
-
-// Issue the bulk copies of step st (its 16-column tile, 512 rows) into the
-// buffer at shared address dst, counted on the mbarrier `full`; one warp.
-__device__ __forceinline__ void ring_issue(const float2 *in, const ColPass &cp, unsigned st,
-                                           int nblk, uint32_t dst, uint32_t full, int lane) {
-  const unsigned plane = st / (unsigned)nblk;
-  const int c0 = (int)(st - plane * (unsigned)nblk) * COLS;
-  const int nc = min(COLS, cp.ncols - c0);
-  const unsigned t = plane / (unsigned)cp.planes_per_t, p = plane - t * cp.planes_per_t;
-  const float2 *ib = in + t * cp.in_t + p * cp.in_p + c0;
-  const uint32_t bytes = (uint32_t)nc * (uint32_t)sizeof(float2);
-  if (lane == 0) ring_expect_tx(full, 512u * bytes);
-  __syncwarp();
-#pragma unroll 4
-  for (int j = 0; j < 16; ++j) {
-    const int row = lane + 32 * j;
-    bulk_load(dst + (uint32_t)(row * RING_LD * sizeof(float2)), ib + (int64_t)row * cp.in_r,
-              bytes, full);
-  }
-}
-
-__global__ void __launch_bounds__(RING_THREADS, 1)
-    k_fft512_cols_ring(const float2 *__restrict__ in, float2 *__restrict__ out, ColPass cp,
-                       const float2 *__restrict__ tw, int *__restrict__ err) {
-  extern __shared__ __align__(128) unsigned char smem_ring[];
-  float2 *s_tw = reinterpret_cast<float2 *>(smem_ring);
-  float2 *bufs = s_tw + TW_LEN;  // RING_NB x [512][RING_LD]
-  uint64_t *full = reinterpret_cast<uint64_t *>(bufs + RING_NB * RING_BUF);
-  // tiles issued into each buffer so far (monotonic): a group waits for step k
-  // of buffer b only once it has been issued, so that the buffer's barrier is
-  // then in step k's phase or just past it and its parity wait is unambiguous
-  volatile unsigned *issued = reinterpret_cast<volatile unsigned *>(full + RING_NB);
-  // raised by a group that gave up a wait: every other wait of the CTA ends too
-  volatile int *s_abort = reinterpret_cast<volatile int *>(issued + RING_NB);
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int nblk = (cp.ncols + COLS - 1) / COLS;
-  const int M = 2 * cp.hm + 1;
-  const unsigned nsteps = (unsigned)cp.nplanes * (unsigned)nblk;
-  // this CTA's steps st = blockIdx.x + k gridDim.x, k < nloc; step k uses buffer k % RING_NB
-  const unsigned nloc = blockIdx.x < nsteps ? (nsteps - 1 - blockIdx.x) / gridDim.x + 1 : 0;
-  for (int i = tid; i < TW_LEN; i += blockDim.x) s_tw[i] = tw[i];
-  if (tid == 0) {
-    for (int b = 0; b < RING_NB; ++b) {
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(full + b)) : "memory");
-      issued[b] = (unsigned)b < nloc ? 1u : 0u;  // warp 0 issues them below
-    }
-    *s_abort = 0;
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  __syncthreads();
-  if (warp == 0) {  // the first RING_NB tiles
-    for (unsigned k = 0; k < RING_NB && k < nloc; ++k)
-      ring_issue(in, cp, blockIdx.x + k * gridDim.x, nblk,
-                 smem_addr(bufs + (size_t)k * RING_BUF), smem_addr(full + k), lane);
-  }
-
-  // compute group g takes steps k = g, g + 2, ...; after storing step k it
-  // issues step k + RING_NB into the buffer it has just released
-  const int g = warp / RING_GW, wi = warp % RING_GW;
-  const int gt = tid - 32 * RING_GW * g;  // thread within the group
-  const int bar_id = 1 + g;
-  for (unsigned k = g; k < nloc; k += RING_GROUPS) {
-    const unsigned st = blockIdx.x + k * gridDim.x;
-    const int b = (int)(k % RING_NB);
-    const uint64_t deadline = now_ns() + RING_WAIT_NS;
-    bool ok = true;
-    while (issued[b] < k / RING_NB + 1) {
-      if (*s_abort || now_ns() > deadline) {
-        ok = false;
-        break;
-      }
-      __nanosleep(32);
-    }
-    ok = ok && ring_wait(smem_addr(full + b), (k / RING_NB) & 1u, deadline, s_abort);
-    if (group_any(bar_id, !ok)) {
-      if (gt == 0) {
-        *s_abort = 1;
-        atomicExch(err, 3);
-      }
-      break;
-    }
-    const unsigned plane = st / (unsigned)nblk;
-    const int c0 = (int)(st - plane * (unsigned)nblk) * COLS;
-    const int nc = min(COLS, cp.ncols - c0);
-    const unsigned t = plane / (unsigned)cp.planes_per_t, p = plane - t * cp.planes_per_t;
-    float2 *ob = out + t * cp.out_t + p * cp.out_p + c0;
-    float2 *buf = bufs + (size_t)b * RING_BUF;
-    if (2 * wi < nc) {
-      constexpr int LD4 = RING_LD / 2;
-      float4 *col = reinterpret_cast<float4 *>(buf + 2 * wi);  // row stride LD4
-      float2 va[16], vb[16];
-#pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        const float4 q = col[(lane + 32 * j) * LD4];
-        va[j] = make_float2(q.x, q.y);
-        vb[j] = make_float2(q.z, q.w);
-      }
-      __syncwarp();
-      warp_fft512_pair(va, vb, col, LD4, s_tw, lane);
-      const int k2 = lane & 15, hb = lane >> 4;
-#pragma unroll
-      for (int i = 0; i < 16; ++i)
-        col[(k2 + 16 * i + 256 * hb) * LD4] = make_float4(va[i].x, va[i].y, vb[i].x, vb[i].y);
-    }
-    group_sync(bar_id);
-    // kept band, coalesced: rows hw = 0 .. hm from tile rows hw, rows hm + 1 .. M - 1
-    // from tile rows 512 + hw - M
-    {
-      const int c = gt & (COLS - 1), r0 = gt >> 4;
-      if (c < nc) {
-        constexpr int RSTEP = 32 * RING_GW / COLS;  // rows per sweep of the group
-        const int64_t ostep = RSTEP * cp.out_r;
-        float2 *dst = ob + (int64_t)r0 * cp.out_r + c;
-        const float2 *tp = buf + r0 * RING_LD + c;
-        int hw = r0;
-        for (; hw <= cp.hm; hw += RSTEP, tp += RSTEP * RING_LD, dst += ostep) *dst = *tp;
-        tp += (512 - M) * RING_LD;
-        for (; hw < M; hw += RSTEP, tp += RSTEP * RING_LD, dst += ostep) *dst = *tp;
-      }
-    }
-    // the group's generic reads and writes of the buffer come before the bulk
-    // copies of the next tile into it
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    group_sync(bar_id);
-    if (wi == 0 && k + RING_NB < nloc) {
-      ring_issue(in, cp, st + RING_NB * gridDim.x, nblk, smem_addr(buf), smem_addr(full + b),
-                 lane);
-      if (lane == 0) {
-        __threadfence_block();
-        issued[b] = k / RING_NB + 2;
-      }
-    }
-  }
-  // Before the CTA ends, the copies issued into each buffer have landed (they
-  // all have unless a group gave up a wait): a buffer's earlier tiles were
-  // waited for before its last one was issued, so only that one can be in
-  // flight.  Bulk copies from global memory complete on their own, so this
-  // wait ends long before its deadline; the abort word does not cut it short.
-  __syncthreads();
-  if (tid == 0) {
-    const uint64_t deadline = now_ns() + RING_WAIT_NS;
-    for (int b = 0; b < RING_NB; ++b) {
-      const unsigned n = issued[b];
-      if (n > 0 && !ring_wait(smem_addr(full + b), (n - 1) & 1u, deadline, nullptr))
-        atomicExch(err, 3);
-    }
-  }
-}
-
 template <typename R> size_t cols_smem() {
   return sizeof(typename Cplx<R>::T) * (TW_LEN + 512 * COL_LD);
 }
@@ -622,10 +346,6 @@ template <typename R> size_t cols_smem() {
 template <typename R> cudaError_t fft512_set_attributes() {
   return cudaFuncSetAttribute(k_fft512_cols<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)cols_smem<R>());
-}
-cudaError_t fft512_ring_set_attributes() {
-  return cudaFuncSetAttribute(k_fft512_cols_ring, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)ring_smem());
 }
 template cudaError_t fft512_set_attributes<float>();
 template cudaError_t fft512_set_attributes<double>();
@@ -643,12 +363,9 @@ void fft512_twiddles(std::vector<double> &tw) {
 
 // grid [ntr][nf2][nf1][pitch] real -> A1 [ntr][nf2][nf1][H1] -> A2 [ntr][nf2][M2][H1]
 // -> G [ntr][M3][M2][H1] (A2 may share the grid's storage; A1 and G share one buffer).
-// ring != 0 (FP32, H1 even): the column passes in the ring form, *err set
-// when one of its bounded waits gives up.
 template <typename R>
 cudaError_t launch_fft512(const R *grid, void *A1, void *A2, void *G, int ntr, int64_t pitch,
-                          int H1, int hm1, int hm2, const void *tw, int nsm, cudaStream_t s,
-                          int ring, int *err) {
+                          int H1, int hm1, int hm2, const void *tw, int nsm, cudaStream_t s) {
   using C = typename Cplx<R>::T;
   const int n = 512;
   const int M2 = 2 * hm1 + 1, M3 = 2 * hm2 + 1;
@@ -671,14 +388,9 @@ cudaError_t launch_fft512(const R *grid, void *A1, void *A2, void *G, int ntr, i
   y.nplanes = (int64_t)ntr * n;
   y.ncols = H1;
   y.hm = hm1;
-  const bool use_ring = sizeof(R) == 4 && ring && err != nullptr && H1 % 2 == 0;
   auto cols = [&](const void *src, void *dst, const ColPass &cp) {
-    if (use_ring)
-      k_fft512_cols_ring<<<nsm, RING_THREADS, ring_smem(), s>>>(
-          (const float2 *)src, (float2 *)dst, cp, (const float2 *)tw, err);
-    else
-      k_fft512_cols<R><<<nsm * cta, 32 * COLS, sm, s>>>((const C *)src, (C *)dst, cp,
-                                                        (const C *)tw);
+    k_fft512_cols<R><<<nsm * cta, 32 * COLS, sm, s>>>((const C *)src, (C *)dst, cp,
+                                                      (const C *)tw);
   };
   cols(A1, A2, y);
   e = cudaGetLastError();
@@ -698,10 +410,8 @@ cudaError_t launch_fft512(const R *grid, void *A1, void *A2, void *G, int ntr, i
   return cudaGetLastError();
 }
 template cudaError_t launch_fft512<float>(const float *, void *, void *, void *, int, int64_t,
-                                          int, int, int, const void *, int, cudaStream_t, int,
-                                          int *);
+                                          int, int, int, const void *, int, cudaStream_t);
 template cudaError_t launch_fft512<double>(const double *, void *, void *, void *, int, int64_t,
-                                           int, int, int, const void *, int, cudaStream_t, int,
-                                           int *);
+                                           int, int, int, const void *, int, cudaStream_t);
 
 }  // namespace sqn

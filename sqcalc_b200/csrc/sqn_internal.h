@@ -144,14 +144,10 @@ std::vector<double> kernel_ft(int64_t nf, int w, double beta, int kmax);
 // Pruned 512-point FFT passes (sqn_fft512.cu): grid -> A1 (x) -> A2 (y) -> G
 // (z), G the compact half spectrum [ntr][2 hm2 + 1][2 hm1 + 1][H1].
 template <typename R> cudaError_t fft512_set_attributes();
-cudaError_t fft512_ring_set_attributes();  // the FP32 ring form of the column passes
 void fft512_twiddles(std::vector<double> &tw);  // the passes' table, interleaved re, im
-// ring != 0: FP32 column passes in the ring form (bulk-copy producer warp,
-// two compute groups; H1 even), *err set when a bounded wait gives up.
 template <typename R>
 cudaError_t launch_fft512(const R *grid, void *A1, void *A2, void *G, int ntr, int64_t pitch,
-                          int H1, int hm1, int hm2, const void *tw, int nsm, cudaStream_t s,
-                          int ring, int *err);
+                          int H1, int hm1, int hm2, const void *tw, int nsm, cudaStream_t s);
 
 // Density amplitudes of requested lattice points from the half spectra.
 template <typename R>

@@ -119,23 +119,3 @@ def test_default_512_path_against_direct_sum():
         else:
             assert dS < 1e-5 and dP < 1e-5, (dS, dP)
 
-
-def test_ring_form_matches_default_passes():
-    """The FP32 column passes in the ring form (SQN_FLAG_FFT_RING: bulk-copy tile
-    ring, two compute groups, time-bounded mbarrier waits) against the default
-    barrier-phased passes on the same frames; sqn_sync must report no wait that
-    gave up.  q_max gives 423 modes per axis (H1 = 212 kept h1 >= 0, even, as the
-    ring's 16-byte bulk copies need)."""
-    tid, fr = frames(2)
-    qmax = 210.5 * 2 * np.pi / L
-    with plan(tid, _lib.PREC_SINGLE, 1e-6, False, fft_ring=True, qmax=qmax) as pr, \
-            plan(tid, _lib.PREC_SINGLE, 1e-6, False, qmax=qmax) as pd:
-        assert list(pr.modes) == [423, 423, 423]
-        assert pr.info.pruned_fft512 == 2 and pd.info.pruned_fft512 == 1
-        for p in (pr, pd):
-            for f in fr:
-                p.accumulate(f)
-        pr.sync()
-        a, b = pr.finalize(), pd.finalize()
-        for x, y in ((a[0], b[0]), (a[1], b[1])):
-            assert np.max(np.abs(x - y)) / max(1.0, float(np.max(np.abs(y)))) < 1e-6
