@@ -337,11 +337,16 @@ int sqn_accumulate_dump(sqn_plan *plan, sqn_dump *dump, int64_t max_frames,
 /* ---- Batches of independent systems ------------------------------------
  * Many uneven systems (each its own cell, atoms, types and grid) whose frames
  * are accumulated together: one plan per system, and one frame of EVERY system
- * captured once into a CUDA graph -- the root stream forks to one stream per
- * system (its prep, scan, scatter, spread, FFT and bin launches form one
- * branch) and joins -- so that a step over all systems is a single graph
- * launch with the systems' kernels running side by side.  No counterpart in the
- * reference, which runs one system per process.
+ * captured once into a CUDA graph, so that a step over all systems is a single
+ * graph launch.  When the systems share precision, transform count and weight
+ * kind (and have no powder pattern), the graph runs each frame stage for all
+ * systems in one launch: bin sort (three launches), spread (one launch over
+ * every system's tiles and transforms), the systems' FFTs as parallel branches,
+ * binning (one launch over every system's rows); otherwise the root stream
+ * forks to one stream per system, each running its own frame path.  With
+ * SQN_FLAG_AUTOTUNE in the descriptors each system's fine grid and width are
+ * chosen by timing.  No counterpart in the reference, which runs one system
+ * per process.
  *
  * sqn_batch_create: descs[nsystems] as for sqn_plan_create (same device; each
  *   desc's stream is ignored, its timing flag cleared); stream is the root
@@ -353,7 +358,11 @@ int sqn_accumulate_dump(sqn_plan *plan, sqn_dump *dump, int64_t max_frames,
  * sqn_batch_plan: the plan of system k (owned by the batch) for
  *   sqn_get_accumulators / sqn_finalize after sqn_batch_sync; do not accumulate
  *   on it directly while graph replays are in flight.
- * sqn_batch_graph_launches: graph replays so far. */
+ * sqn_batch_graph_launches: graph replays so far.
+ * sqn_batch_launch_count: kernels of this library launched by those replays
+ *   (cuFFT's own kernels not counted).
+ * sqn_batch_multi: 1 when the batch runs the multi-system launches, 0 when it
+ *   runs one branch per system. */
 typedef struct sqn_batch_s sqn_batch;
 int sqn_batch_create(const sqn_plan_desc *descs, int32_t nsystems, void *stream,
                      sqn_batch **out);
@@ -362,6 +371,8 @@ int sqn_batch_accumulate(sqn_batch *batch, const double *const *pos, int64_t nfr
 int sqn_batch_sync(sqn_batch *batch);
 int sqn_batch_plan(sqn_batch *batch, int32_t system, sqn_plan **plan);
 int64_t sqn_batch_graph_launches(const sqn_batch *batch);
+int64_t sqn_batch_launch_count(const sqn_batch *batch);
+int32_t sqn_batch_multi(const sqn_batch *batch);
 int sqn_batch_destroy(sqn_batch *batch);
 
 /* Size of the fixed device scratch array of sqn_spread_frame_noalloc (per GPU). */

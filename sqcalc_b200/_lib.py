@@ -33,7 +33,8 @@ EXPORTS = (
     "sqn_peek_num_async", "sqn_finalize", "sqn_reset", "sqn_stage_times", "sqn_launch_count",
     "sqn_plan_destroy", "sqn_spread_frame_noalloc", "sqn_sq_grad", "sqn_accumulator_view",
     "sqn_set_frame_count", "sqn_batch_create", "sqn_batch_accumulate", "sqn_batch_sync",
-    "sqn_batch_plan", "sqn_batch_graph_launches", "sqn_batch_destroy", "sqn_type1_default_opts",
+    "sqn_batch_plan", "sqn_batch_graph_launches", "sqn_batch_launch_count",
+    "sqn_batch_multi", "sqn_batch_destroy", "sqn_type1_default_opts",
     "sqn_type1_makeplan", "sqn_type1f_makeplan", "sqn_type1_setpts", "sqn_type1f_setpts",
     "sqn_type1_execute", "sqn_type1f_execute", "sqn_type1_destroy", "sqn_dump_open",
     "sqn_dump_next", "sqn_dump_last_error", "sqn_dump_rewind", "sqn_dump_close",
@@ -160,6 +161,10 @@ def load():
     L.sqn_batch_plan.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(vp)]
     L.sqn_batch_graph_launches.argtypes = [vp]
     L.sqn_batch_graph_launches.restype = i64
+    L.sqn_batch_launch_count.argtypes = [vp]
+    L.sqn_batch_launch_count.restype = i64
+    L.sqn_batch_multi.argtypes = [vp]
+    L.sqn_batch_multi.restype = ctypes.c_int32
     L.sqn_batch_destroy.argtypes = [vp]
     L.sqn_type1_default_opts.argtypes = [ctypes.POINTER(Type1Opts)]
     L.sqn_type1_default_opts.restype = None
@@ -502,6 +507,15 @@ class Batch:
 
     def graph_launches(self):
         return int(self._L.sqn_batch_graph_launches(self._h))
+
+    def launch_count(self):
+        """Kernels of this library launched by the graph replays so far."""
+        return int(self._L.sqn_batch_launch_count(self._h))
+
+    @property
+    def multi(self):
+        """True when every frame stage runs for all systems in one launch."""
+        return bool(self._L.sqn_batch_multi(self._h))
 
     def close(self):
         if getattr(self, "_h", None) and self._h.value:

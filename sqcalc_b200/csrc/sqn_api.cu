@@ -1548,6 +1548,20 @@ struct sqn_batch_s {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   int64_t replays = 0;
+  // Multi-system path: the sort, the spread and the binning of every system
+  // in one launch each (BatchSys table and prefix sums in device memory);
+  // the FFTs stay per system, as parallel branches.
+  bool multi = false;
+  bool fp64 = false;
+  int ntr = 0, hist_max = 0;
+  bool xray = false;
+  int64_t natoms = 0;
+  int spread_blocks = 0, bin_blocks = 0;
+  BatchSys *d_sys = nullptr;
+  int64_t *d_apre = nullptr;
+  int *d_spre = nullptr, *d_bpre = nullptr;
+  int64_t launches_per_step = 0;  // kernels of ours per frame of every system
+  int64_t launches = 0;
 };
 
 namespace {
@@ -1562,8 +1576,125 @@ void free_batch(sqn_batch *b) {
     if (e) cudaEventDestroy(e);
   if (b->fork) cudaEventDestroy(b->fork);
   for (sqn_plan *p : b->plans) free_plan(p);
+  if (b->d_sys) cudaFree(b->d_sys);
+  if (b->d_apre) cudaFree(b->d_apre);
+  if (b->d_spre) cudaFree(b->d_spre);
+  if (b->d_bpre) cudaFree(b->d_bpre);
   if (b->own_root && b->root) cudaStreamDestroy(b->root);
   delete b;
+}
+
+// The multi-system path needs one precision, one transform count and weight
+// kind, no powder pattern and at most MAX_BATCH_SYSTEMS systems.
+bool batch_multi_ok(const sqn_batch *b) {
+  if (b->plans.empty() || b->plans.size() > (size_t)MAX_BATCH_SYSTEMS) return false;
+  const sqn_plan *p0 = b->plans[0];
+  for (const sqn_plan *p : b->plans) {
+    if (p->fp64 != p0->fp64 || p->ntr != p0->ntr || p->bg.xray != p0->bg.xray || p->bg.xrd ||
+        p->inplace || p->ntr > MAX_FAST_T || (size_t)hist_len(p->bg) * 8 > 160 * 1024)
+      return false;
+  }
+  return true;
+}
+
+// Build the BatchSys table and the prefix sums of the multi-system launches.
+int setup_batch_multi(sqn_batch *b) {
+  const size_t n = b->plans.size();
+  std::vector<BatchSys> sys(n);
+  std::vector<int64_t> apre(n + 1, 0);
+  std::vector<int> spre(n + 1, 0), bpre(n + 1, 0);
+  constexpr int kRowsPerBinBlock = 256;  // 8 warps x 32 rows
+  int64_t sblk = 0, bblk = 0;
+  b->hist_max = 0;
+  for (size_t k = 0; k < n; ++k) {
+    sqn_plan *p = b->plans[k];
+    BatchSys &S = sys[k];
+    std::memset(&S, 0, sizeof(S));
+    S.g = p->fg;
+    S.b = p->fft512 ? p->bg512 : p->bg;
+    S.pos = p->d_pos[0];
+    S.species = p->d_species;
+    S.counts = p->d_counts;
+    S.starts = p->d_starts;
+    S.key = p->d_key;
+    S.slot = p->d_slot;
+    S.recs = p->d_recs;
+    S.strength = p->d_strength;
+    S.grid = p->d_grid;
+    S.G = p->d_G;
+    S.rows = p->d_rows;
+    for (int d = 0; d < 3; ++d) S.inv[d] = p->d_inv[d];
+    S.amp = p->d_amp;
+    S.xcoef = p->d_xcoef;
+    S.acc = p->d_acc;
+    S.gnum = p->d_gnum;
+    S.nkeys = p->nkeys;
+    S.nrows = p->nrows;
+    apre[k + 1] = apre[k] + p->desc.natoms;
+    sblk += (int64_t)p->fg.ntiles * p->ntr;
+    bblk += std::max<int64_t>(1, (p->nrows + kRowsPerBinBlock - 1) / kRowsPerBinBlock);
+    if (sblk >= INT32_MAX || bblk >= INT32_MAX) return SQN_ERR_NOT_SUPPORTED;
+    spre[k + 1] = (int)sblk;
+    bpre[k + 1] = (int)bblk;
+    b->hist_max = std::max(b->hist_max, hist_len(p->bg));
+  }
+  b->natoms = apre[n];
+  b->spread_blocks = (int)sblk;
+  b->bin_blocks = (int)bblk;
+  b->fp64 = b->plans[0]->fp64;
+  b->ntr = b->plans[0]->ntr;
+  b->xray = b->plans[0]->bg.xray != 0;
+  if (cudaMalloc(&b->d_sys, n * sizeof(BatchSys)) != cudaSuccess ||
+      cudaMalloc(&b->d_apre, (n + 1) * sizeof(int64_t)) != cudaSuccess ||
+      cudaMalloc(&b->d_spre, (n + 1) * sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&b->d_bpre, (n + 1) * sizeof(int)) != cudaSuccess) {
+    cudaGetLastError();
+    return SQN_ERR_ALLOC;
+  }
+  if (cudaMemcpy(b->d_sys, sys.data(), n * sizeof(BatchSys), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(b->d_apre, apre.data(), (n + 1) * sizeof(int64_t), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(b->d_spre, spre.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(b->d_bpre, bpre.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
+    return SQN_ERR_CUDA;
+  const cudaError_t e = b->fp64 ? batch_set_attributes<double>(b->ntr, b->xray, b->hist_max)
+                                : batch_set_attributes<float>(b->ntr, b->xray, b->hist_max);
+  if (e != cudaSuccess) return SQN_ERR_CUDA;
+  b->multi = true;
+  return SQN_OK;
+}
+
+// One frame of every system on the multi-system path, queued on the root
+// stream: sort and spread of all systems (four launches), the systems' FFTs
+// as parallel branches, the binning of all systems (one launch).
+template <typename R> int batch_frame_multi(sqn_batch *b) {
+  cudaStream_t root = b->root;
+  BatchPrefix pre{b->d_apre, b->d_spre, b->d_bpre};
+  const int n = (int)b->plans.size();
+  cudaError_t e = launch_batch_sort<R>(b->d_sys, n, pre, b->natoms, root);
+  if (e == cudaSuccess)
+    e = launch_batch_spread<R>(b->d_sys, n, pre, b->spread_blocks, b->plans[0]->fg.chunk, root);
+  if (e != cudaSuccess || cudaEventRecord(b->fork, root) != cudaSuccess) return SQN_ERR_CUDA;
+  int64_t own = 5;
+  for (int k = 0; k < n; ++k) {
+    sqn_plan *p = b->plans[k];
+    if (cudaStreamWaitEvent(p->stream, b->fork, 0) != cudaSuccess) return SQN_ERR_CUDA;
+    if (p->fft512) {
+      if (launch_fft512<R>((const R *)p->d_grid, p->d_G, p->d_grid, p->d_G, p->ntr, p->fg.pitch,
+                           p->hm[0] + 1, p->hm[1], p->hm[2], p->d_tw512, p->nsm,
+                           p->stream) != cudaSuccess)
+        return SQN_ERR_CUDA;
+      own += 3;
+    } else if (exec_forward(p, p->stream, p->d_grid, p->d_G) != CUFFT_SUCCESS) {
+      return SQN_ERR_CUFFT;
+    }
+    if (cudaEventRecord(b->joins[k], p->stream) != cudaSuccess ||
+        cudaStreamWaitEvent(root, b->joins[k], 0) != cudaSuccess)
+      return SQN_ERR_CUDA;
+  }
+  e = launch_batch_bin<R>(b->d_sys, n, pre, b->bin_blocks, b->ntr, b->xray, b->hist_max, root);
+  if (e != cudaSuccess) return SQN_ERR_CUDA;
+  b->launches_per_step = own;
+  return SQN_OK;
 }
 
 // One frame of every system, captured once: the root stream forks to each
@@ -1574,8 +1705,13 @@ int capture_batch(sqn_batch *b) {
   cudaStream_t root = b->root;
   if (cudaStreamBeginCapture(root, cudaStreamCaptureModeRelaxed) != cudaSuccess)
     return SQN_ERR_CUDA;
-  int st = cudaEventRecord(b->fork, root) == cudaSuccess ? SQN_OK : SQN_ERR_CUDA;
-  for (size_t k = 0; k < b->plans.size() && st == SQN_OK; ++k) {
+  int st = SQN_OK;
+  if (b->multi) {
+    st = b->fp64 ? batch_frame_multi<double>(b) : batch_frame_multi<float>(b);
+  } else if (cudaEventRecord(b->fork, root) != cudaSuccess) {
+    st = SQN_ERR_CUDA;
+  }
+  for (size_t k = 0; k < b->plans.size() && st == SQN_OK && !b->multi; ++k) {
     sqn_plan *p = b->plans[k];
     if (cudaStreamWaitEvent(p->stream, b->fork, 0) != cudaSuccess) {
       st = SQN_ERR_CUDA;
@@ -1585,6 +1721,7 @@ int capture_batch(sqn_batch *b) {
     // the capture itself accumulates nothing
     p->nframes -= 1;
     p->launches -= frame_launches(p);
+    b->launches_per_step += frame_launches(p);
     if (st == SQN_OK && (cudaEventRecord(b->joins[k], p->stream) != cudaSuccess ||
                          cudaStreamWaitEvent(root, b->joins[k], 0) != cudaSuccess))
       st = SQN_ERR_CUDA;
@@ -1652,7 +1789,11 @@ int sqn_batch_create(const sqn_plan_desc *descs, int32_t nsystems, void *stream,
   }
   if (st == SQN_OK) {
     cudaSetDevice(b->device);
-    st = capture_batch(b);
+    // every plan's set-up work is done before the capture starts
+    for (sqn_plan *p : b->plans)
+      if (st == SQN_OK && sync_plan(p) != SQN_OK) st = SQN_ERR_CUDA;
+    if (st == SQN_OK && batch_multi_ok(b)) st = setup_batch_multi(b);
+    if (st == SQN_OK) st = capture_batch(b);
   }
   if (st != SQN_OK) {
     free_batch(b);
@@ -1685,9 +1826,10 @@ int sqn_batch_accumulate(sqn_batch *b, const double *const *pos, int64_t nframes
     }
     if (cudaGraphLaunch(b->exec, b->root) != cudaSuccess) return SQN_ERR_CUDA;
     b->replays++;
+    b->launches += b->launches_per_step;
     for (sqn_plan *p : b->plans) {
       p->nframes++;
-      p->launches += frame_launches(p);
+      if (!b->multi) p->launches += frame_launches(p);
     }
   }
   return SQN_OK;
@@ -1707,6 +1849,10 @@ int sqn_batch_plan(sqn_batch *b, int32_t system, sqn_plan **plan) {
 }
 
 int64_t sqn_batch_graph_launches(const sqn_batch *b) { return b ? b->replays : -1; }
+
+int64_t sqn_batch_launch_count(const sqn_batch *b) { return b ? b->launches : -1; }
+
+int32_t sqn_batch_multi(const sqn_batch *b) { return b ? (b->multi ? 1 : 0) : -1; }
 
 int sqn_batch_destroy(sqn_batch *b) {
   if (!b) return SQN_ERR_PLAN_NOTVALID;

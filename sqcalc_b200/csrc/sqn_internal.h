@@ -166,6 +166,49 @@ inline int64_t spread_nkeys(const FrameGeom &g) {
   return (int64_t)g.ntiles * (g.ntr > 1 ? g.ntr : 1);
 }
 
+// One system of a batch for the multi-system kernels: its geometry and the
+// device buffers of its plan.  The batch keeps an array of these in device
+// memory and runs each frame stage for all systems in one launch.
+struct BatchSys {
+  FrameGeom g;
+  BinGeom b;
+  const double *pos;
+  const uint8_t *species;
+  int *counts, *starts;
+  uint32_t *key, *slot;
+  void *recs;
+  const void *strength;
+  void *grid;
+  const void *G;
+  const int4 *rows;
+  const void *inv[3];
+  const double *amp, *xcoef;
+  double *acc, *gnum;
+  int nkeys, nrows;
+};
+// Block and atom offsets of the systems in the multi-system launches
+// (prefix sums, nsys + 1 entries each, device memory).
+struct BatchPrefix {
+  const int64_t *atoms;  // atoms of systems < s
+  const int *spread;     // spread CTAs (tiles x transforms) of systems < s
+  const int *bin;        // bin CTAs of systems < s
+};
+constexpr int MAX_BATCH_SYSTEMS = 1024;
+template <typename R>
+cudaError_t launch_batch_sort(const BatchSys *sys, int nsys, const BatchPrefix &pre,
+                              int64_t natoms, cudaStream_t s);
+template <typename R>
+cudaError_t launch_batch_spread(const BatchSys *sys, int nsys, const BatchPrefix &pre,
+                                int nblocks, int chunk, cudaStream_t s);
+// All systems share ntr, the x-ray flag and no powder pattern; hist_max is the
+// largest nquant * nq.
+template <typename R>
+cudaError_t launch_batch_bin(const BatchSys *sys, int nsys, const BatchPrefix &pre, int nblocks,
+                             int ntr, bool xray, int hist_max, cudaStream_t s);
+// Shared-memory limits of the multi-system spread and bin kernels (call once,
+// before any stream capture).
+template <typename R> cudaError_t batch_set_attributes(int ntr, bool xray, int hist_max);
+
 // Adjoint (sqn_adjoint.cu).
 struct Recip {
   double b[9];  // b_j = b[3*j + r]

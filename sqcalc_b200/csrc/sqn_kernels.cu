@@ -37,28 +37,36 @@ namespace {
 
 using namespace dev;
 
+// Bin key of atom i and its slot in the bin.
+__device__ __forceinline__ void prep_atom(const double *__restrict__ pos,
+                                          const uint8_t *__restrict__ species,
+                                          const FrameGeom &g, int *__restrict__ counts,
+                                          uint32_t *__restrict__ key, uint32_t *__restrict__ slot,
+                                          int64_t i) {
+  AtomCell c;
+  atom_cell(pos, i, g, c);
+  int l0, l1, l2;
+  // bins of transform t follow those of transform t - 1 (one transform per species)
+  const uint32_t k = home_key(c, g, l0, l1, l2) +
+                     (g.ntr > 1 ? (uint32_t)species[i] * (uint32_t)g.ntiles : 0u);
+  key[i] = k;
+  slot[i] = (uint32_t)atomicAdd(&counts[k], 1);
+}
+
 __global__ void k_prep(const double *__restrict__ pos, const uint8_t *__restrict__ species,
                        FrameGeom g, int *__restrict__ counts, uint32_t *__restrict__ key,
                        uint32_t *__restrict__ slot) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < g.natoms;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    AtomCell c;
-    atom_cell(pos, i, g, c);
-    int l0, l1, l2;
-    // bins of transform t follow those of transform t - 1 (one transform per species)
-    const uint32_t k = home_key(c, g, l0, l1, l2) +
-                       (g.ntr > 1 ? (uint32_t)species[i] * (uint32_t)g.ntiles : 0u);
-    key[i] = k;
-    slot[i] = (uint32_t)atomicAdd(&counts[k], 1);
-  }
+       i += (int64_t)gridDim.x * blockDim.x)
+    prep_atom(pos, species, g, counts, key, slot, i);
 }
 
 // Exclusive scan of counts[0..n) into starts[0..n], then zero counts for the
 // next frame.  One CTA of 1024 threads walks the array in chunks of 4096
 // (four consecutive counts per thread, vector loads and stores), carrying the
 // running total from chunk to chunk.
-__global__ void __launch_bounds__(1024) k_scan(int *__restrict__ counts, int *__restrict__ starts,
-                                               int n) {
+__device__ __forceinline__ void scan_counts(int *__restrict__ counts, int *__restrict__ starts,
+                                            int n) {
   __shared__ int wsum[32];
   __shared__ int s_carry;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -117,25 +125,40 @@ __global__ void __launch_bounds__(1024) k_scan(int *__restrict__ counts, int *__
   if (tid == 0) starts[n] = s_carry;
 }
 
+__global__ void __launch_bounds__(1024) k_scan(int *__restrict__ counts, int *__restrict__ starts,
+                                               int n) {
+  scan_counts(counts, starts, n);
+}
+
+// The 16-byte (FP32) / 32-byte (FP64) record of atom i at its sorted position.
+template <typename R>
+__device__ __forceinline__ void scatter_atom(const double *__restrict__ pos,
+                                             const uint8_t *__restrict__ species,
+                                             const FrameGeom &g, const uint32_t *__restrict__ key,
+                                             const uint32_t *__restrict__ slot,
+                                             const int *__restrict__ starts, R *__restrict__ recs,
+                                             int32_t *__restrict__ orig, int64_t i) {
+  AtomCell c;
+  atom_cell(pos, i, g, c);
+  const int sp = species[i];
+  int l0, l1, l2;
+  (void)home_key(c, g, l0, l1, l2);
+  const int64_t dst = (int64_t)starts[key[i]] + slot[i];
+  if (orig) orig[dst] = (int32_t)i;
+  store_rec(recs + dst * REC_SLOTS,
+            pack_rec<R>((uint32_t)l0 | ((uint32_t)l1 << 8) | ((uint32_t)l2 << 16) |
+                        ((uint32_t)sp << 24)),
+            (R)c.off[0], (R)c.off[1], (R)c.off[2]);
+}
+
 template <typename R>
 __global__ void k_scatter(const double *__restrict__ pos, const uint8_t *__restrict__ species,
                           FrameGeom g, const uint32_t *__restrict__ key,
                           const uint32_t *__restrict__ slot, const int *__restrict__ starts,
                           R *__restrict__ recs, int32_t *__restrict__ orig) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < g.natoms;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    AtomCell c;
-    atom_cell(pos, i, g, c);
-    const int sp = species[i];
-    int l0, l1, l2;
-    (void)home_key(c, g, l0, l1, l2);
-    const int64_t dst = (int64_t)starts[key[i]] + slot[i];
-    if (orig) orig[dst] = (int32_t)i;
-    store_rec(recs + dst * REC_SLOTS,
-              pack_rec<R>((uint32_t)l0 | ((uint32_t)l1 << 8) | ((uint32_t)l2 << 16) |
-                          ((uint32_t)sp << 24)),
-              (R)c.off[0], (R)c.off[1], (R)c.off[2]);
-  }
+       i += (int64_t)gridDim.x * blockDim.x)
+    scatter_atom<R>(pos, species, g, key, slot, starts, recs, orig, i);
 }
 
 // Eight z values of a staged row (16-byte aligned) with vector loads.
@@ -205,10 +228,11 @@ __device__ __forceinline__ unsigned group_mask(int r, int w, int len, int n) {
 constexpr unsigned ZLO = 1u << 8, ZHI = 1u << 9;
 
 template <typename R>
-__global__ void __launch_bounds__(SPREAD_THREADS, sizeof(R) == 4 ? 2 : 1)
-    k_spread(const R *__restrict__ recs, const int *__restrict__ starts, FrameGeom g,
-             const R *__restrict__ strength, R *__restrict__ grid,
-             const R *__restrict__ ptw = nullptr) {
+__device__ __forceinline__ void spread_tile(const R *__restrict__ recs,
+                                            const int *__restrict__ starts, const FrameGeom &g,
+                                            const R *__restrict__ strength, R *__restrict__ grid,
+                                            const R *__restrict__ ptw, const int tile,
+                                            const int tr) {
   const int chunk = g.chunk;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R *s_rows = reinterpret_cast<R *>(smem_raw);                        // [chunk][SPREAD_ROW]
@@ -225,7 +249,6 @@ __global__ void __launch_bounds__(SPREAD_THREADS, sizeof(R) == 4 ? 2 : 1)
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int cx = (warp & 3) * PATCH_X + (lane & 7);   // this lane's x cell in the tile
   const int cy = (warp >> 2) * PATCH_Y + (lane >> 3);  // and its y cell
-  const int tile = blockIdx.x, tr = blockIdx.y;
   const int t0 = tile % g.ntile[0];
   const int t1 = (tile / g.ntile[0]) % g.ntile[1];
   const int t2 = tile / (g.ntile[0] * g.ntile[1]);
@@ -411,32 +434,34 @@ __global__ void __launch_bounds__(SPREAD_THREADS, sizeof(R) == 4 ? 2 : 1)
   }
 }
 
+template <typename R>
+__global__ void __launch_bounds__(SPREAD_THREADS, sizeof(R) == 4 ? 2 : 1)
+    k_spread(const R *__restrict__ recs, const int *__restrict__ starts, FrameGeom g,
+             const R *__restrict__ strength, R *__restrict__ grid,
+             const R *__restrict__ ptw = nullptr) {
+  spread_tile<R>(recs, starts, g, strength, grid, ptw, blockIdx.x, blockIdx.y);
+}
+
 // ---------------------------------------------------------------------------
 // Fused deconvolve + weighted total + pair products + FP64 shell binning.
 // NT > 0: exactly NT transforms (unrolled).  NT == 0: any ntr <= MAX_FAST_T.
 // Rows (h2, h3) are dealt to warps; lanes walk h1 >= 0 (32 consecutive complex
 // values per warp and transform, one coalesced read).
 // ---------------------------------------------------------------------------
-template <typename R, int NT, bool SMEM, bool XR, bool XD>
-__global__ void __launch_bounds__(256, 2)
-    k_bin(const int4 *__restrict__ rows, int nrows, const typename Cplx<R>::T *__restrict__ G,
-          BinGeom b, const R *__restrict__ inv1, const R *__restrict__ inv2,
-          const R *__restrict__ inv3, const double *__restrict__ amp,
-          const double *__restrict__ xcoef, double *__restrict__ acc, double *__restrict__ gnum) {
-  extern __shared__ double s_hist[];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int nwarps = blockDim.x >> 5;
-  const int nhist = hist_len(b);
-  double *hist = SMEM ? s_hist : acc;
-  double *xhist = XD ? hist + b.nquant * b.nq : nullptr;
-  if (SMEM) {
-    for (int i = tid; i < nhist; i += blockDim.x) s_hist[i] = 0.0;
-    __syncthreads();
-  }
+// Rows r = r0, r0 + rstep, ... of the half space, one warp each, into the
+// histograms hist (and xhist for the powder pattern, gnum for the grid).
+template <typename R, int NT, bool XR, bool XD>
+__device__ __forceinline__ void bin_rows(const int4 *__restrict__ rows, int nrows,
+                                         const typename Cplx<R>::T *__restrict__ G,
+                                         const BinGeom &b, const R *__restrict__ inv1,
+                                         const R *__restrict__ inv2, const R *__restrict__ inv3,
+                                         const double *__restrict__ amp,
+                                         const double *__restrict__ xcoef, double *hist,
+                                         double *xhist, double *__restrict__ gnum, int r0,
+                                         int rstep, int lane) {
   const int ntr = NT > 0 ? NT : b.ntr;
   constexpr int TM = NT > 0 ? NT : MAX_FAST_T;
-
-  for (int r = blockIdx.x * nwarps + warp; r < nrows; r += gridDim.x * nwarps) {
+  for (int r = r0; r < nrows; r += rstep) {
     const int4 row = rows[r];
     const int h2 = row.x, h3 = row.y, lo = row.z, hi = row.w;
     const int64_t ky = h2 >= 0 ? h2 : b.nf[1] + h2;
@@ -462,6 +487,26 @@ __global__ void __launch_bounds__(256, 2)
                               gbase + h1, lane, xhist);
     }
   }
+}
+
+template <typename R, int NT, bool SMEM, bool XR, bool XD>
+__global__ void __launch_bounds__(256, 2)
+    k_bin(const int4 *__restrict__ rows, int nrows, const typename Cplx<R>::T *__restrict__ G,
+          BinGeom b, const R *__restrict__ inv1, const R *__restrict__ inv2,
+          const R *__restrict__ inv3, const double *__restrict__ amp,
+          const double *__restrict__ xcoef, double *__restrict__ acc, double *__restrict__ gnum) {
+  extern __shared__ double s_hist[];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nwarps = blockDim.x >> 5;
+  const int nhist = hist_len(b);
+  double *hist = SMEM ? s_hist : acc;
+  double *xhist = XD ? hist + b.nquant * b.nq : nullptr;
+  if (SMEM) {
+    for (int i = tid; i < nhist; i += blockDim.x) s_hist[i] = 0.0;
+    __syncthreads();
+  }
+  bin_rows<R, NT, XR, XD>(rows, nrows, G, b, inv1, inv2, inv3, amp, xcoef, hist, xhist, gnum,
+                          blockIdx.x * nwarps + warp, gridDim.x * nwarps, lane);
   if (SMEM) {
     __syncthreads();
     for (int i = tid; i < nhist; i += blockDim.x) {
@@ -574,6 +619,109 @@ __global__ void k_gather_modes(const typename Cplx<R>::T *__restrict__ G, BinGeo
       rho[2 * (t * nm + m)] = vx * cs - vy * sn;
       rho[2 * (t * nm + m) + 1] = vx * sn + vy * cs;
     }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Multi-system kernels of a batch: each frame stage runs for every system of
+// the batch in one launch.  Atoms, spread CTAs and bin CTAs are numbered
+// across the systems; a thread or CTA finds its system by binary search in the
+// batch's prefix sums and takes that system's geometry and buffers from the
+// BatchSys array.
+// ---------------------------------------------------------------------------
+
+// The s with pre[s] <= b < pre[s + 1] (pre[0] = 0, pre[nsys] > b).
+template <typename T>
+__device__ __forceinline__ int find_system(const T *pre, int nsys, T b) {
+  int lo = 0, hi = nsys;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (pre[mid] <= b) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+__global__ void k_batch_prep(const BatchSys *__restrict__ sys, int nsys,
+                             const int64_t *__restrict__ apre, int64_t natoms) {
+  __shared__ int64_t s_pre[MAX_BATCH_SYSTEMS + 1];
+  for (int i = threadIdx.x; i <= nsys; i += blockDim.x) s_pre[i] = apre[i];
+  __syncthreads();
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < natoms;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int s = find_system(s_pre, nsys, i);
+    const BatchSys &S = sys[s];
+    prep_atom(S.pos, S.species, S.g, S.counts, S.key, S.slot, i - s_pre[s]);
+  }
+}
+
+__global__ void __launch_bounds__(1024) k_batch_scan(const BatchSys *__restrict__ sys) {
+  const BatchSys &S = sys[blockIdx.x];
+  scan_counts(S.counts, S.starts, S.nkeys);
+}
+
+template <typename R>
+__global__ void k_batch_scatter(const BatchSys *__restrict__ sys, int nsys,
+                                const int64_t *__restrict__ apre, int64_t natoms) {
+  __shared__ int64_t s_pre[MAX_BATCH_SYSTEMS + 1];
+  for (int i = threadIdx.x; i <= nsys; i += blockDim.x) s_pre[i] = apre[i];
+  __syncthreads();
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < natoms;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int s = find_system(s_pre, nsys, i);
+    const BatchSys &S = sys[s];
+    scatter_atom<R>(S.pos, S.species, S.g, S.key, S.slot, S.starts, (R *)S.recs, nullptr,
+                    i - s_pre[s]);
+  }
+}
+
+// CTA b spreads tile (local % ntiles) of transform (local / ntiles) of its system.
+template <typename R>
+__global__ void __launch_bounds__(SPREAD_THREADS, sizeof(R) == 4 ? 2 : 1)
+    k_batch_spread(const BatchSys *__restrict__ sys, int nsys, const int *__restrict__ bpre) {
+  __shared__ FrameGeom s_g;
+  __shared__ int s_sys, s_local;
+  if (threadIdx.x == 0) {
+    const int s = find_system(bpre, nsys, (int)blockIdx.x);
+    s_sys = s;
+    s_local = (int)blockIdx.x - bpre[s];
+    s_g = sys[s].g;
+  }
+  __syncthreads();
+  const BatchSys &S = sys[s_sys];
+  spread_tile<R>((const R *)S.recs, S.starts, s_g, (const R *)S.strength, (R *)S.grid, nullptr,
+                 s_local % s_g.ntiles, s_local / s_g.ntiles);
+}
+
+// The CTAs of a system share its rows; each CTA bins into a shared histogram
+// of that system's nquant * nq sums and adds it to the system's accumulators.
+template <typename R, int NT, bool XR>
+__global__ void __launch_bounds__(256, 2)
+    k_batch_bin(const BatchSys *__restrict__ sys, int nsys, const int *__restrict__ bpre) {
+  extern __shared__ double s_hist[];
+  __shared__ BinGeom s_b;
+  __shared__ int s_sys, s_lb, s_nb;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nwarps = blockDim.x >> 5;
+  if (tid == 0) {
+    const int s = find_system(bpre, nsys, (int)blockIdx.x);
+    s_sys = s;
+    s_lb = (int)blockIdx.x - bpre[s];
+    s_nb = bpre[s + 1] - bpre[s];
+    s_b = sys[s].b;
+  }
+  __syncthreads();
+  const BatchSys &S = sys[s_sys];
+  const int nhist = s_b.nquant * s_b.nq;
+  for (int i = tid; i < nhist; i += blockDim.x) s_hist[i] = 0.0;
+  __syncthreads();
+  bin_rows<R, NT, XR, false>(S.rows, S.nrows, (const typename Cplx<R>::T *)S.G, s_b,
+                             (const R *)S.inv[0], (const R *)S.inv[1], (const R *)S.inv[2],
+                             S.amp, S.xcoef, s_hist, nullptr, S.gnum, s_lb * nwarps + warp,
+                             s_nb * nwarps, lane);
+  __syncthreads();
+  for (int i = tid; i < nhist; i += blockDim.x) {
+    const double v = s_hist[i];
+    if (v != 0.0) atomicAdd(&S.acc[i], v);
   }
 }
 
@@ -782,5 +930,93 @@ template cudaError_t launch_bin<double>(const int4 *, int, const void *, const B
                                         const double *, const double *, const double *,
                                         const double *, const double *, double *, double *, int,
                                         cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// Multi-system launches of a batch
+// ---------------------------------------------------------------------------
+template <typename R>
+cudaError_t launch_batch_sort(const BatchSys *sys, int nsys, const BatchPrefix &pre,
+                              int64_t natoms, cudaStream_t s) {
+  if (nsys < 1 || nsys > MAX_BATCH_SYSTEMS) return cudaErrorInvalidValue;
+  k_batch_prep<<<grid_for(natoms, 256), 256, 0, s>>>(sys, nsys, pre.atoms, natoms);
+  k_batch_scan<<<nsys, 1024, 0, s>>>(sys);
+  k_batch_scatter<R><<<grid_for(natoms, 256), 256, 0, s>>>(sys, nsys, pre.atoms, natoms);
+  return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_batch_spread(const BatchSys *sys, int nsys, const BatchPrefix &pre,
+                                int nblocks, int chunk, cudaStream_t s) {
+  if (nsys < 1 || nblocks < 1) return cudaErrorInvalidValue;
+  k_batch_spread<R><<<nblocks, SPREAD_THREADS, spread_smem_bytes(chunk, sizeof(R) == 8), s>>>(
+      sys, nsys, pre.spread);
+  return cudaGetLastError();
+}
+
+template <typename R, int NT>
+static cudaError_t batch_bin_nt(const BatchSys *sys, int nsys, const BatchPrefix &pre,
+                                int nblocks, bool xray, size_t smem, bool attr_only,
+                                cudaStream_t s) {
+  if (xray) {
+    if (attr_only)
+      return cudaFuncSetAttribute(k_batch_bin<R, NT, true>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_batch_bin<R, NT, true><<<nblocks, 256, smem, s>>>(sys, nsys, pre.bin);
+  } else {
+    if (attr_only)
+      return cudaFuncSetAttribute(k_batch_bin<R, NT, false>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_batch_bin<R, NT, false><<<nblocks, 256, smem, s>>>(sys, nsys, pre.bin);
+  }
+  return cudaGetLastError();
+}
+
+// attr_only: set the kernel's shared-memory limit (before any capture), launch nothing.
+template <typename R>
+static cudaError_t batch_bin(const BatchSys *sys, int nsys, const BatchPrefix &pre, int nblocks,
+                             int ntr, bool xray, int hist_max, bool attr_only, cudaStream_t s) {
+  const size_t smem = (size_t)hist_max * sizeof(double);
+  if (smem > 160 * 1024 || ntr < 1 || ntr > MAX_FAST_T) return cudaErrorInvalidValue;
+  switch (ntr) {
+    case 1: return batch_bin_nt<R, 1>(sys, nsys, pre, nblocks, xray, smem, attr_only, s);
+    case 2: return batch_bin_nt<R, 2>(sys, nsys, pre, nblocks, xray, smem, attr_only, s);
+    case 3: return batch_bin_nt<R, 3>(sys, nsys, pre, nblocks, xray, smem, attr_only, s);
+    case 4: return batch_bin_nt<R, 4>(sys, nsys, pre, nblocks, xray, smem, attr_only, s);
+    default: return batch_bin_nt<R, 0>(sys, nsys, pre, nblocks, xray, smem, attr_only, s);
+  }
+}
+
+template <typename R>
+cudaError_t launch_batch_bin(const BatchSys *sys, int nsys, const BatchPrefix &pre, int nblocks,
+                             int ntr, bool xray, int hist_max, cudaStream_t s) {
+  return batch_bin<R>(sys, nsys, pre, nblocks, ntr, xray, hist_max, false, s);
+}
+
+template <typename R>
+cudaError_t batch_set_attributes(int ntr, bool xray, int hist_max) {
+  int dev = 0, optin = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess)
+    e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (e == cudaSuccess) e = smem_optin(k_batch_spread<R>, optin);
+  BatchPrefix none{};
+  if (e == cudaSuccess) e = batch_bin<R>(nullptr, 0, none, 0, ntr, xray, hist_max, true, nullptr);
+  return e;
+}
+
+template cudaError_t launch_batch_sort<float>(const BatchSys *, int, const BatchPrefix &, int64_t,
+                                              cudaStream_t);
+template cudaError_t launch_batch_sort<double>(const BatchSys *, int, const BatchPrefix &,
+                                               int64_t, cudaStream_t);
+template cudaError_t launch_batch_spread<float>(const BatchSys *, int, const BatchPrefix &, int,
+                                                int, cudaStream_t);
+template cudaError_t launch_batch_spread<double>(const BatchSys *, int, const BatchPrefix &, int,
+                                                 int, cudaStream_t);
+template cudaError_t launch_batch_bin<float>(const BatchSys *, int, const BatchPrefix &, int, int,
+                                             bool, int, cudaStream_t);
+template cudaError_t launch_batch_bin<double>(const BatchSys *, int, const BatchPrefix &, int,
+                                              int, bool, int, cudaStream_t);
+template cudaError_t batch_set_attributes<float>(int, bool, int);
+template cudaError_t batch_set_attributes<double>(int, bool, int);
 
 }  // namespace sqn
