@@ -10,19 +10,20 @@
 namespace sqn {
 
 // Spread tile in fine-grid cells (x fastest).  A CTA of 16 warps owns one
-// 32 x 16 x 16 tile of ONE transform (grid y index = transform); warp k owns
+// 32 x 16 x 32 tile of ONE transform (grid y index = transform); warp k owns
 // the 8 x 4 (x, y) patch ((k % 4) * 8, (k / 4) * 4) of it and each lane keeps
-// the 16 z-cells of its (x, y) column in registers.  The bin sort keys points
-// by (transform, tile), so a CTA reads only the bins of its own transform.
+// 16 z-cells of its (x, y) column in registers, in two passes over the tile.
+// The bin sort keys points by (transform, tile), so a CTA reads only the bins
+// of its own transform.
 constexpr int TILE_X = 32;
 constexpr int TILE_Y = 16;
-constexpr int TILE_Z = 16;
+constexpr int TILE_Z = 32;
 constexpr int PATCH_X = 8;
 constexpr int PATCH_Y = 4;
 constexpr int SPREAD_WARPS = (TILE_X / PATCH_X) * (TILE_Y / PATCH_Y);  // 16
 constexpr int SPREAD_THREADS = 32 * SPREAD_WARPS;                       // 512
-// staged values per point: x row, y row, z row, 4 of padding (row pitch 68
-// values: consecutive rows start 4 banks apart)
+// staged values per point: x row, y row, z row, 4 of padding (row pitch 84
+// values: consecutive rows start 20 banks apart)
 constexpr int SPREAD_ROW = TILE_X + TILE_Y + TILE_Z + 4;
 static_assert((TILE_X & (TILE_X - 1)) == 0 && (TILE_Y & (TILE_Y - 1)) == 0 &&
                   (TILE_Z & (TILE_Z - 1)) == 0,
@@ -35,12 +36,12 @@ constexpr int MAX_W = 16;
 constexpr int MAX_BINS_DIM = 3;
 constexpr int MAX_NB = MAX_BINS_DIM * MAX_BINS_DIM * MAX_BINS_DIM;  // neighbour bins of a tile
 constexpr int MAX_FAST_T = 8;                  // species held in registers (k_bin)
-// Shape facts k_spread hard-codes (lane -> cell map, patch masks, 8-wide z
-// halves, 16-byte aligned staged rows).
+// Shape facts k_spread hard-codes (lane -> cell map, patch masks, 8-cell z
+// groups, 16-byte aligned staged rows).
 static_assert(TILE_X / PATCH_X == 4 && PATCH_X == 8 && PATCH_Y == 4,
               "k_spread maps warp & 3 / lane & 7 / lane >> 3 onto the patches");
-static_assert(4 + TILE_Y / PATCH_Y <= 8, "patch mask bits 0-7, z-half bits 8-9");
-static_assert(TILE_Z == 16, "two 8-cell z halves per lane");
+static_assert(4 + TILE_Y / PATCH_Y <= 8, "patch mask bits 0-7, z-group bits 8-11");
+static_assert(TILE_Z == 32, "two passes of two 8-cell z groups per lane");
 static_assert((TILE_X + TILE_Y) % 4 == 0 && SPREAD_ROW % 4 == 0,
               "staged rows and their z part are 16-byte aligned");
 static_assert(MAX_W - 1 < TILE_X && MAX_W - 1 < TILE_Y && MAX_W - 1 < TILE_Z,

@@ -212,20 +212,24 @@ __device__ __forceinline__ unsigned group_mask(int r, int w, int len, int n) {
 }
 
 // ---------------------------------------------------------------------------
-// Gather spreading, one CTA per (32 x 16 x 16 tile, transform).
+// Gather spreading, one CTA per (32 x 16 x 32 tile, transform).
 // The CTA lists the bins of its transform that can reach the tile (at most 3
 // per dimension), loads their point records, keeps the points whose support
-// meets the tile (compacted with one shared atomic per warp) and stages for
-// each its kernel values already shifted onto the tile's cells (32 x, 16 y,
-// 16 z with the strength folded in; zero where the support does not reach),
-// with a mask of the 8 x 4 patches and the two 8-cell z halves it reaches.  A
-// warp's visit of a point is then two scalar loads, a multiply, and per z half
-// that the point reaches two vector loads and four packed FMAs per lane.
-// Every cell of the tile is written exactly once: no zeroing, no atomics.
+// meets the tile (in candidate order: warp counts, then a prefix over the
+// warps) and stages for each its kernel values already shifted onto the
+// tile's cells (32 x, 16 y, 32 z with the strength folded in; zero where the
+// support does not reach), with a mask of the 8 x 4 patches and of the four
+// 8-cell z groups it reaches.  The tile is then accumulated in two passes of
+// 16 z cells (16 registers per lane): a warp's visit of a point is two scalar
+// loads, a multiply, and per z group of the pass that the point reaches two
+// vector loads and four packed FMAs per lane.  The staging serves both passes
+// when the tile's points fit the shared-memory capacity (g.chunk points);
+// otherwise the points are staged in windows of that many, per pass.  Every
+// cell of the tile is written exactly once: no zeroing, no atomics.
 // ptw != nullptr (one grid per y index, g.ntr == 1): the weight of a point is
 // ptw[y * natoms + record index] instead of strength[species].
 // ---------------------------------------------------------------------------
-constexpr unsigned ZLO = 1u << 8, ZHI = 1u << 9;
+constexpr int ZPASS = 16;  // z cells per accumulation pass
 
 template <typename R>
 __device__ __forceinline__ void spread_tile(const R *__restrict__ recs,
@@ -233,18 +237,18 @@ __device__ __forceinline__ void spread_tile(const R *__restrict__ recs,
                                             const R *__restrict__ strength, R *__restrict__ grid,
                                             const R *__restrict__ ptw, const int tile,
                                             const int tr) {
-  const int chunk = g.chunk;
+  const int cap = g.chunk;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  R *s_rows = reinterpret_cast<R *>(smem_raw);                        // [chunk][SPREAD_ROW]
-  R *s_off = s_rows + (size_t)chunk * SPREAD_ROW;                      // [chunk][4]
-  int4 *s_meta = reinterpret_cast<int4 *>(s_off + (size_t)chunk * 4);  // [chunk]
-  unsigned *s_mask = reinterpret_cast<unsigned *>(s_meta + chunk);     // [chunk]
+  R *s_rows = reinterpret_cast<R *>(smem_raw);                      // [cap][SPREAD_ROW]
+  R *s_off = s_rows + (size_t)cap * SPREAD_ROW;                      // [cap][4]
+  int4 *s_meta = reinterpret_cast<int4 *>(s_off + (size_t)cap * 4);  // [cap]
+  unsigned *s_mask = reinterpret_cast<unsigned *>(s_meta + cap);     // [cap]
   __shared__ int s_bstart[MAX_NB];
   __shared__ int s_bpref[MAX_NB + 1];
   __shared__ int s_borg[MAX_NB][3];
   __shared__ int s_bl[3][MAX_BINS_DIM];
   __shared__ int s_nbl[3];
-  __shared__ int s_nkept;
+  __shared__ int s_wcount[SPREAD_WARPS];
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int cx = (warp & 3) * PATCH_X + (lane & 7);   // this lane's x cell in the tile
@@ -313,124 +317,143 @@ __device__ __forceinline__ void spread_tile(const R *__restrict__ recs,
   __syncthreads();
   const int total = s_bpref[nb];
 
-  R acc[TILE_Z];
-#pragma unroll
-  for (int z = 0; z < TILE_Z; ++z) acc[z] = R(0);
   const unsigned xbit = 1u << (warp & 3), ybit = 1u << (4 + (warp >> 2));
   const R halfw = R(0.5) * (R)w - R(0.5);
   const R c2 = R(4) / ((R)w * (R)w);
   const R beta = (R)g.beta;
+  int kept = -1;  // points of the tile (after the first staging)
+  int npts = 0;   // points staged in the current window
+  R acc[ZPASS];
 
-  for (int base = 0; base < total; base += chunk) {
-    if (tid == 0) s_nkept = 0;
-    __syncthreads();  // the previous pass's visits have read the rows
-    // 1. candidates whose support meets the tile, compacted
-    const int i = base + tid;
-    bool keep = false;
-    int4 meta = make_int4(0, 0, 0, 0);
-    unsigned mask = 0u;
-    R rec[REC_SLOTS];
-    if (tid < chunk && i < total) {
-      // bin of candidate i: s_bpref[b] <= i < s_bpref[b + 1]
-      int lo = 0, hi = nb;
-      while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (s_bpref[mid] <= i) lo = mid; else hi = mid;
-      }
-      const int ridx = s_bstart[lo] + (i - s_bpref[lo]);
-      load_rec(recs + (int64_t)ridx * REC_SLOTS, rec);
-      const uint32_t packed = unpack_rec<R>(rec[0]);
-      int rx = s_borg[lo][0] + (int)(packed & 255u) - X0;
-      int ry = s_borg[lo][1] + (int)((packed >> 8) & 255u) - Y0;
-      int rz = s_borg[lo][2] + (int)((packed >> 16) & 255u) - Z0;
-      if (rx < 0) rx += g.nf[0];
-      if (ry < 0) ry += g.nf[1];
-      if (rz < 0) rz += g.nf[2];
-      keep = (rx < tx || rx + w > g.nf[0]) && (ry < ty || ry + w > g.nf[1]) &&
-             (rz < tz || rz + w > g.nf[2]);
-      if (keep) {
-        mask = group_mask<PATCH_X>(rx, w, tx, g.nf[0]) |
-               (group_mask<PATCH_Y>(ry, w, ty, g.nf[1]) << 4) |
-               (group_mask<8>(rz, w, tz, g.nf[2]) << 8);
-        // with per-point weights the slot carries the record index
-        meta = make_int4(rx, ry, rz, ptw ? ridx : (int)(packed >> 24));
-      }
-    }
-    const unsigned bal = __ballot_sync(FULL, keep);
-    int wbase = 0;
-    if (lane == 0 && bal) wbase = atomicAdd(&s_nkept, __popc(bal));
-    wbase = __shfl_sync(FULL, wbase, 0);
-    if (keep) {
-      const int p = wbase + __popc(bal & ((1u << lane) - 1u));
-      s_meta[p] = meta;
-      s_mask[p] = mask;
-      store_rec(s_off + (size_t)p * 4, R(0), rec[1], rec[2], rec[3]);
-    }
-    __syncthreads();
-    const int npts = s_nkept;
-
-    // 2. kernel values shifted onto the tile's cells: row c of point p holds
-    //    phi at tile cell c (x: c < 32, y: next 16, z: next 16, times the
-    //    weight), zero outside the support or the grid.  One thread per
-    //    (point, axis) clears its row and writes the w support values that
-    //    fall in the tile (the same thread, so no barrier between the two).
-    for (int e = tid; e < 3 * npts; e += SPREAD_THREADS) {
-      const int d = e >= 2 * npts ? 2 : (e >= npts ? 1 : 0);
-      const int p = e - d * npts;
-      const int4 m = s_meta[p];
-      const int rel = d == 0 ? m.x : (d == 1 ? m.y : m.z);
-      const int len = d == 0 ? TILE_X : (d == 1 ? TILE_Y : TILE_Z);
-      const int lim = d == 0 ? tx : (d == 1 ? ty : tz);
-      const int n = g.nf[d];
-      const R off = s_off[(size_t)p * 4 + 1 + d];
-      const R sc = d == 2 ? (ptw ? ptw[m.w] : strength[m.w]) : R(1);
-      R *row = s_rows + (size_t)p * SPREAD_ROW + (d == 0 ? 0 : (d == 1 ? TILE_X : TILE_X + TILE_Y));
-      for (int j = 0; j < len; j += 4) store_rec(row + j, R(0), R(0), R(0), R(0));
-      // support cell k sits at tile cell rel + k, cyclically (rel in [0, n))
-      for (int k = 0; k < w; ++k) {
-        int cell = rel + k;
-        if (cell >= n) cell -= n;
-        if (cell < lim) row[cell] = es_at(k, off, halfw, c2, beta) * sc;
-      }
-    }
-    __syncthreads();
-
-    // 3. each warp walks only the points that reach its patch
-    for (int pb = 0; pb < npts; pb += 32) {
-      const int p = pb + lane;
-      unsigned m = 0u;
-      if (p < npts) m = s_mask[p];
-      unsigned am = __ballot_sync(FULL, (m & xbit) && (m & ybit));
-      while (am) {
-        const int src = __ffs(am) - 1;
-        am &= am - 1u;
-        const unsigned zm = __shfl_sync(FULL, m, src);
-        const R *row = s_rows + (size_t)(pb + src) * SPREAD_ROW;
-        const R a = row[cx] * row[TILE_X + cy];
-        const R *zr = row + TILE_X + TILE_Y;
-        if (zm & ZLO) {
-          R z[8];
-          load_z8(zr, z);
+  for (int h = 0; h * ZPASS < tz; ++h) {
 #pragma unroll
-          for (int k = 0; k < 8; k += 2) fma2(a, z[k], z[k + 1], acc[k], acc[k + 1]);
+    for (int z = 0; z < ZPASS; ++z) acc[z] = R(0);
+    for (int win = 0;; win += cap) {
+      if (!(h > 0 && kept <= cap)) {
+        // ---- stage the kept points win .. win + cap - 1 (candidate order)
+        __syncthreads();  // the previous visits have read the rows
+        int kbase = 0;
+        for (int cb = 0; cb < total; cb += SPREAD_THREADS) {
+          const int i = cb + tid;
+          bool keep = false;
+          int4 meta = make_int4(0, 0, 0, 0);
+          unsigned mask = 0u;
+          R rec[REC_SLOTS];
+          if (i < total) {
+            // bin of candidate i: s_bpref[b] <= i < s_bpref[b + 1]
+            int lo = 0, hi = nb;
+            while (hi - lo > 1) {
+              const int mid = (lo + hi) >> 1;
+              if (s_bpref[mid] <= i) lo = mid; else hi = mid;
+            }
+            const int ridx = s_bstart[lo] + (i - s_bpref[lo]);
+            load_rec(recs + (int64_t)ridx * REC_SLOTS, rec);
+            const uint32_t packed = unpack_rec<R>(rec[0]);
+            int rx = s_borg[lo][0] + (int)(packed & 255u) - X0;
+            int ry = s_borg[lo][1] + (int)((packed >> 8) & 255u) - Y0;
+            int rz = s_borg[lo][2] + (int)((packed >> 16) & 255u) - Z0;
+            if (rx < 0) rx += g.nf[0];
+            if (ry < 0) ry += g.nf[1];
+            if (rz < 0) rz += g.nf[2];
+            keep = (rx < tx || rx + w > g.nf[0]) && (ry < ty || ry + w > g.nf[1]) &&
+                   (rz < tz || rz + w > g.nf[2]);
+            if (keep) {
+              mask = group_mask<PATCH_X>(rx, w, tx, g.nf[0]) |
+                     (group_mask<PATCH_Y>(ry, w, ty, g.nf[1]) << 4) |
+                     (group_mask<8>(rz, w, tz, g.nf[2]) << 8);
+              // with per-point weights the slot carries the record index
+              meta = make_int4(rx, ry, rz, ptw ? ridx : (int)(packed >> 24));
+            }
+          }
+          const unsigned bal = __ballot_sync(FULL, keep);
+          if (lane == 0) s_wcount[warp] = __popc(bal);
+          __syncthreads();
+          int woff = 0, btot = 0;
+#pragma unroll
+          for (int k = 0; k < SPREAD_WARPS; ++k) {
+            const int c = s_wcount[k];
+            woff += k < warp ? c : 0;
+            btot += c;
+          }
+          const int k = kbase + woff + __popc(bal & ((1u << lane) - 1u)) - win;
+          if (keep && k >= 0 && k < cap) {
+            s_meta[k] = meta;
+            s_mask[k] = mask;
+            store_rec(s_off + (size_t)k * 4, R(0), rec[1], rec[2], rec[3]);
+          }
+          kbase += btot;
+          __syncthreads();  // s_wcount is reused by the next batch
         }
-        if (zm & ZHI) {
-          R z[8];
-          load_z8(zr + 8, z);
+        kept = kbase;
+        npts = min(cap, kept - win);
+
+        // kernel values shifted onto the tile's cells: row c of point p holds
+        // phi at tile cell c (x: c < 32, y: next 16, z: next 32, times the
+        // weight), zero outside the support or the grid.  One thread per
+        // (point, axis) clears its row and writes the w support values that
+        // fall in the tile (the same thread, so no barrier between the two).
+        for (int e = tid; e < 3 * npts; e += SPREAD_THREADS) {
+          const int d = e >= 2 * npts ? 2 : (e >= npts ? 1 : 0);
+          const int p = e - d * npts;
+          const int4 m = s_meta[p];
+          const int rel = d == 0 ? m.x : (d == 1 ? m.y : m.z);
+          const int len = d == 0 ? TILE_X : (d == 1 ? TILE_Y : TILE_Z);
+          const int lim = d == 0 ? tx : (d == 1 ? ty : tz);
+          const int n = g.nf[d];
+          const R off = s_off[(size_t)p * 4 + 1 + d];
+          const R sc = d == 2 ? (ptw ? ptw[m.w] : strength[m.w]) : R(1);
+          R *row = s_rows + (size_t)p * SPREAD_ROW +
+                   (d == 0 ? 0 : (d == 1 ? TILE_X : TILE_X + TILE_Y));
+          for (int j = 0; j < len; j += 4) store_rec(row + j, R(0), R(0), R(0), R(0));
+          // support cell k sits at tile cell rel + k, cyclically (rel in [0, n))
+          for (int k = 0; k < w; ++k) {
+            int cell = rel + k;
+            if (cell >= n) cell -= n;
+            if (cell < lim) row[cell] = es_at(k, off, halfw, c2, beta) * sc;
+          }
+        }
+        __syncthreads();
+      }
+
+      // ---- each warp walks only the points that reach its patch in this pass
+      const unsigned zsel = 3u << (8 + 2 * h);
+      for (int pb = 0; pb < npts; pb += 32) {
+        const int p = pb + lane;
+        unsigned m = 0u;
+        if (p < npts) m = s_mask[p];
+        unsigned am = __ballot_sync(FULL, (m & xbit) && (m & ybit) && (m & zsel));
+        while (am) {
+          const int src = __ffs(am) - 1;
+          am &= am - 1u;
+          const unsigned zm = __shfl_sync(FULL, m, src) >> (8 + 2 * h);
+          const R *row = s_rows + (size_t)(pb + src) * SPREAD_ROW;
+          const R a = row[cx] * row[TILE_X + cy];
+          const R *zr = row + TILE_X + TILE_Y + h * ZPASS;
+          if (zm & 1u) {
+            R z[8];
+            load_z8(zr, z);
 #pragma unroll
-          for (int k = 0; k < 8; k += 2) fma2(a, z[k], z[k + 1], acc[8 + k], acc[9 + k]);
+            for (int k = 0; k < 8; k += 2) fma2(a, z[k], z[k + 1], acc[k], acc[k + 1]);
+          }
+          if (zm & 2u) {
+            R z[8];
+            load_z8(zr + 8, z);
+#pragma unroll
+            for (int k = 0; k < 8; k += 2) fma2(a, z[k], z[k + 1], acc[8 + k], acc[9 + k]);
+          }
         }
       }
+      if (win + cap >= kept) break;
     }
-  }
 
-  if (cx < tx && cy < ty) {
-    const int64_t zs = (int64_t)g.nf[1] * g.pitch;
-    R *out = grid + (int64_t)tr * g.vol_real + ((int64_t)Z0 * g.nf[1] + (Y0 + cy)) * g.pitch +
-             X0 + cx;
+    if (cx < tx && cy < ty) {
+      const int64_t zs = (int64_t)g.nf[1] * g.pitch;
+      R *out = grid + (int64_t)tr * g.vol_real +
+               ((int64_t)(Z0 + h * ZPASS) * g.nf[1] + (Y0 + cy)) * g.pitch + X0 + cx;
 #pragma unroll
-    for (int z = 0; z < TILE_Z; ++z)
-      if (z < tz) out[z * zs] = acc[z];
+      for (int z = 0; z < ZPASS; ++z)
+        if (h * ZPASS + z < tz) out[z * zs] = acc[z];
+    }
   }
 }
 
