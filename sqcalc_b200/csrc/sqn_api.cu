@@ -617,7 +617,7 @@ int setup_plan(sqn_plan *p, const sqn_plan_desc *d) {
 
   // --- tiles ---------------------------------------------------------------
   FrameGeom &g = p->fg;
-  const int tmax[3] = {TILE_X, TILE_Y, TILE_Z};
+  const int tmax[3] = {TILE_X, TILE_Y, spread_tile_z(p->nf, p->ntr, p->nsm)};
   for (int i = 0; i < 3; ++i) {
     g.nf[i] = (int)p->nf[i];
     g.tile[i] = (int)std::min<int64_t>(tmax[i], p->nf[i]);

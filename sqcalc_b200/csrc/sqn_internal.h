@@ -47,6 +47,16 @@ static_assert((TILE_X + TILE_Y) % 4 == 0 && SPREAD_ROW % 4 == 0,
 static_assert(MAX_W - 1 < TILE_X && MAX_W - 1 < TILE_Y && MAX_W - 1 < TILE_Z,
               "a tile's bin list per dimension fits MAX_BINS_DIM for every w <= MAX_W");
 static_assert(MAX_NB <= 32, "one bin per lane in the bin-list prefix");
+static_assert(MAX_W - 1 < TILE_Z / 2, "the half-depth tiles of small grids keep <= 3 bins too");
+
+// z extent of the spread tiles of a fine grid: TILE_Z (two accumulation passes
+// over one staging of the points) when the grids still give at least 4 CTAs
+// per SM, else TILE_Z / 2 (one pass; small grids keep twice the CTAs).
+inline int spread_tile_z(const int64_t *nf, int ngrids, int nsm) {
+  const int64_t nxy = ((nf[0] + TILE_X - 1) / TILE_X) * ((nf[1] + TILE_Y - 1) / TILE_Y);
+  const int64_t ctas = nxy * ((nf[2] + TILE_Z - 1) / TILE_Z) * (int64_t)ngrids;
+  return ctas >= 4 * (int64_t)nsm ? TILE_Z : TILE_Z / 2;
+}
 
 // Point records written by the bin sort and read by the spread and
 // interpolation kernels: four R-sized slots per atom,

@@ -116,7 +116,14 @@ extern "C" int sqn_spread_frame_noalloc(const double *pos, int64_t natoms,
   I(3, 3) = (M(1, 1) * M(2, 2) - M(1, 2) * M(2, 1));
   for (int k = 0; k < 9; ++k) g.inv[k] = inv[k] / det;
   std::memcpy(g.origin, origin, sizeof(g.origin));
-  const int tmax[3] = {TILE_X, TILE_Y, TILE_Z};
+  // the same spread tiles a plan of this grid uses (they depend on the SM count)
+  int dev = 0, nsm = 148;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+    cudaGetLastError();
+    return SQN_ERR_NO_DEVICE;
+  }
+  const int tmax[3] = {TILE_X, TILE_Y, spread_tile_z(nf, ntr, nsm)};
   for (int d = 0; d < 3; ++d) {
     g.nf[d] = (int)nf[d];
     g.tile[d] = (int)(nf[d] < tmax[d] ? nf[d] : tmax[d]);

@@ -237,7 +237,10 @@ int make_type1(int type, int dim, const int64_t *n_modes, int iflag, int ntransf
   for (int k = 0; k < 9; ++k) g.inv[k] = 0.0;
   g.inv[0] = g.inv[4] = g.inv[8] = 1.0 / two_pi;
   for (int d = 0; d < 3; ++d) g.origin[d] = -0.5 * two_pi;
-  const int tmax[3] = {TILE_X, TILE_Y, TILE_Z};
+  int nsm = 148;
+  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, p->device) != cudaSuccess)
+    return fail(SQN_ERR_CUDA);
+  const int tmax[3] = {TILE_X, TILE_Y, spread_tile_z(p->nf, 2 * p->ntr, nsm)};
   for (int d = 0; d < 3; ++d) {
     g.nf[d] = (int)p->nf[d];
     g.tile[d] = (int)std::min<int64_t>(p->nf[d], tmax[d]);
