@@ -589,7 +589,9 @@ def grad_leg(W, K, stream, dist, local_rank):
     N = 1e5, 2 types 1:2, loss sum_shells (S - S_target)^2 over q in [0.5, 8],
     S_target from a copy displaced by N(0, 0.2^2).  One evaluation = one
     sqn_sq_grad call with dL/dS: the weighted forward transform recomputed,
-    three type-2 interpolations, S and the FP64 gradient returned."""
+    three type-2 interpolations, S and the FP64 gradient returned.  Each plan's
+    fine grid and kernel width are chosen by the autotuner, timing the gradient
+    evaluation itself."""
     import torch
     from sqcalc_b200 import _lib
 
@@ -608,7 +610,8 @@ def grad_leg(W, K, stream, dist, local_rank):
     for name, prec, eps in (("f32+f64acc", _lib.PREC_SINGLE, 1e-6), ("f64", _lib.PREC_DOUBLE, 1e-10)):
         with _lib.Plan(np.eye(3).reshape(9) * GRAD_BOX, np.zeros(3), types, qmin=GRAD_QMIN,
                        qmax=GRAD_QMAX, nq=GRAD_NQ, partials=False, precision=prec, eps=eps,
-                       device=local_rank, stream=stream.cuda_stream, grad=True) as p:
+                       device=local_rank, stream=stream.cuda_stream, grad=True,
+                       autotune=True) as p:
             S_t, _ = p.sq_grad(target_pos)
             S, _ = p.sq_grad(d)
             dLdS = 2.0 * (S - S_t)
@@ -626,7 +629,7 @@ def grad_leg(W, K, stream, dist, local_rank):
             grads[name] = g.cpu().numpy()
             out[name] = {"value": k / t, "ms_per_eval": 1e3 * t / k, "eps": eps, "steps": k,
                          "modes": list(p.modes), "fine_grid": list(p.info.nf),
-                         "kernel_width": p.info.kernel_width,
+                         "kernel_width": p.info.kernel_width, "autotuned": bool(p.info.autotuned),
                          "gpu_launches_per_eval": (p.launch_count() - l0) / k}
     # The headline is the FP64 adjoint: within 1e-6 relative of the FP64
     # direct-sum gradient (tests/test_gpu_grad.py measures ~1e-13).  The FP32

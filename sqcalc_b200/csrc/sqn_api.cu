@@ -450,6 +450,19 @@ int autotune_grid(sqn_plan *p, const sqn_plan_desc *d, double eps, TuneResult *o
                    cudaSuccess
                ? SQN_OK
                : SQN_ERR_CUDA;
+  // dS/dr plans are timed on their gradient evaluation (forward recomputed,
+  // three type-2 interpolations), the others on frame accumulation
+  const bool grad = (d->flags & SQN_FLAG_GRAD) != 0;
+  std::vector<double> ones((size_t)d->nq, 1.0), S((size_t)d->nq);
+  double *dgrad = nullptr;
+  if (st == SQN_OK && grad && cudaMalloc(&dgrad, sizeof(double) * 3 * (size_t)N) != cudaSuccess) {
+    cudaGetLastError();
+    st = SQN_ERR_ALLOC;
+  }
+  auto run = [&](sqn_plan *sp) {
+    return grad ? sqn_sq_grad(sp, dpos, SQN_DEVICE, ones.data(), S.data(), dgrad)
+                : sqn_accumulate_frames(sp, dpos, 1, SQN_DEVICE);
+  };
   TuneResult best{0.0, 0, 0, 1e300};
   constexpr int kFrames = 3;
   for (size_t c = 0; c < cand.size() && st == SQN_OK; ++c) {
@@ -459,12 +472,11 @@ int autotune_grid(sqn_plan *p, const sqn_plan_desc *d, double eps, TuneResult *o
     sd.kernel_width = cand[c].second;
     sqn_plan *sp = nullptr;
     if (sqn_plan_create(&sd, &sp) > SQN_WARN_EPS_TOO_SMALL || !sp) continue;  // e.g. no memory
-    int rc = sqn_accumulate_frames(sp, dpos, 1, SQN_DEVICE);
+    int rc = run(sp);
     if (rc == SQN_OK) rc = sqn_sync(sp);
     float ms = 0.f;
     if (rc == SQN_OK && cudaEventRecord(e0, sp->stream) == cudaSuccess) {
-      for (int f = 0; f < kFrames && rc == SQN_OK; ++f)
-        rc = sqn_accumulate_frames(sp, dpos, 1, SQN_DEVICE);
+      for (int f = 0; f < kFrames && rc == SQN_OK; ++f) rc = run(sp);
       if (rc == SQN_OK && (cudaEventRecord(e1, sp->stream) != cudaSuccess ||
                            cudaEventSynchronize(e1) != cudaSuccess ||
                            cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
@@ -482,6 +494,7 @@ int autotune_grid(sqn_plan *p, const sqn_plan_desc *d, double eps, TuneResult *o
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   cudaFree(dpos);
+  if (dgrad) cudaFree(dgrad);
   if (st != SQN_OK) return st;
   if (best.ms >= 1e300) return SQN_ERR_ALLOC;
   best.ncand = (int)cand.size();

@@ -35,3 +35,24 @@ def test_autotuned_plan_meets_the_bar_and_caches():
     with _lib.Plan(cell, np.zeros(3), tid, **kw) as q:
         assert q.info.autotuned == 1 and q.info.tune_candidates == 0  # from the cache
         assert (tuple(q.info.nf), q.info.kernel_width) == chosen
+
+
+def test_autotuned_gradient_plan_meets_the_bar():
+    """A dS/dr plan tuned on its gradient evaluation: FP64 gradient within 1e-6
+    relative of the FP64 direct-sum gradient (the differentiation form's bar)."""
+    rng = np.random.default_rng(17)
+    n, box = 2000, 30.0
+    types = np.repeat([1, 2], [n // 3, n - n // 3]).astype(np.int32)
+    rng.shuffle(types)
+    pos = rng.random((n, 3)) * box
+    with _lib.Plan(np.eye(3).reshape(9) * box, np.zeros(3), types, qmin=0.5, qmax=8.0, nq=150,
+                   norm=_lib.NORM_MEAN, partials=True, precision=_lib.PREC_DOUBLE, eps=1e-12,
+                   grad=True, autotune=True) as plan:
+        assert plan.info.autotuned == 1
+        dLdS = rng.standard_normal(plan.nq)
+        _, g = plan.sq_grad(pos, dLdS)
+        den = plan.accumulators()["den"]
+    grid = O.configure_grid(np.eye(3) * box, 0.5, 8.0, 150)
+    wgt = np.where(den > 0, dLdS / np.where(den > 0, den, 1.0), 0.0)
+    ref = O.direct_grad(pos, np.ones(n), np.eye(3) * box, np.zeros(3), grid, wgt)
+    assert np.max(np.abs(g - ref)) / np.max(np.abs(ref)) < 1e-6
