@@ -3,7 +3,9 @@
 Mirrors the option surface and exit codes of ``sqcalc static --device gpu``
 (app/main.f90:41-259, src/sqc_options.f90:330-600) for the hot path only:
 -i -m -w --norm --partials/--no-partials -fz --grid --precision --eps --qmin
---qmax --nq --device --gpu-id, output file (``-`` for stdout).
+--qmax --nq --device --gpu-id --xrd --format, output file (``-`` for stdout).
+A --grid or --xrd file named ``.h5``/``.hdf5`` (or any name under
+``--format hdf5``) is written as HDF5 (src/sqc_hdf5.f90) by ``h5file``.
 """
 from __future__ import annotations
 
@@ -14,7 +16,7 @@ import sys
 import time
 
 
-from . import _lib
+from . import _lib, h5file
 from .cell import Cell
 from .dump import Frame
 from .static import GpuStructureFactor, SqcalcError
@@ -49,6 +51,7 @@ def parse(argv):
     lp.add_argument("--lp", dest="lp", action="store_true", default=None)
     lp.add_argument("--no-lp", dest="lp", action="store_false")
     p.add_argument("--nq", type=int, default=500)
+    p.add_argument("--format", default=None)
     p.add_argument("--device", default="gpu", choices=["gpu", "cuda"])
     p.add_argument("--gpu-id", type=int, default=0)
     p.add_argument("--method", default="nufft", choices=["nufft", "finufft"])
@@ -66,6 +69,13 @@ def main(argv=None):
         a = parse(argv[1:])
     except SystemExit as e:
         sys.exit(2 if e.code else 0)
+    # --format (src/sqc_options.f90:556-567)
+    if a.format is not None:
+        fmt = {"text": "text", "txt": "text", "ascii": "text",
+               "hdf5": "hdf5", "h5": "hdf5", "hdf": "hdf5"}.get(a.format)
+        if fmt is None:
+            _die(2, 'unknown format "%s" (use text or hdf5)' % a.format)
+        a.format = fmt
     # --xrd and its settings (src/sqc_options.f90:620-658)
     xrd = None
     if a.xrd is not None:
@@ -136,12 +146,25 @@ def main(argv=None):
     method.plan.sync()
     if not a.quiet:
         sys.stderr.write("  frames     : %d in %.3f s\n" % (n, time.time() - t0))
+    # app/main.f90:390-488: text tables first, then the HDF5 files.
+    grid_h5 = a.grid is not None and h5file.wants_hdf5(a.grid, a.format)
+    xrd_h5 = a.xrd is not None and h5file.wants_hdf5(a.xrd, a.format)
     try:
-        method.write_results(a.output, a.grid)
-        if a.xrd is not None:
+        method.write_results(a.output, None if grid_h5 else a.grid)
+        if a.xrd is not None and not xrd_h5:
             method.write_xrd(a.xrd)
     except OSError as e:
         _die(11, str(e))
+    if xrd_h5:
+        try:
+            method.write_xrd_hdf5(a.xrd)
+        except h5file.H5Error as e:
+            _die(21, str(e))
+    if grid_h5:
+        try:
+            method.write_hdf5(a.grid)
+        except h5file.H5Error as e:
+            _die(18, str(e))
     method.close()
 
 

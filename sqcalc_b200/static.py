@@ -16,7 +16,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from . import _lib
+from . import _lib, h5file
 from .cell import Cell
 from .weights import WEIGHT_NEUTRON, WEIGHT_XRAY, WeightScheme
 
@@ -26,6 +26,11 @@ PRECISION_NAMES = {"double": _lib.PREC_DOUBLE, "float64": _lib.PREC_DOUBLE,
                    "f64": _lib.PREC_DOUBLE, "single": _lib.PREC_SINGLE,
                    "float": _lib.PREC_SINGLE, "float32": _lib.PREC_SINGLE,
                    "f32": _lib.PREC_SINGLE}
+
+
+# scheme_label (src/sqc_weights.f90:176-187)
+WEIGHT_LABELS = {WEIGHT_NEUTRON: "neutron bound coherent scattering lengths",
+                 WEIGHT_XRAY: "X-ray atomic form factors f(q)"}
 
 
 class SqcalcError(Exception):
@@ -204,6 +209,99 @@ class GpuStructureFactor:
                     q = kept.qvec[i]
                     fh.write("%14.8f  %14.8f  %14.8f  %s\n" % (q[0], q[1], q[2], fortran_es(Sg[i])))
         return S, Sp, Sg
+
+    # --- HDF5 results (src/sqc_hdf5.f90) ------------------------------------
+    def pair_list(self):
+        """(a, b, label) of every pair of present types, a <= b, in the order of
+        write_shell_partials (src/sqc_hdf5.f90:1322-1352)."""
+        out = []
+        for t in range(1, self.ntypes + 1):
+            for u in range(t, self.ntypes + 1):
+                if self.type_counts[t - 1] == 0 or self.type_counts[u - 1] == 0:
+                    continue
+                out.append((t, u, self.scheme.pair_label(t, u)))
+        return out
+
+    def _run_attrs(self, root):
+        """The run attributes of hdf5_write_results (src/sqc_hdf5.f90:86-131)."""
+        root.attr("nframes", int(self.nframes))
+        root.attr("natoms", int(self.natoms))
+        root.attr("nmodes", int(self.nmodes))
+        root.attr("nq", int(self.nq))
+        root.attr("qmin", float(self.qmin))
+        root.attr("qmax", float(self.qmax))
+        root.attr("eps", float(self.eps))
+        root.attr("cell", np.asarray(self.cell.a, dtype=np.float64).reshape(3, 3))
+        root.attr("weight", WEIGHT_LABELS.get(self.scheme.kind, "unit weights"))
+        root.attr("norm", {_lib.NORM_SELF: "self", _lib.NORM_NATOM: "n"}.get(self.norm, "mean"))
+        root.attr("device", "gpu")
+        root.attr("precision", "single" if self.precision == _lib.PREC_SINGLE else "double")
+        mapping = ",".join("%d:%s" % (t, self.scheme.species[t])
+                           for t in range(1, self.scheme.mapped_types() + 1)
+                           if self.scheme.species.get(t, ""))
+        root.attr("mapping", mapping)
+
+    def write_hdf5(self, path):
+        """hdf5_write_results (src/sqc_hdf5.f90:46-210): the run attributes,
+        /shell/{q,S,count} (+ /shell/S_partial/<pair>, /shell/pairs and the
+        partial_normalization attribute) and, with --grid, /grid/{qx,qy,qz,S,h,k,l}."""
+        S, Sp, Sg, _ = self.results()
+        acc = self.plan.accumulators()
+        root = h5file.Group()
+        self._run_attrs(root)
+        shell = root.group("shell")
+        shell.dataset("q", np.array([self.q_of_shell(s) for s in range(self.nq)]))
+        shell.dataset("S", np.asarray(S, dtype=np.float64))
+        shell.dataset("count", np.asarray(acc["shell_count"], dtype=np.int64))
+        pairs = self.pair_list() if self.partials else []
+        if pairs and self.nq > 0:
+            sp = shell.group("S_partial")
+            for t, u, lab in pairs:
+                sp.dataset(lab, np.asarray(Sp[t - 1, u - 1, :], dtype=np.float64))
+            shell.dataset("pairs", [lab for _, _, lab in pairs], strlen=18)
+            shell.attr("partial_normalization", "faber-ziman" if self.faber_ziman else "ovito")
+        if self.want_grid:
+            kept = enumerate_modes(self.cell, self.modes, self.qmin, self.qmax)
+            grid = root.group("grid")
+            for r, name in enumerate(("qx", "qy", "qz")):
+                grid.dataset(name, kept.qvec[:, r])
+            grid.dataset("S", np.asarray(Sg, dtype=np.float64))
+            for r, name in enumerate(("h", "k", "l")):
+                grid.dataset(name, kept.hkl[:, r].astype(np.int32))
+        h5file.write_file(path, root)
+
+    def write_xrd_hdf5(self, path):
+        """hdf5_write_xrd (src/sqc_hdf5.f90:1050-1141) with write_xrd_partials
+        (:1144-1200): the pattern's attributes and /xrd/{two_theta,I,count}
+        (+ /xrd/I_partial/<pair> and /xrd/pairs)."""
+        if not self.xrd:
+            return None
+        tth, I, Ip, cnt, nf = self.plan.xrd()
+        lo, hi = self.xrd.get("range", (1.0, 179.0))
+        root = h5file.Group()
+        root.attr("lambda", float(self.xrd["lam"]))
+        root.attr("two_theta_min", float(lo))
+        root.attr("two_theta_max", float(hi))
+        root.attr("step", float(self.plan.info.xrd_step))
+        root.attr("bins", int(len(tth)))
+        root.attr("nframes", int(nf))
+        root.attr("natoms", int(self.natoms))
+        root.attr("lorentz_polarization", "on" if self.xrd.get("lp", True) else "off")
+        root.attr("intensity", "sum of |rho(q)|^2 over the reciprocal lattice points of the "
+                  "bin, per atom and per frame")
+        g = root.group("xrd")
+        g.dataset("two_theta", np.asarray(tth, dtype=np.float64))
+        g.dataset("I", np.asarray(I, dtype=np.float64))
+        g.dataset("count", np.asarray(cnt, dtype=np.int64))
+        pairs = self.pair_list() if (self.partials and len(tth) > 0) else []
+        if pairs:
+            sub = g.group("I_partial")
+            for t, u, lab in pairs:
+                sub.dataset(lab, np.asarray(Ip[t - 1, u - 1, :], dtype=np.float64))
+            g.dataset("pairs", [lab for _, _, lab in pairs], strlen=18)
+            g.attr("partial_normalization", "intensity: I = sum_a I(a-a) + 2 sum_{a<b} I(a-b)")
+        h5file.write_file(path, root)
+        return tth, I, Ip, cnt
 
     def write_xrd(self, path):
         """The powder pattern table of sf_write_xrd (src/sqc_structure_factor.f90:964-1031)."""

@@ -88,3 +88,59 @@ def test_cli_multi_frame_matches_library(tmp_path):
         S = p.finalize()[0]
     got = np.loadtxt(out)
     np.testing.assert_allclose(got[:, 1], S, rtol=1e-9, atol=1e-12)
+
+
+def test_cli_hdf5_grid_and_xrd_match_text_tables(tmp_path):
+    """--grid x.h5 / --xrd y.h5 (src/sqc_hdf5.f90:46-210, :1050-1200): the HDF5
+    datasets hold the same numbers as the text tables of the same run."""
+    import h5read
+    path = str(tmp_path / "m.dump")
+    open(path, "w").write("".join(frame(t, 300, 10.0, 20 + t) for t in range(3)))
+    base = ["-i", path, "-m", "1:Si,2:O", "-w", "neutron", "--eps", "1e-10",
+            "--xrd-lambda", "1.5406", "--xrd-range", "10", "120", "-q"]
+    txt = ["--grid", str(tmp_path / "g.txt"), "--xrd", str(tmp_path / "x.txt"),
+           str(tmp_path / "s.txt")]
+    h5 = ["--grid", str(tmp_path / "g.h5"), "--xrd", str(tmp_path / "x.h5"),
+          str(tmp_path / "s2.txt")]
+    for extra in (txt, h5):
+        r = cli(base + extra)
+        assert r.returncode == 0, r.stderr
+    shell = np.loadtxt(str(tmp_path / "s.txt"))
+    grid = np.loadtxt(str(tmp_path / "g.txt"))
+    xrd = np.loadtxt(str(tmp_path / "x.txt"))
+    f = h5read.read(str(tmp_path / "g.h5"))
+    assert f.attrs["nframes"] == 3 and f.attrs["natoms"] == 300
+    assert f.attrs["nmodes"] == grid.shape[0] == f["shell/count"].value.sum()
+    assert f.attrs["mapping"] == "1:Si,2:O" and f.attrs["device"] == "gpu"
+    assert f.attrs["weight"] == "neutron bound coherent scattering lengths"
+    assert f.attrs["norm"] == "mean" and f.attrs["precision"] == "double"
+    assert f.attrs["cell"].shape == (3, 3) and f.attrs["cell"][0, 0] == 10.0
+    np.testing.assert_allclose(f["shell/q"].value, shell[:, 0], atol=1e-6)
+    np.testing.assert_allclose(f["shell/S"].value, shell[:, 1], rtol=1e-11, atol=1e-300)
+    assert f["shell/pairs"].value == ["Si-Si", "Si-O", "O-O"]
+    assert f["shell"].attrs["partial_normalization"] == "ovito"
+    for j, lab in enumerate(["Si-Si", "Si-O", "O-O"]):
+        np.testing.assert_allclose(f["shell/S_partial/" + lab].value, shell[:, 2 + j],
+                                   rtol=1e-11, atol=1e-300)
+    for j, name in enumerate(["qx", "qy", "qz"]):
+        np.testing.assert_allclose(f["grid/" + name].value, grid[:, j], atol=1e-8)
+    np.testing.assert_allclose(f["grid/S"].value, grid[:, 3], rtol=1e-11, atol=1e-300)
+    b = 2.0 * np.pi / 10.0
+    np.testing.assert_allclose(f["grid/h"].value * b, grid[:, 0], atol=1e-8)
+    np.testing.assert_allclose(f["grid/l"].value * b, grid[:, 2], atol=1e-8)
+    x = h5read.read(str(tmp_path / "x.h5"))
+    assert x.attrs["lambda"] == 1.5406 and x.attrs["bins"] == xrd.shape[0]
+    assert x.attrs["lorentz_polarization"] == "on"
+    np.testing.assert_allclose(x["xrd/two_theta"].value, xrd[:, 0], atol=1e-4)
+    np.testing.assert_allclose(x["xrd/I"].value, xrd[:, 1], rtol=1e-11, atol=1e-300)
+    assert x["xrd/count"].value.sum() > 0
+    for j, lab in enumerate(["Si-Si", "Si-O", "O-O"]):
+        np.testing.assert_allclose(x["xrd/I_partial/" + lab].value, xrd[:, 2 + j],
+                                   rtol=1e-11, atol=1e-300)
+    # --format text keeps a .h5 name a text table; an unknown format is exit 2
+    r = cli(base[:-1] + ["--format", "text", "--grid", str(tmp_path / "t.h5"), "-q",
+                         str(tmp_path / "s3.txt")])
+    assert r.returncode == 0, r.stderr
+    assert open(str(tmp_path / "t.h5")).readline().startswith("# qx qy qz")
+    r = cli(base + ["--format", "csv", str(tmp_path / "s4.txt")])
+    assert r.returncode == 2
