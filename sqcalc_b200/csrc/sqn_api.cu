@@ -681,25 +681,6 @@ int setup_plan(sqn_plan *p, const sqn_plan_desc *d) {
   b.norm = d->norm;
   b.natoms = d->natoms;
   if (d->norm < 1 || d->norm > 3) return SQN_ERR_INVALID_ARGUMENT;
-  {
-    // Bound on one mode's contribution to a shell sum: |rho_a| <= N_a, so the
-    // weighted total is at most (sum_a |w_a|max N_a)^2 and a pair product at most
-    // (sum_a N_a)^2, times 2 for the mirror mode; 10 % on top covers the NUFFT
-    // and rounding errors of the transformed values.
-    double sa = 0.0, s1 = 0.0;
-    for (int k = 0; k < p->nspecies; ++k) {
-      const double n = (double)p->type_counts[p->species_type[k] - 1];
-      double amax = std::fabs(p->amp_sp[k]);
-      if (xray) {
-        amax = std::fabs(p->xcoef_sp[9 * k + 8]);
-        for (int i = 0; i < 4; ++i) amax += std::fabs(p->xcoef_sp[9 * k + i]);
-      }
-      sa += amax * n;
-      s1 += n;
-    }
-    b.vmax = 2.2 * std::max(sa * sa, s1 * s1);
-    b.fx_scale = b.fx_inv = 0.0;
-  }
 
   // --- powder XRD bins (sf_configure_xrd, src/sqc_structure_factor.f90:846-905)
   b.xrd = 0;

@@ -160,38 +160,6 @@ __device__ __forceinline__ void hist_add(double *hist, int s, double v, bool kee
   }
 }
 
-// Fixed-point shell sums.  hist[s] holds round(sum * scale) as a two's-complement
-// int64 split into an (unsigned lo, int hi) word pair, so that a value adds with
-// 32-bit shared atomics (several times the rate of 64-bit ones): the low word's
-// atomic returns its old value, which tells whether it wrapped, and the high
-// word takes the high part plus that carry (skipped when both are zero).  The
-// sum is exact and independent of the order of the adds; the plan chooses a
-// power-of-two scale for which no sum a CTA can form reaches 2^62.
-__device__ __forceinline__ void fx_add(double *hist, int s, double v, double scale) {
-  const long long q = __double2ll_rn(v * scale);
-  unsigned *wp = reinterpret_cast<unsigned *>(hist + s);
-  const unsigned lo = (unsigned)(unsigned long long)q;
-  const int hi = (int)(q >> 32);
-  const unsigned old = atomicAdd(wp, lo);
-  const int up = hi + ((old + lo < old) ? 1 : 0);
-  if (up != 0) atomicAdd(reinterpret_cast<int *>(wp + 1), up);
-}
-// The fixed-point sum hist[i] as a double (times 1 / scale).
-__device__ __forceinline__ double fx_value(const double *hist, int i, double inv_scale) {
-  const unsigned *wp = reinterpret_cast<const unsigned *>(hist + i);
-  const long long q = (long long)(((unsigned long long)wp[1] << 32) | wp[0]);
-  return (double)q * inv_scale;
-}
-__device__ __forceinline__ void hist_add_fx(double *hist, int s, double v, bool keep, bool uni,
-                                            int s0, int lane, double scale) {
-  if (uni) {
-    v = warp_sum(keep ? v : 0.0);
-    if (lane == 0) fx_add(hist, s0, v, scale);
-  } else if (keep) {
-    fx_add(hist, s, v, scale);
-  }
-}
-
 template <typename R> struct Cplx;
 template <> struct Cplx<float> { using T = float2; };
 template <> struct Cplx<double> { using T = double2; };
@@ -264,7 +232,7 @@ __device__ __forceinline__ void xrd_bin_weight(const BinGeom &b, double q, int &
 // gnum[gidx] (each mode is visited once per frame).  The reference's
 // counterpart is the host loops of src/sqc_structure_factor.f90:481-521
 // and :595-643.
-template <typename R, int TM, bool XR, bool XD = false, bool FX = false>
+template <typename R, int TM, bool XR, bool XD = false>
 __device__ __forceinline__ void bin_mode(const BinGeom &b, int ntr, bool inrange, int h1, int h2,
                                          int h3, const double *crow,
                                          const typename Cplx<R>::T (&v)[TM], R dec,
@@ -272,13 +240,6 @@ __device__ __forceinline__ void bin_mode(const BinGeom &b, int ntr, bool inrange
                                          const double *__restrict__ xcoef, double *hist,
                                          double *__restrict__ gnum, int64_t gidx, int lane,
                                          double *xhist = nullptr) {
-  // shell sums in FP64 shared atomics, or fixed point (FX, b.fx_scale)
-  auto add = [&](double *h, int sh, double val, bool kp, bool un, int sh0) {
-    if constexpr (FX)
-      hist_add_fx(h, sh, val, kp, un, sh0, lane, b.fx_scale);
-    else
-      hist_add(h, sh, val, kp, un, sh0, lane);
-  };
   double ql = 0.0;
   int s = 0;
   const bool keep = inrange && classify_mode(b, crow, h1, h2, h3, s, ql);
@@ -309,7 +270,7 @@ __device__ __forceinline__ void bin_mode(const BinGeom &b, int ntr, bool inrange
   if (b.want_grid && keep) gnum[gidx] += I;
   const int s0 = __shfl_sync(FULL, s, __ffs(act) - 1);
   const bool uni = __all_sync(FULL, !keep || s == s0);
-  add(hist, s, mult * I, keep, uni, s0);
+  hist_add(hist, s, mult * I, keep, uni, s0, lane);
   if (b.partials) {
     int p = 1;
 #pragma unroll
@@ -317,7 +278,8 @@ __device__ __forceinline__ void bin_mode(const BinGeom &b, int ntr, bool inrange
 #pragma unroll
       for (int c = a; c < TM; ++c) {
         if (c < ntr) {
-          add(hist + p * b.nq, s, mult * (re[a] * re[c] + im[a] * im[c]), keep, uni, s0);
+          hist_add(hist + p * b.nq, s, mult * (re[a] * re[c] + im[a] * im[c]), keep, uni, s0,
+                   lane);
           ++p;
         }
       }

@@ -110,10 +110,6 @@ struct BinGeom {
   // sums in the accumulator buffer
   int xrd, xbins, xquant, xlp;
   double xlambda, xmin, xstep;  // Angstrom, degrees, degrees
-  // bound on the magnitude of one mode's contribution to a shell sum (both
-  // mirrors counted); the bin kernel derives its fixed-point scale from it
-  double vmax;
-  double fx_scale, fx_inv;  // set per launch: 2^k and 2^-k
 };
 
 // FP64 sums of one frame pass: shell sums, then the powder-pattern sums.

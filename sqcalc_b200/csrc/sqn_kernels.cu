@@ -25,7 +25,6 @@
 // (external/finufft/src/cuda/3d/spreadinterp3d.cuh:276-383,
 //  external/finufft/src/cuda/deconvolve_wrapper.cu:76-118) followed by the host
 // loops of src/sqc_structure_factor.f90:457-643.
-#include <cmath>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -474,7 +473,7 @@ __global__ void __launch_bounds__(SPREAD_THREADS, sizeof(R) == 4 ? 2 : 1)
 // ---------------------------------------------------------------------------
 // Rows r = r0, r0 + rstep, ... of the half space, one warp each, into the
 // histograms hist (and xhist for the powder pattern, gnum for the grid).
-template <typename R, int NT, bool XR, bool XD, bool FX = false>
+template <typename R, int NT, bool XR, bool XD>
 __device__ __forceinline__ void bin_rows(const int4 *__restrict__ rows, int nrows,
                                          const typename Cplx<R>::T *__restrict__ G,
                                          const BinGeom &b, const R *__restrict__ inv1,
@@ -507,15 +506,13 @@ __device__ __forceinline__ void bin_rows(const int4 *__restrict__ rows, int nrow
       for (int t = 0; t < TM; ++t)
         if (t < ntr && inrow) v[t] = G[(int64_t)t * b.vol_cplx + rowbase + h1];
       const R dec = inrow ? inv1[h1] * dyz : R(0);
-      bin_mode<R, TM, XR, XD, FX>(b, ntr, inrow, h1, h2, h3, crow, v, dec, amp, xcoef, hist,
-                                  gnum, gbase + h1, lane, xhist);
+      bin_mode<R, TM, XR, XD>(b, ntr, inrow, h1, h2, h3, crow, v, dec, amp, xcoef, hist, gnum,
+                              gbase + h1, lane, xhist);
     }
   }
 }
 
-// FX (with SMEM, without the powder pattern): the CTA's shell sums in fixed
-// point (fx_add), converted to FP64 when flushed.
-template <typename R, int NT, bool SMEM, bool XR, bool XD, bool FX = false>
+template <typename R, int NT, bool SMEM, bool XR, bool XD>
 __global__ void __launch_bounds__(256, 2)
     k_bin(const int4 *__restrict__ rows, int nrows, const typename Cplx<R>::T *__restrict__ G,
           BinGeom b, const R *__restrict__ inv1, const R *__restrict__ inv2,
@@ -531,12 +528,12 @@ __global__ void __launch_bounds__(256, 2)
     for (int i = tid; i < nhist; i += blockDim.x) s_hist[i] = 0.0;
     __syncthreads();
   }
-  bin_rows<R, NT, XR, XD, FX>(rows, nrows, G, b, inv1, inv2, inv3, amp, xcoef, hist, xhist,
-                              gnum, blockIdx.x * nwarps + warp, gridDim.x * nwarps, lane);
+  bin_rows<R, NT, XR, XD>(rows, nrows, G, b, inv1, inv2, inv3, amp, xcoef, hist, xhist, gnum,
+                          blockIdx.x * nwarps + warp, gridDim.x * nwarps, lane);
   if (SMEM) {
     __syncthreads();
     for (int i = tid; i < nhist; i += blockDim.x) {
-      const double v = FX ? fx_value(s_hist, i, b.fx_inv) : s_hist[i];
+      const double v = s_hist[i];
       if (v != 0.0) atomicAdd(&acc[i], v);
     }
   }
@@ -863,29 +860,14 @@ cudaError_t launch_spread_pw(const R *recs, const int *starts, const FrameGeom &
   return cudaGetLastError();
 }
 
-// Fixed-point scale of a bin launch: the largest power of two for which no
-// shell sum a CTA can form (its modes x the per-mode bound) reaches 2^62; 0
-// (FP64 atomics) without a bound.
-static double bin_fx_scale(const BinGeom &b, int nrows, int blocks, int warps_per_block) {
-  if (!(b.vmax > 0.0)) return 0.0;
-  const int64_t rows_per_warp = (nrows + (int64_t)blocks * warps_per_block - 1) /
-                                ((int64_t)blocks * warps_per_block);
-  const double modes = (double)rows_per_warp * warps_per_block * (double)(b.hm[0] + 1);
-  const int k = (int)std::floor(std::log2(std::ldexp(1.0, 62) / (modes * b.vmax)));
-  return std::ldexp(1.0, k);
-}
-
 template <typename R, int NT, bool XR>
-static cudaError_t bin_dispatch_xr(const int4 *rows, int nrows, const void *G, const BinGeom &bg,
+static cudaError_t bin_dispatch_xr(const int4 *rows, int nrows, const void *G, const BinGeom &b,
                                    const R *i1, const R *i2, const R *i3, const double *amp,
                                    const double *xc, double *acc, double *gnum, int nsm,
                                    cudaStream_t s) {
   using C = typename Cplx<R>::T;
-  const size_t hist = (size_t)hist_len(bg) * sizeof(double);
+  const size_t hist = (size_t)hist_len(b) * sizeof(double);
   const int blocks = nsm * 4;
-  BinGeom b = bg;
-  b.fx_scale = bin_fx_scale(bg, nrows, blocks, 256 / 32);
-  b.fx_inv = b.fx_scale > 0.0 ? 1.0 / b.fx_scale : 0.0;
   if (hist <= 160 * 1024) {
     if (b.xrd) {
       cudaError_t e = cudaFuncSetAttribute(k_bin<R, NT, true, XR, true>,
@@ -893,12 +875,6 @@ static cudaError_t bin_dispatch_xr(const int4 *rows, int nrows, const void *G, c
       if (e != cudaSuccess) return e;
       k_bin<R, NT, true, XR, true><<<blocks, 256, hist, s>>>(rows, nrows, (const C *)G, b, i1,
                                                              i2, i3, amp, xc, acc, gnum);
-    } else if (b.fx_scale > 0.0) {
-      cudaError_t e = cudaFuncSetAttribute(k_bin<R, NT, true, XR, false, true>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hist);
-      if (e != cudaSuccess) return e;
-      k_bin<R, NT, true, XR, false, true><<<blocks, 256, hist, s>>>(
-          rows, nrows, (const C *)G, b, i1, i2, i3, amp, xc, acc, gnum);
     } else {
       cudaError_t e = cudaFuncSetAttribute(k_bin<R, NT, true, XR, false>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hist);
