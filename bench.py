@@ -787,24 +787,19 @@ def run_ours(args, rank, world, local_rank):
         c1 = nf[0] // 2 + 1
         spread_bytes = ntr * vol * p + N_ATOMS * (16 if p == 4 else 32)
         bin_bytes = ntr * (info.nmodes // 2) * 2 * p
-        # algorithmic bytes of each stage over its CUDA-event time
-        m = list(info.modes)
-        H1, M2, M3 = (m[0] - 1) // 2 + 1, m[1], m[2]
-        if info.pruned_fft512 and info.fused_zbin:
-            # x and y passes here; the z pass reads A2 inside the fused binning kernel
-            fft_bytes = ntr * (vol * p + 2 * nf[2] * nf[1] * H1 * 2 * p
-                               + nf[2] * M2 * H1 * 2 * p)
-            bin_bytes = ntr * nf[2] * M2 * H1 * 2 * p
-        elif info.pruned_fft512:
-            fft_bytes = ntr * (vol * p + 2 * nf[2] * nf[1] * H1 * 2 * p
-                               + 2 * nf[2] * M2 * H1 * 2 * p + M3 * M2 * H1 * 2 * p)
-        else:
-            fft_bytes = ntr * (vol * p + vol // nf[0] * c1 * 2 * p)  # one-pass lower bound
         kern = "spread" if stage_ms["spread_ms"] >= stage_ms["bin_ms"] else "bin"
         kb = spread_bytes if kern == "spread" else bin_bytes
         kms = stage_ms["spread_ms"] if kern == "spread" else stage_ms["bin_ms"]
         achieved = kb / (kms * 1e-3) / 1e9
         frame_bytes = ntr * (3 * vol * p + (info.nmodes // 2) * 2 * p) + N_ATOMS * (24 + 1)
+        # algorithmic bytes of each stage over its CUDA-event time
+        m = list(info.modes)
+        H1, M2, M3 = (m[0] - 1) // 2 + 1, m[1], m[2]
+        if info.pruned_fft512:
+            fft_bytes = ntr * (vol * p + 2 * nf[2] * nf[1] * H1 * 2 * p
+                               + 2 * nf[2] * M2 * H1 * 2 * p + M3 * M2 * H1 * 2 * p)
+        else:
+            fft_bytes = ntr * (vol * p + vol // nf[0] * c1 * 2 * p)  # one-pass lower bound
         stage_roofline = {}
         for name, nbytes, ms in (("spread", spread_bytes, stage_ms["spread_ms"]),
                                  ("fft", fft_bytes, stage_ms["fft_ms"]),
@@ -822,31 +817,24 @@ def run_ours(args, rank, world, local_rank):
                 "parallelism": "frames sharded over %d GPU(s)" % world,
                 "upsampfac": info.upsampfac, "kernel_width": info.kernel_width,
                 "fine_grid": nf, "nmodes_kept": info.nmodes, "ntransforms": ntr}),
-            "roofline": {"bound": "hbm", "kernel": "k_spread" if kern == "spread" else (
-                             "k_fft512_zbin" if info.fused_zbin else "k_bin"),
+            "roofline": {"bound": "hbm", "kernel": "k_spread" if kern == "spread" else "k_bin",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
-                         "traffic": dram_traffic("k_spread" if kern == "spread" else (
-                             "k_fft512_zbin" if info.fused_zbin else "k_bin")),
+                         "traffic": dram_traffic("k_" + kern),
                          "algorithmic_bytes_per_launch": kb, "launch_ms": kms},
             "pipeline": {"bytes_per_frame": frame_bytes, "ms_per_frame": frame_ms,
                          "achieved_gbs": frame_bytes / (frame_ms * 1e-3) / 1e9,
                          "frac": frame_bytes / (frame_ms * 1e-3) / 1e9 / peak,
                          "stage_ms": stage_ms, "stage_roofline": stage_roofline,
-                         "stage_roofline_note": (
-                             "HBM roofline per stage (measured copy peak); fft = the x and y "
-                             "pruned 512-point passes' reads and writes, bin = the z pass "
-                             "fused with the shell binning (reads the y pass's output)"
-                             if info.fused_zbin else
-                             "HBM roofline per stage (measured copy peak); fft = the pruned "
-                             "512-point passes' reads and writes")},
+                         "stage_roofline_note": "HBM roofline per stage (measured copy "
+                                                "peak); fft = the pruned 512-point passes' "
+                                                "reads and writes"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": fbytes,
                     "d2h_bytes_per_step": NQ * 8},
             "gpu_launches": launches,
             "gpu_launches_note": "own kernels per frame: prep, scan, scatter, spread, the "
-                                 "x and y pruned 512-point FFT passes and the z pass fused "
-                                 "with the shell binning (512^3 grids; otherwise cuFFT, not "
-                                 "counted, and bin)",
+                                 "three pruned 512-point FFT passes (512^3 grids; cuFFT "
+                                 "kernels, not counted, otherwise) and bin",
             "fp64": fp64,
             "reference_gpu_baseline": ref_gpu,
             "plain_fp64_config": small,

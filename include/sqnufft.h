@@ -141,9 +141,6 @@ typedef struct sqn_plan_info {
   int32_t autotuned;        /* 1: fine grid and width chosen by timing (SQN_FLAG_AUTOTUNE) */
   int32_t tune_candidates;  /* (sigma, w) pairs timed (0 when the choice came from the cache) */
   double tune_ms;           /* measured milliseconds per frame of the chosen pair */
-  int32_t fused_zbin;       /* 1: with pruned_fft512, the frame path interleaves the
-                               transforms and fuses the z pass with the shell binning */
-  int32_t reserved0;
 } sqn_plan_info;
 
 typedef struct sqn_plan_s sqn_plan;

@@ -103,8 +103,6 @@ class SqnInfo(ctypes.Structure):
         ("autotuned", ctypes.c_int32),
         ("tune_candidates", ctypes.c_int32),
         ("tune_ms", ctypes.c_double),
-        ("fused_zbin", ctypes.c_int32),
-        ("reserved0", ctypes.c_int32),
     ]
 
 

@@ -270,7 +270,6 @@ struct sqn_plan_s {
   int64_t c1pitch = 0;  // complex row pitch of the half spectrum
   // pruned 512-point passes (every axis 512): compact half spectrum in d_G
   bool fft512 = false;
-  bool zbin = false;  // ... with the transforms interleaved and the z pass fused with binning
   void *d_tw512 = nullptr;
   BinGeom bg512{};
   // density amplitudes (sqn_density_modes): request buffers, grown on demand
@@ -887,7 +886,6 @@ int setup_plan(sqn_plan *p, const sqn_plan_desc *d) {
     p->bg512.c1 = p->hm[0] + 1;
     p->bg512.vol_cplx = p->bg512.c1 * p->bg512.nf[1] * p->bg512.nf[2];
     p->fft512 = true;
-    p->zbin = fft512_bin_fits(p->bg512, p->fp64);
   }
 
   // --- adjoint buffers (dS/dr) -----------------------------------------------
@@ -939,7 +937,7 @@ int setup_plan(sqn_plan *p, const sqn_plan_desc *d) {
 }
 
 // Kernels of ours that one frame launches.
-int frame_launches(const sqn_plan *p) { return p->fft512 ? (p->zbin ? 7 : 8) : 5; }
+int frame_launches(const sqn_plan *p) { return p->fft512 ? 8 : 5; }
 
 // All queued work of the plan finished.
 int sync_plan(sqn_plan *p) {
@@ -1051,22 +1049,6 @@ template <typename R> int run_frame(sqn_plan *p, const double *dpos, int slot) {
                        s);
   if (e != cudaSuccess) return SQN_ERR_CUDA;
   if (p->timing) cudaEventRecord(ev[2], s);
-  if (p->zbin) {
-    // x pass into d_G, y pass back into the (consumed) grid, both with the
-    // transforms interleaved; the z pass bins as it transforms
-    e = launch_fft512_xy_il<R>((const R *)grid, p->d_G, grid, p->ntr, g.pitch, p->hm[0] + 1,
-                               p->hm[1], p->d_tw512, p->nsm, s);
-    if (e != cudaSuccess) return SQN_ERR_CUDA;
-    if (p->timing) cudaEventRecord(ev[3], s);
-    e = launch_fft512_zbin<R>(grid, p->hm[0] + 1, p->d_tw512, p->bg512, (const R *)p->d_inv[0],
-                              (const R *)p->d_inv[1], (const R *)p->d_inv[2], p->d_amp,
-                              p->d_xcoef, p->d_acc, p->d_gnum, p->nsm, s);
-    if (e != cudaSuccess) return SQN_ERR_CUDA;
-    if (p->timing) cudaEventRecord(ev[4], s);
-    p->launches += 7;
-    p->nframes++;
-    return SQN_OK;
-  }
   if (p->fft512) {
     // x pass into d_G, y pass back into the (consumed) grid, z pass into d_G
     e = launch_fft512<R>((const R *)grid, p->d_G, grid, p->d_G, p->ntr, g.pitch, p->hm[0] + 1,
@@ -1203,7 +1185,6 @@ int sqn_plan_info_get(const sqn_plan *p, sqn_plan_info *info) {
   info->nspecies = p->nspecies;
   info->device_bytes = p->device_bytes;
   info->pruned_fft512 = p->fft512 ? 1 : 0;
-  info->fused_zbin = p->zbin ? 1 : 0;
   info->natoms = p->desc.natoms;
   info->xrd_bins = p->bg.xrd ? p->bg.xbins : 0;
   info->xrd_step = p->bg.xrd ? p->bg.xstep : 0.0;

@@ -205,14 +205,10 @@ template <typename R> __host__ __device__ constexpr int x_warps() {
   return sizeof(R) == 4 ? 8 : 4;
 }
 
-// ilT = 0: rows (t, z, y) in order, output A1[t][z][y][h1].  ilT = T > 0: the
-// transforms interleaved, output A1[z][y][h1][t]; pair index pr = u T + t
-// takes rows (t, z, 2 u') and (t, z, 2 u' + 1) so that the T warps writing one
-// output region run side by side (their stride-T stores meet in L2).
 template <typename R>
 __global__ void __launch_bounds__(32 * x_warps<R>())
     k_fft512_x(const R *__restrict__ grid, typename Cplx<R>::T *__restrict__ A1, int64_t nrows,
-               int64_t pitch, int H1, const typename Cplx<R>::T *__restrict__ tw, int ilT) {
+               int64_t pitch, int H1, const typename Cplx<R>::T *__restrict__ tw) {
   using C = typename Cplx<R>::T;
   constexpr int X_WARPS = x_warps<R>();
   __shared__ C s_tw[TW_LEN];
@@ -222,22 +218,10 @@ __global__ void __launch_bounds__(32 * x_warps<R>())
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   C *line = s_line[warp];
   const int64_t npairs = (nrows + 1) >> 1;
-  const int64_t rows_t = ilT > 0 ? nrows / ilT : 0;  // rows of one transform (even)
   for (int64_t pr = (int64_t)blockIdx.x * X_WARPS + warp; pr < npairs;
        pr += (int64_t)gridDim.x * X_WARPS) {
-    int64_t row, obase, ostep;
-    if (ilT > 0) {
-      const unsigned u = (unsigned)pr / (unsigned)ilT, t = (unsigned)pr - u * (unsigned)ilT;
-      row = (int64_t)t * rows_t + 2 * (int64_t)u;
-      obase = 2 * (int64_t)u * H1 * ilT + t;
-      ostep = ilT;
-    } else {
-      row = 2 * pr;
-      obase = row * H1;
-      ostep = 1;
-    }
-    const R *r0 = grid + row * pitch;
-    const bool two = row + 1 < nrows;
+    const R *r0 = grid + (2 * pr) * pitch;
+    const bool two = 2 * pr + 1 < nrows;
     C v[16];
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
@@ -251,8 +235,7 @@ __global__ void __launch_bounds__(32 * x_warps<R>())
     for (int a = 0; a < 16; ++a) line[k2 + 16 * a + 256 * b] = v[a];
     __syncwarp();
     // X1[h] = (Z[h] + conj Z[512-h]) / 2, X2[h] = (Z[h] - conj Z[512-h]) / (2i)
-    C *o0 = A1 + obase;
-    const int64_t o2 = (int64_t)H1 * ostep;
+    C *o0 = A1 + (2 * pr) * H1;
     for (int h = lane; h < H1; h += 32) {
       const C zh = line[h];
       const C zm = line[(512 - h) & 511];
@@ -261,8 +244,8 @@ __global__ void __launch_bounds__(32 * x_warps<R>())
       x1.y = R(0.5) * (zh.y - zm.y);
       x2.x = R(0.5) * (zh.y + zm.y);
       x2.y = R(0.5) * (zm.x - zh.x);
-      o0[h * ostep] = x1;
-      if (two) o0[o2 + h * ostep] = x2;
+      o0[h] = x1;
+      if (two) o0[H1 + h] = x2;
     }
     __syncwarp();
   }
@@ -358,148 +341,6 @@ template <typename R> size_t cols_smem() {
   return sizeof(typename Cplx<R>::T) * (TW_LEN + 512 * COL_LD);
 }
 
-// ---------------------------------------------------------------------------
-// z pass fused with the shell binning, on the interleaved layout
-// A2[z][h2][h1][t]: a step takes G consecutive h1 of one h2 plane, i.e. the
-// G * ntr consecutive columns (h1, t) (one coalesced row segment per z),
-// transforms them along z in the staged tile, and bins the G * (2 hm3 + 1)
-// kept modes (h1, h2, h3) straight from the tile with all ntr values of each
-// mode at hand: deconvolution, weighted total, pair products and FP64 shell
-// sums in per-CTA shared histograms (the same per-mode arithmetic as k_bin).
-// The spectrum itself is never written.
-// ---------------------------------------------------------------------------
-struct ZBin {
-  int64_t in_p, in_r;  // A2 strides (complex elements) of an h2 plane and of a z row
-  int M2;              // h2 planes (2 hm2' + 1, FFT order)
-  int H1;              // h1 = 0 .. H1 - 1
-  int G;               // h1 per step
-};
-
-template <typename R, int NT, bool XR, bool XD>
-__global__ void __launch_bounds__(32 * COLS, sizeof(R) == 4 ? 2 : 1)
-    k_fft512_zbin(const typename Cplx<R>::T *__restrict__ in, ZBin zp,
-                  const typename Cplx<R>::T *__restrict__ tw, BinGeom b,
-                  const R *__restrict__ inv1, const R *__restrict__ inv2,
-                  const R *__restrict__ inv3, const double *__restrict__ amp,
-                  const double *__restrict__ xcoef, double *__restrict__ acc,
-                  double *__restrict__ gnum) {
-  using C = typename Cplx<R>::T;
-  constexpr int TM = NT > 0 ? NT : MAX_FAST_T;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C *s_tw = reinterpret_cast<C *>(smem_raw);
-  C *tile = s_tw + TW_LEN;  // [512][COL_LD]
-  double *hist = reinterpret_cast<double *>(tile + 512 * COL_LD);
-  const int nhist = hist_len(b);
-  double *xhist = XD ? hist + b.nquant * b.nq : nullptr;
-  for (int i = threadIdx.x; i < TW_LEN; i += blockDim.x) s_tw[i] = tw[i];
-  for (int i = threadIdx.x; i < nhist; i += blockDim.x) hist[i] = 0.0;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int ntr = NT > 0 ? NT : b.ntr;
-  const int hm2 = b.hm[1], hm3 = b.hm[2];
-  const int M3 = 2 * hm3 + 1;
-  const unsigned nblk = (unsigned)((zp.H1 + zp.G - 1) / zp.G);
-  const unsigned nsteps = (unsigned)zp.M2 * nblk;
-  for (unsigned st = blockIdx.x; st < nsteps; st += gridDim.x) {
-    const unsigned plane = st / nblk;
-    const int h1_0 = (int)(st - plane * nblk) * zp.G;
-    const int ng = min(zp.G, zp.H1 - h1_0);
-    const int nc = ng * ntr;
-    const C *ib = in + (int64_t)plane * zp.in_p + (int64_t)h1_0 * ntr;
-    const int c = threadIdx.x & (COLS - 1), r0 = threadIdx.x >> 4;
-    const C *src = ib + (int64_t)r0 * zp.in_r + c;
-    const int64_t step = 32 * zp.in_r;
-    __syncthreads();  // the previous step's binning has read the tile
-    if (c < nc) {
-#pragma unroll
-      for (int k0 = 0; k0 < 512 / 32; k0 += 8) {
-        C ld[8];
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-          ld[k] = src[0];
-          src += step;
-        }
-#pragma unroll
-        for (int k = 0; k < 8; ++k) tile[(r0 + 32 * (k0 + k)) * COL_LD + c] = ld[k];
-      }
-    }
-    __syncthreads();
-    if (warp < nc) {
-      C *col = tile + warp;
-      C v[16];
-#pragma unroll
-      for (int j = 0; j < 16; ++j) v[j] = col[(lane + 32 * j) * COL_LD];
-      __syncwarp();
-      warp_fft512(v, col, COL_LD, s_tw, lane);
-      const int k2 = lane & 15, bb = lane >> 4;
-#pragma unroll
-      for (int a = 0; a < 16; ++a) col[(k2 + 16 * a + 256 * bb) * COL_LD] = v[a];
-    }
-    __syncthreads();
-    // modes (h1_0 + g, h2, h3): lanes walk h3 (tile row h3 mod 512)
-    const int h2 = (int)plane <= hm2 ? (int)plane : (int)plane - zp.M2;
-    const R d2 = inv2[abs(h2)];
-    const int nmode = ng * M3;
-    for (int base = warp * 32; base < nmode; base += 32 * COLS) {
-      const int idx = base + lane;
-      const bool inr = idx < nmode;
-      const int g = inr ? idx / M3 : 0;
-      const int hw = inr ? idx - g * M3 : 0;
-      const int h3 = hw <= hm3 ? hw : hw - M3;
-      const int h1 = h1_0 + g;
-      const C *trow = tile + (h3 >= 0 ? h3 : 512 + h3) * COL_LD + g * ntr;
-      C v[TM];
-#pragma unroll
-      for (int t = 0; t < TM; ++t)
-        if (t < ntr && inr) v[t] = trow[t];
-      const R dec = inr ? inv1[h1] * d2 * inv3[abs(h3)] : R(0);
-      double crow[3];
-      row_const(b, h2, h3, crow);
-      const int64_t gidx =
-          ((int64_t)(h3 + hm3) * b.m2 + (int64_t)(h2 + hm2)) * (int64_t)(b.hm[0] + 1) + h1;
-      bin_mode<R, TM, XR, XD>(b, ntr, inr, h1, h2, h3, crow, v, dec, amp, xcoef, hist, gnum,
-                              gidx, lane, xhist);
-    }
-  }
-  __syncthreads();
-  for (int i = threadIdx.x; i < nhist; i += blockDim.x) {
-    const double v = hist[i];
-    if (v != 0.0) atomicAdd(&acc[i], v);
-  }
-}
-
-template <typename R> size_t zbin_smem(const BinGeom &b) {
-  return cols_smem<R>() + sizeof(double) * (size_t)hist_len(b);
-}
-
-template <typename R, int NT, bool XR, bool XD>
-cudaError_t launch_zbin_k(const void *A2, const ZBin &zp, const void *tw, const BinGeom &b,
-                          const R *i1, const R *i2, const R *i3, const double *amp,
-                          const double *xc, double *acc, double *gnum, int nsm, cudaStream_t s) {
-  using C = typename Cplx<R>::T;
-  const size_t sm = zbin_smem<R>(b);
-  cudaError_t e = cudaFuncSetAttribute(k_fft512_zbin<R, NT, XR, XD>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-  if (e != cudaSuccess) return e;
-  // two CTAs per SM where the shared memory allows it (FP32, histograms up to ~32 KB)
-  const int cta = (sizeof(R) == 4 && 2 * (sm + 1024) <= 228 * 1024) ? 2 : 1;
-  k_fft512_zbin<R, NT, XR, XD><<<nsm * cta, 32 * COLS, sm, s>>>(
-      (const C *)A2, zp, (const C *)tw, b, i1, i2, i3, amp, xc, acc, gnum);
-  return cudaGetLastError();
-}
-
-template <typename R, int NT>
-cudaError_t launch_zbin_nt(const void *A2, const ZBin &zp, const void *tw, const BinGeom &b,
-                           const R *i1, const R *i2, const R *i3, const double *amp,
-                           const double *xc, double *acc, double *gnum, int nsm,
-                           cudaStream_t s) {
-  if (b.xray) {
-    if (b.xrd) return launch_zbin_k<R, NT, true, true>(A2, zp, tw, b, i1, i2, i3, amp, xc, acc, gnum, nsm, s);
-    return launch_zbin_k<R, NT, true, false>(A2, zp, tw, b, i1, i2, i3, amp, xc, acc, gnum, nsm, s);
-  }
-  if (b.xrd) return launch_zbin_k<R, NT, false, true>(A2, zp, tw, b, i1, i2, i3, amp, xc, acc, gnum, nsm, s);
-  return launch_zbin_k<R, NT, false, false>(A2, zp, tw, b, i1, i2, i3, amp, xc, acc, gnum, nsm, s);
-}
-
 }  // namespace
 
 template <typename R> cudaError_t fft512_set_attributes() {
@@ -531,7 +372,7 @@ cudaError_t launch_fft512(const R *grid, void *A1, void *A2, void *G, int ntr, i
   const int64_t nrows = (int64_t)ntr * n * n;
   if ((int64_t)ntr * n * ((H1 + COLS - 1) / COLS) >= ((int64_t)1 << 31)) return cudaErrorInvalidValue;
   k_fft512_x<R><<<nsm * 8, 32 * x_warps<R>(), 0, s>>>(grid, (C *)A1, nrows, pitch, H1,
-                                                      (const C *)tw, 0);
+                                                      (const C *)tw);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   const size_t sm = cols_smem<R>();
@@ -568,80 +409,6 @@ cudaError_t launch_fft512(const R *grid, void *A1, void *A2, void *G, int ntr, i
   cols(A2, G, z);
   return cudaGetLastError();
 }
-bool fft512_bin_fits(const BinGeom &b, bool fp64) {
-  if (b.ntr < 1 || b.ntr > MAX_FAST_T) return false;
-  const size_t sm = fp64 ? zbin_smem<double>(b) : zbin_smem<float>(b);
-  return sm <= 227 * 1024;
-}
-
-// x and y passes into the interleaved layout: grid [ntr][512][512][pitch] real
-// -> A1 [512][512][H1][ntr] -> A2 [512][2 hm1 + 1][H1][ntr].
-template <typename R>
-cudaError_t launch_fft512_xy_il(const R *grid, void *A1, void *A2, int ntr, int64_t pitch,
-                                int H1, int hm1, const void *tw, int nsm, cudaStream_t s) {
-  using C = typename Cplx<R>::T;
-  const int n = 512;
-  const int M2 = 2 * hm1 + 1;
-  const int64_t ncols = (int64_t)H1 * ntr;
-  if (ntr < 1 || ntr > MAX_FAST_T || (int64_t)n * ((ncols + COLS - 1) / COLS) >= ((int64_t)1 << 31))
-    return cudaErrorInvalidValue;
-  k_fft512_x<R><<<nsm * 8, 32 * x_warps<R>(), 0, s>>>(grid, (C *)A1, (int64_t)ntr * n * n, pitch,
-                                                      H1, (const C *)tw, ntr);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
-  ColPass y;
-  y.in_t = 0;
-  y.in_p = (int64_t)n * ncols;
-  y.in_r = ncols;
-  y.out_t = 0;
-  y.out_p = (int64_t)M2 * ncols;
-  y.out_r = ncols;
-  y.planes_per_t = n;
-  y.nplanes = n;
-  y.ncols = (int)ncols;
-  y.hm = hm1;
-  const int cta = sizeof(R) == 4 ? 2 : 1;
-  k_fft512_cols<R><<<nsm * cta, 32 * COLS, cols_smem<R>(), s>>>((const C *)A1, (C *)A2, y,
-                                                                 (const C *)tw);
-  return cudaGetLastError();
-}
-
-// z pass fused with the shell binning over A2 of launch_fft512_xy_il; the
-// histograms of b (hist_len(b) sums) are added into acc.
-template <typename R>
-cudaError_t launch_fft512_zbin(const void *A2, int H1, const void *tw, const BinGeom &b,
-                               const R *inv1, const R *inv2, const R *inv3, const double *amp,
-                               const double *xcoef, double *acc, double *gnum, int nsm,
-                               cudaStream_t s) {
-  if (!fft512_bin_fits(b, sizeof(R) == 8) || H1 != b.hm[0] + 1) return cudaErrorInvalidValue;
-  ZBin zp;
-  zp.M2 = 2 * b.hm[1] + 1;
-  zp.H1 = H1;
-  zp.G = COLS / b.ntr;
-  zp.in_p = (int64_t)H1 * b.ntr;
-  zp.in_r = (int64_t)zp.M2 * zp.in_p;
-  switch (b.ntr) {
-    case 1: return launch_zbin_nt<R, 1>(A2, zp, tw, b, inv1, inv2, inv3, amp, xcoef, acc, gnum, nsm, s);
-    case 2: return launch_zbin_nt<R, 2>(A2, zp, tw, b, inv1, inv2, inv3, amp, xcoef, acc, gnum, nsm, s);
-    case 3: return launch_zbin_nt<R, 3>(A2, zp, tw, b, inv1, inv2, inv3, amp, xcoef, acc, gnum, nsm, s);
-    case 4: return launch_zbin_nt<R, 4>(A2, zp, tw, b, inv1, inv2, inv3, amp, xcoef, acc, gnum, nsm, s);
-    default: return launch_zbin_nt<R, 0>(A2, zp, tw, b, inv1, inv2, inv3, amp, xcoef, acc, gnum, nsm, s);
-  }
-}
-
-template cudaError_t launch_fft512_xy_il<float>(const float *, void *, void *, int, int64_t, int,
-                                                int, const void *, int, cudaStream_t);
-template cudaError_t launch_fft512_xy_il<double>(const double *, void *, void *, int, int64_t,
-                                                 int, int, const void *, int, cudaStream_t);
-template cudaError_t launch_fft512_zbin<float>(const void *, int, const void *, const BinGeom &,
-                                               const float *, const float *, const float *,
-                                               const double *, const double *, double *,
-                                               double *, int, cudaStream_t);
-template cudaError_t launch_fft512_zbin<double>(const void *, int, const void *, const BinGeom &,
-                                                const double *, const double *, const double *,
-                                                const double *, const double *, double *,
-                                                double *, int, cudaStream_t);
-
 template cudaError_t launch_fft512<float>(const float *, void *, void *, void *, int, int64_t,
                                           int, int, int, const void *, int, cudaStream_t);
 template cudaError_t launch_fft512<double>(const double *, void *, void *, void *, int, int64_t,

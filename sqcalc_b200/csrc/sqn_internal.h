@@ -160,21 +160,6 @@ template <typename R>
 cudaError_t launch_fft512(const R *grid, void *A1, void *A2, void *G, int ntr, int64_t pitch,
                           int H1, int hm1, int hm2, const void *tw, int nsm, cudaStream_t s);
 
-// The same passes with the transforms interleaved and the z pass fused with
-// the shell binning (sqn_fft512.cu): grid -> A1 [512][512][H1][ntr] (x) ->
-// A2 [512][2 hm1 + 1][H1][ntr] (y) -> shell sums of b added into acc (z +
-// bin; no spectrum is written).  fft512_bin_fits: the fused pass's shared
-// memory (tile, twiddles, histograms) fits one CTA.
-bool fft512_bin_fits(const BinGeom &b, bool fp64);
-template <typename R>
-cudaError_t launch_fft512_xy_il(const R *grid, void *A1, void *A2, int ntr, int64_t pitch,
-                                int H1, int hm1, const void *tw, int nsm, cudaStream_t s);
-template <typename R>
-cudaError_t launch_fft512_zbin(const void *A2, int H1, const void *tw, const BinGeom &b,
-                               const R *inv1, const R *inv2, const R *inv3, const double *amp,
-                               const double *xcoef, double *acc, double *gnum, int nsm,
-                               cudaStream_t s);
-
 // Density amplitudes of requested lattice points from the half spectra.
 template <typename R>
 cudaError_t launch_gather_modes(const void *G, const BinGeom &b, const int *hkl, int64_t nm,

@@ -1,9 +1,6 @@
-"""Pruned 512-point FFT passes on 512^3 fine grids -- on the frame path the x
-and y passes with the transforms interleaved and the z pass fused with the
-shell binning (k_fft512_x, k_fft512_cols, k_fft512_zbin): S(q), the partials,
-the per-mode grid and the powder pattern against the same plan on cuFFT R2C +
-k_bin (SQN_FLAG_CUFFT), FP32 and FP64, 1 to 5 transforms; and the default
-512^3 path against the FP64 direct sum."""
+"""Pruned 512-point FFT passes (k_fft512_x, k_fft512_cols) on 512^3 fine grids:
+S(q), the partials and the per-mode grid against the same plan on cuFFT R2C
+(SQN_FLAG_CUFFT), FP32 and FP64."""
 import numpy as np
 import pytest
 
@@ -40,7 +37,6 @@ def test_pruned_passes_match_cufft(precision, eps, tol, grid):
             plan(tid, precision, eps, True, want_grid=grid) as pc:
         assert list(pp.info.nf) == [512, 512, 512]
         assert pp.info.pruned_fft512 == 1 and pc.info.pruned_fft512 == 0
-        assert pp.info.fused_zbin == 1 and pc.info.fused_zbin == 0
         for p in (pp, pc):
             for f in fr:
                 p.accumulate(f)
@@ -51,36 +47,8 @@ def test_pruned_passes_match_cufft(precision, eps, tol, grid):
         assert np.max(np.abs(a[1] - b[1])) / max(1.0, float(np.max(np.abs(b[1])))) < tol
         if grid:
             assert np.max(np.abs(a[2] - b[2])) / max(1.0, float(np.max(np.abs(b[2])))) < 10 * tol
-        # x, y and the fused z + bin pass against k_bin: two more kernels per frame
-        assert pp.launch_count() - pc.launch_count() == 2 * len(fr)
-
-
-@pytest.mark.parametrize("ntypes", [1, 2, 4, 5])
-def test_fused_zbin_transform_counts(ntypes):
-    """Every transform count the fused pass instantiates (1, 2, 4 unrolled; 5 on
-    the generic path) -- 16 // T h1 columns per step, T values per mode -- with
-    mixed-sign partials, against the cuFFT plan (FP32, 2e-6 of max |S|)."""
-    rng = np.random.default_rng(30 + ntypes)
-    n = 20000
-    tid = (rng.integers(0, ntypes, n) + 1).astype(np.int32)
-    base = rng.random((n, 3)) * L
-    fr = [base + rng.normal(0, 0.3, (n, 3)) for _ in range(2)]
-    b = np.linspace(3.0, 9.0, ntypes)
-
-    def mk(cufft):
-        return _lib.Plan(np.eye(3).reshape(9) * L, np.zeros(3), tid, ntypes=ntypes,
-                         weight=_lib.WEIGHT_NEUTRON, amp_const=b, qmin=0.5, qmax=QMAX, nq=250,
-                         partials=True, precision=_lib.PREC_SINGLE, eps=1e-6, cufft=cufft)
-    with mk(False) as pp, mk(True) as pc:
-        assert pp.info.fused_zbin == 1 and pp.info.ntransforms == ntypes
-        for p in (pp, pc):
-            for f in fr:
-                p.accumulate(f)
-        ca, cb = pp.accumulators()["shell_count"], pc.accumulators()["shell_count"]
-        np.testing.assert_array_equal(ca, cb)
-        a, c = pp.finalize(), pc.finalize()
-        for x, y in ((a[0], c[0]), (a[1], c[1])):
-            assert np.max(np.abs(x - y)) / max(1.0, float(np.max(np.abs(y)))) < 2e-6
+        # three more kernels per frame than the cuFFT plan
+        assert pp.launch_count() - pc.launch_count() == 3 * len(fr)
 
 
 def test_pruned_passes_xray_weights_and_powder_pattern():
@@ -99,7 +67,6 @@ def test_pruned_passes_xray_weights_and_powder_pattern():
                          cufft=cufft, xrd=xrd)
     with mk(False) as pp, mk(True) as pc:
         assert pp.info.pruned_fft512 == 1 and pc.info.pruned_fft512 == 0
-        assert pp.info.fused_zbin == 1
         for p in (pp, pc):
             for f in fr:
                 p.accumulate(f)
@@ -137,7 +104,6 @@ def test_default_512_path_against_direct_sum():
                        weight=_lib.WEIGHT_NEUTRON, amp_const=b, qmin=0.0, qmax=6.0, nq=500,
                        partials=True, precision=prec, eps=eps) as p:
             assert list(p.info.nf) == [512, 512, 512] and p.info.pruned_fft512 == 1
-            assert p.info.fused_zbin == 1
             for f in fr:
                 p.accumulate(f)
             counts = p.accumulators()["shell_count"]
