@@ -138,9 +138,10 @@ def test_cli_hdf5_grid_and_xrd_match_text_tables(tmp_path):
         np.testing.assert_allclose(x["xrd/I_partial/" + lab].value, xrd[:, 2 + j],
                                    rtol=1e-11, atol=1e-300)
     # --format text keeps a .h5 name a text table; an unknown format is exit 2
-    r = cli(base[:-1] + ["--format", "text", "--grid", str(tmp_path / "t.h5"), "-q",
-                         str(tmp_path / "s3.txt")])
+    r = cli(base[:-1] + ["--format", "text", "--grid", str(tmp_path / "t.h5"),
+                         "--xrd", str(tmp_path / "x3.h5"), "-q", str(tmp_path / "s3.txt")])
     assert r.returncode == 0, r.stderr
     assert open(str(tmp_path / "t.h5")).readline().startswith("# qx qy qz")
+    assert open(str(tmp_path / "x3.h5")).readline().startswith("# xrd: lambda")
     r = cli(base + ["--format", "csv", str(tmp_path / "s4.txt")])
     assert r.returncode == 2

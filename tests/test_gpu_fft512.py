@@ -51,6 +51,34 @@ def test_pruned_passes_match_cufft(precision, eps, tol, grid):
         assert pp.launch_count() - pc.launch_count() == 3 * len(fr)
 
 
+@pytest.mark.parametrize("ntypes", [1, 2, 4, 5])
+def test_pruned_passes_transform_counts(ntypes):
+    """Every transform count k_bin instantiates on the compact spectrum (1, 2, 4
+    unrolled; 5 on the generic path), with mixed-sign partials, against the
+    cuFFT plan (FP32, 2e-6 of max |S|; shell counts identical)."""
+    rng = np.random.default_rng(30 + ntypes)
+    n = 20000
+    tid = (rng.integers(0, ntypes, n) + 1).astype(np.int32)
+    base = rng.random((n, 3)) * L
+    fr = [base + rng.normal(0, 0.3, (n, 3)) for _ in range(2)]
+    b = np.linspace(3.0, 9.0, ntypes)
+
+    def mk(cufft):
+        return _lib.Plan(np.eye(3).reshape(9) * L, np.zeros(3), tid, ntypes=ntypes,
+                         weight=_lib.WEIGHT_NEUTRON, amp_const=b, qmin=0.5, qmax=QMAX, nq=250,
+                         partials=True, precision=_lib.PREC_SINGLE, eps=1e-6, cufft=cufft)
+    with mk(False) as pp, mk(True) as pc:
+        assert pp.info.pruned_fft512 == 1 and pp.info.ntransforms == ntypes
+        for p in (pp, pc):
+            for f in fr:
+                p.accumulate(f)
+        ca, cb = pp.accumulators()["shell_count"], pc.accumulators()["shell_count"]
+        np.testing.assert_array_equal(ca, cb)
+        a, c = pp.finalize(), pc.finalize()
+        for x, y in ((a[0], c[0]), (a[1], c[1])):
+            assert np.max(np.abs(x - y)) / max(1.0, float(np.max(np.abs(y)))) < 2e-6
+
+
 def test_pruned_passes_xray_weights_and_powder_pattern():
     """q-dependent (x-ray) amplitudes and the two-theta histogram of the powder
     pattern read from the compact spectrum, against the cuFFT plan."""
