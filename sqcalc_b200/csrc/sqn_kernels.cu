@@ -177,17 +177,12 @@ __device__ __forceinline__ void load_z8(const double *src, double (&z)[8]) {
   }
 }
 
-// c0 += a z0, c1 += a z1: one packed FP32 FMA (fma.rn.f32x2, sm_100) in FP32,
-// two FMAs in FP64.
+// c0 += a z0, c1 += a z1: one packed FP32 FMA (the sm_100 builtin, which the
+// register allocator sees through) in FP32, two FMAs in FP64.
 __device__ __forceinline__ void fma2(float a, float z0, float z1, float &c0, float &c1) {
-  asm("{\n\t.reg .b64 pa, pz, pc;\n\t"
-      "mov.b64 pa, {%2, %2};\n\t"
-      "mov.b64 pz, {%3, %4};\n\t"
-      "mov.b64 pc, {%0, %1};\n\t"
-      "fma.rn.f32x2 pc, pa, pz, pc;\n\t"
-      "mov.b64 {%0, %1}, pc;\n\t}"
-      : "+f"(c0), "+f"(c1)
-      : "f"(a), "f"(z0), "f"(z1));
+  const float2 r = __ffma2_rn(make_float2(a, a), make_float2(z0, z1), make_float2(c0, c1));
+  c0 = r.x;
+  c1 = r.y;
 }
 __device__ __forceinline__ void fma2(double a, double z0, double z1, double &c0, double &c1) {
   c0 = fma(a, z0, c0);
