@@ -59,15 +59,19 @@ __device__ __forceinline__ uint32_t home_key(const AtomCell &c, const FrameGeom 
 
 // ES kernel: phi(t) = exp(beta (sqrt(1 - (2t/w)^2) - 1)) on |t| < w/2, else 0
 // (external/finufft/include/cufinufft/spreadinterp.h:84-98).
-// FP32: the hardware approximations of sqrt and 2^x (relative errors near
-// 2^-22 on the kernel values, below the FP32 plans' smallest eps, FLT_EPSILON;
-// the error of a value far out in the tail is relative to that small value).
+// FP32: the hardware approximations of sqrt and 2^x, exp(u) = 2^(u log2 e)
+// (relative errors near 2^-22 on the kernel values, below the FP32 plans'
+// smallest eps, FLT_EPSILON; the error of a value far out in the tail is
+// relative to that small value).  Both in their flush-to-zero forms: the
+// arguments are 1 - z2 in (0, 1] and beta (r - 1) log2 e in [-beta log2 e, 0]
+// (beta < 40), and the results sqrt in (0, 1] and 2^x >= 2^-58, all normal.
 __device__ __forceinline__ float es_phi(float t, float c2, float beta) {
+  constexpr float kLog2e = 1.44269504088896340736f;
   const float z2 = c2 * t * t;
-  if (!(z2 < 1.0f)) return 0.0f;
-  float r;
-  asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(1.0f - z2));
-  return __expf(beta * (r - 1.0f));
+  float r, e;
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(fmaxf(1.0f - z2, 0.0f)));
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(e) : "f"(beta * (r - 1.0f) * kLog2e));
+  return z2 < 1.0f ? e : 0.0f;
 }
 __device__ __forceinline__ double es_phi(double t, double c2, double beta) {
   const double z2 = c2 * t * t;

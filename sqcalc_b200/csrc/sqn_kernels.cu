@@ -363,13 +363,17 @@ __device__ __forceinline__ void spread_tile(const R *__restrict__ recs,
           const unsigned bal = __ballot_sync(FULL, keep);
           if (lane == 0) s_wcount[warp] = __popc(bal);
           __syncthreads();
-          int woff = 0, btot = 0;
+          // offsets of the warps' kept points: an inclusive scan of the warp
+          // counts across lanes, read back at this warp
+          const int wc = lane < SPREAD_WARPS ? s_wcount[lane] : 0;
+          int wincl = wc;
 #pragma unroll
-          for (int k = 0; k < SPREAD_WARPS; ++k) {
-            const int c = s_wcount[k];
-            woff += k < warp ? c : 0;
-            btot += c;
+          for (int o = 1; o < SPREAD_WARPS; o <<= 1) {
+            const int t = __shfl_up_sync(FULL, wincl, o);
+            if (lane >= o) wincl += t;
           }
+          const int woff = __shfl_sync(FULL, wincl - wc, warp);
+          const int btot = __shfl_sync(FULL, wincl, SPREAD_WARPS - 1);
           const int k = kbase + woff + __popc(bal & ((1u << lane) - 1u)) - win;
           if (keep && k >= 0 && k < cap) {
             s_meta[k] = meta;
@@ -400,11 +404,15 @@ __device__ __forceinline__ void spread_tile(const R *__restrict__ recs,
           R *row = s_rows + (size_t)p * SPREAD_ROW +
                    (d == 0 ? 0 : (d == 1 ? TILE_X : TILE_X + TILE_Y));
           for (int j = 0; j < len; j += 4) store_rec(row + j, R(0), R(0), R(0), R(0));
-          // support cell k sits at tile cell rel + k, cyclically (rel in [0, n))
-          for (int k = 0; k < w; ++k) {
-            int cell = rel + k;
-            if (cell >= n) cell -= n;
-            if (cell < lim) row[cell] = es_at(k, off, halfw, c2, beta) * sc;
+          // support cell k sits at tile cell rel + k, cyclically (rel in [0, n));
+          // unrolled to the largest width so the evaluations overlap
+#pragma unroll
+          for (int k = 0; k < MAX_W; ++k) {
+            if (k < w) {
+              int cell = rel + k;
+              if (cell >= n) cell -= n;
+              if (cell < lim) row[cell] = es_at(k, off, halfw, c2, beta) * sc;
+            }
           }
         }
         __syncthreads();
