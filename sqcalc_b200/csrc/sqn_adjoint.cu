@@ -92,19 +92,24 @@ __global__ void __launch_bounds__(256, 2)
 // One warp per atom in bin-sorted order: U_i(s_j) by ES interpolation of the
 // three real grids, then dL/dr_j = 2 c_j sum_i b_i U_i.  Lanes 0..w-1 evaluate
 // the kernel values of the support along each axis (the same expression as
-// the spread); lanes then take (dy, dz) pairs of the support and walk the x
-// row, the values broadcast by shuffles.
+// the spread).  The two half-warps then walk the w^2 (dy, dz) rows of the
+// support, alternately, with lane x of a half on cell dx = x of the row, so a
+// load instruction reads two contiguous row segments (not 32 scattered
+// cells); each lane accumulates its cells' weighted values in FP64 and the
+// warp sums them at the end.
 template <typename R>
 __global__ void __launch_bounds__(256)
     k_interp(const R *__restrict__ recs, const int32_t *__restrict__ orig,
              const double *__restrict__ pos, FrameGeom g, const R *__restrict__ U, Recip rb,
              const double *__restrict__ camp, double *__restrict__ grad) {
   const int lane = threadIdx.x & 31;
+  const int half = lane >> 4, x = lane & 15;
   const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
-  const int w = g.w, ww = w * w;
+  const int w = g.w;
   const R halfw = R(0.5) * (R)w - R(0.5);
   const R c2 = R(4) / ((R)w * (R)w);
   const R beta = (R)g.beta;
+  const bool xin = x < w;  // w <= MAX_W = 16
   for (int64_t p = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); p < g.natoms;
        p += nwarps) {
     const int j = orig[p];
@@ -117,32 +122,37 @@ __global__ void __launch_bounds__(256)
     const R kxl = es_at(kl, rec[1], halfw, c2, beta);
     const R kyl = es_at(kl, rec[2], halfw, c2, beta);
     const R kzl = es_at(kl, rec[3], halfw, c2, beta);
+    const R kx = __shfl_sync(FULL, kxl, x);  // this lane's x weight (lanes x < w)
+    int ix = c.ix0[0] + x;
+    if (ix >= g.nf[0]) ix -= g.nf[0];
     double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-    for (int base = 0; base < ww; base += 32) {
-      const int idx = base + lane;
-      const bool act = idx < ww;
-      const int dz = act ? idx / w : 0, dy = act ? idx - dz * w : 0;
+    // rows r = half, half + 2, ...: (dy, dz) = (r mod w, r / w), advanced by two
+    int dy = half, dz = 0;
+    if (dy >= w) {
+      dy -= w;
+      ++dz;
+    }
+    // every lane runs the same iterations (the shuffles are warp-wide); the
+    // odd row count leaves the second half one row short on its last step
+    const int nrow = w * w, niter = (nrow + 1) >> 1;
+    for (int i = 0; i < niter; ++i) {
+      const bool rin = half + 2 * i < nrow;
       int iy = c.ix0[1] + dy;
       if (iy >= g.nf[1]) iy -= g.nf[1];
       int iz = c.ix0[2] + dz;
       if (iz >= g.nf[2]) iz -= g.nf[2];
-      const int64_t rowoff = ((int64_t)iz * g.nf[1] + iy) * g.pitch;
-      const R wyz = __shfl_sync(FULL, kyl, dy) * __shfl_sync(FULL, kzl, dz);
-      R u0 = 0, u1 = 0, u2 = 0;
-      for (int dx = 0; dx < w; ++dx) {
-        int ix = c.ix0[0] + dx;
-        if (ix >= g.nf[0]) ix -= g.nf[0];
-        const R k = __shfl_sync(FULL, kxl, dx);
-        if (act) {
-          u0 += k * U[rowoff + ix];
-          u1 += k * U[g.vol_real + rowoff + ix];
-          u2 += k * U[2 * g.vol_real + rowoff + ix];
-        }
+      const R wyz = __shfl_sync(FULL, kyl, dy & 31) * __shfl_sync(FULL, kzl, dz & 31);
+      if (xin && rin) {
+        const int64_t o = ((int64_t)iz * g.nf[1] + iy) * g.pitch + ix;
+        const double k = (double)(wyz * kx);
+        a0 = fma(k, (double)U[o], a0);
+        a1 = fma(k, (double)U[g.vol_real + o], a1);
+        a2 = fma(k, (double)U[2 * g.vol_real + o], a2);
       }
-      if (act) {
-        a0 += (double)wyz * (double)u0;
-        a1 += (double)wyz * (double)u1;
-        a2 += (double)wyz * (double)u2;
+      dy += 2;
+      if (dy >= w) {
+        dy -= w;
+        ++dz;
       }
     }
     a0 = warp_sum(a0);
