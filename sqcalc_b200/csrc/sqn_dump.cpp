@@ -95,6 +95,71 @@ bool parse_double(const char *b, const char *e, double &v) {
   return r.ec == std::errc() && r.ptr == e;
 }
 
+// Exact powers of ten 1e0 .. 1e22 (every one is a double without rounding).
+constexpr double kPow10[23] = {1e0,  1e1,  1e2,  1e3,  1e4,  1e5,  1e6,  1e7,
+                               1e8,  1e9,  1e10, 1e11, 1e12, 1e13, 1e14, 1e15,
+                               1e16, 1e17, 1e18, 1e19, 1e20, 1e21, 1e22};
+
+// The same double as parse_double, faster for the plain decimals of a dump:
+// when the significant digits form an integer w < 2^53 and the decimal
+// exponent e satisfies |e| <= 22, w and 10^|e| are exact doubles and one IEEE
+// multiplication or division rounds w * 10^e correctly (Clinger's fast path,
+// W. D. Clinger, "How to read floating point numbers accurately", PLDI 1990).
+// Anything else (more digits, larger exponents, inf, nan, stray characters)
+// goes to std::from_chars.
+bool parse_double_fast(const char *b, const char *e, double &v) {
+  const char *p = b;
+  bool neg = false;
+  if (p < e && (*p == '+' || *p == '-')) neg = *p++ == '-';
+  uint64_t w = 0;
+  int sig = 0, e10 = 0;
+  bool digit = false, ok = true;
+  for (; p < e && (unsigned)(*p - '0') < 10u; ++p) {
+    digit = true;
+    const int d = *p - '0';
+    if (sig == 0 && d == 0) continue;
+    if (sig < 19) {
+      w = w * 10 + (uint64_t)d;
+      ++sig;
+    } else {
+      ok = false;
+    }
+  }
+  if (p < e && *p == '.') {
+    for (++p; p < e && (unsigned)(*p - '0') < 10u; ++p) {
+      digit = true;
+      const int d = *p - '0';
+      if (sig == 0 && d == 0) {
+        --e10;
+        continue;
+      }
+      if (sig < 19) {
+        w = w * 10 + (uint64_t)d;
+        ++sig;
+        --e10;
+      } else {
+        ok = false;
+      }
+    }
+  }
+  if (ok && digit && p < e && (*p == 'e' || *p == 'E')) {
+    const char *q = p + 1;
+    bool eneg = false;
+    if (q < e && (*q == '+' || *q == '-')) eneg = *q++ == '-';
+    int x = 0, nx = 0;
+    for (; q < e && (unsigned)(*q - '0') < 10u && nx < 6; ++q, ++nx) x = x * 10 + (*q - '0');
+    if (nx == 0) ok = false;
+    e10 += eneg ? -x : x;
+    p = q;
+  }
+  if (!(ok && digit && p == e && w < (1ull << 53) && e10 >= -22 && e10 <= 22))
+    return parse_double(b, e, v);
+  double r = (double)w;
+  r = e10 >= 0 ? r * kPow10[e10] : r / kPow10[-e10];
+  v = neg ? -r : r;
+  return true;
+}
+
 bool parse_int(const char *b, const char *e, int64_t &v) {
   if (b < e && *b == '+') ++b;
   auto r = std::from_chars(b, e, v);
@@ -115,33 +180,98 @@ struct Columns {
   int id = -1, type = -1, x = -1, y = -1, z = -1, ncol = 0;
 };
 
-// Parse lines [first, first + count) starting at text offset `off` of a block.
+// The end of the token at q: the first ' ', '\t', '\r' or '\n' at or after q,
+// or e.  Eight bytes at a time: the lowest flagged byte of
+// (w - 0x21...) & ~w & 0x80... is the first byte below 0x21 (a borrow only
+// flags bytes above a true one); other control bytes stay in the token.
+const char *token_end(const char *q, const char *e) {
+  for (;;) {
+    while (q + 8 <= e) {
+      uint64_t w;
+      std::memcpy(&w, q, 8);
+      const uint64_t m = (w - 0x2121212121212121ull) & ~w & 0x8080808080808080ull;
+      if (m) {
+        q += __builtin_ctzll(m) >> 3;
+        break;
+      }
+      q += 8;
+    }
+    while (q < e && (unsigned char)*q > 0x20) ++q;
+    if (q >= e || is_space(*q) || *q == '\n') return q;
+    ++q;  // a control byte inside the token
+  }
+}
+
+// Parse lines [first, first + count) of a block, the first starting at p: the
+// columns are walked in one pass (a line needs at least ncol tokens; later
+// tokens are ignored) and only id, type and the coordinates are converted.
 int parse_lines(const char *p, const char *end, int64_t first, int64_t count, const Columns &c,
                 double *pos, int32_t *type_id, int64_t *ids) {
-  std::vector<std::pair<const char *, const char *>> tk;
   for (int64_t i = first; i < first + count; ++i) {
-    const char *nl = static_cast<const char *>(std::memchr(p, '\n', (size_t)(end - p)));
-    const char *le = nl ? nl : end;
-    if (tokens(p, le, tk) < c.ncol) return 8;
-    double x, y, z;
-    int64_t t;
-    if (!parse_double(tk[c.x].first, tk[c.x].second, x) ||
-        !parse_double(tk[c.y].first, tk[c.y].second, y) ||
-        !parse_double(tk[c.z].first, tk[c.z].second, z) ||
-        !parse_int(tk[c.type].first, tk[c.type].second, t))
-      return 8;
-    pos[3 * i + 0] = x;
-    pos[3 * i + 1] = y;
-    pos[3 * i + 2] = z;
-    type_id[i] = (int32_t)t;
-    if (ids) {
-      int64_t id = i + 1;
-      if (c.id >= 0 && !parse_int(tk[c.id].first, tk[c.id].second, id)) return 8;
-      ids[i] = id;
+    double xyz[3] = {0.0, 0.0, 0.0};
+    int64_t t = 0, id = i + 1;
+    const char *q = p;
+    for (int col = 0; col < c.ncol; ++col) {
+      while (q < end && is_space(*q)) ++q;
+      if (q >= end || *q == '\n') return 8;
+      const char *tb = q;
+      q = token_end(q, end);
+      if (col == c.x || col == c.y || col == c.z) {
+        double v;
+        if (!parse_double_fast(tb, q, v)) return 8;
+        if (col == c.x) xyz[0] = v;
+        if (col == c.y) xyz[1] = v;
+        if (col == c.z) xyz[2] = v;
+      }
+      if (col == c.type && !parse_int(tb, q, t)) return 8;
+      if (ids && col == c.id && !parse_int(tb, q, id)) return 8;
     }
+    pos[3 * i + 0] = xyz[0];
+    pos[3 * i + 1] = xyz[1];
+    pos[3 * i + 2] = xyz[2];
+    type_id[i] = (int32_t)t;
+    if (ids) ids[i] = id;
+    const char *nl = static_cast<const char *>(std::memchr(q, '\n', (size_t)(end - q)));
     p = nl ? nl + 1 : end;
   }
   return 0;
+}
+
+// Newlines in [b, e), eight bytes at a time: for x = word ^ 0x0a0a..., a byte
+// of x is zero exactly when the high bit of ((x & 0x7f..) + 0x7f..) | x is clear
+// in it (the addition cannot carry across bytes).
+size_t count_newlines(const char *b, const char *e) {
+  size_t n = 0;
+  const char *p = b;
+  constexpr uint64_t kNl = 0x0a0a0a0a0a0a0a0aull, k7f = 0x7f7f7f7f7f7f7f7full;
+  for (; p + 8 <= e; p += 8) {
+    uint64_t w;
+    std::memcpy(&w, p, 8);
+    const uint64_t x = w ^ kNl;
+    const uint64_t t = ((x & k7f) + k7f) | x;
+    n += (size_t)__builtin_popcountll(~t & ~k7f);
+  }
+  for (; p < e; ++p) n += *p == '\n';
+  return n;
+}
+
+// The position just past the n-th newline at or after `from` (n >= 1), or
+// size when the file has fewer: whole 4 KB blocks are counted, the block
+// holding the newline is scanned.
+size_t nth_newline(const char *base, size_t size, size_t from, int64_t n) {
+  size_t p = from;
+  while (p < size) {
+    const size_t q = std::min(size, p + 4096);
+    const int64_t c = (int64_t)count_newlines(base + p, base + q);
+    if (c < n) {
+      n -= c;
+      p = q;
+      continue;
+    }
+    for (; p < q; ++p)
+      if (base[p] == '\n' && --n == 0) return p + 1;
+  }
+  return size;
 }
 
 // One frame.  0 ok, 1 end of file (no further frame), 4-9 malformed.
@@ -201,34 +331,70 @@ int read_frame(sqn_dump *d, int64_t capacity, int64_t *natoms_out, int64_t *time
   }
   *natoms_out = natoms;
   if (natoms > capacity) return -1;  // caller's buffers too small
-  // the ATOMS block: find its end and each thread's first line
-  const int nt = (int)std::max<int64_t>(1, std::min<int64_t>(d->nthreads, natoms / 4096 + 1));
-  const int64_t per = (natoms + nt - 1) / nt;
-  std::vector<size_t> starts((size_t)nt + 1, d->size);
-  size_t p = off;
-  for (int64_t i = 0; i < natoms; ++i) {
-    if (i % per == 0) starts[(size_t)(i / per)] = p;
-    if (p >= d->size) return 8;
-    const void *nl = std::memchr(d->base + p, '\n', d->size - p);
-    p = nl ? (size_t)(static_cast<const char *>(nl) - d->base) + 1 : d->size;
+  // The ATOMS block: natoms lines from off.  Threads split a byte region that
+  // should hold it (twice the first line's length per atom, widened when it
+  // does not) and count the lines that start in their parts; a prefix over the
+  // parts gives every part's first line index, the block end, and then the
+  // threads parse the lines that start in their parts, all in parallel.
+  int nt = (int)std::max<int64_t>(1, std::min<int64_t>(d->nthreads, natoms / 4096 + 1));
+  const char *base = d->base;
+  const size_t size = d->size;
+  if (off >= size) return 8;
+  size_t len1;
+  {
+    const void *nl = std::memchr(base + off, '\n', size - off);
+    len1 = nl ? (size_t)(static_cast<const char *>(nl) - (base + off)) + 1 : size - off;
   }
-  const size_t block_end = p;
-  std::vector<int> err((size_t)nt, 0);
-  auto work = [&](int k) {
-    const int64_t first = (int64_t)k * per;
-    const int64_t count = std::min<int64_t>(per, natoms - first);
-    if (count <= 0) return;
-    err[(size_t)k] = parse_lines(d->base + starts[(size_t)k], d->base + block_end, first, count,
-                                 c, pos, type_id, ids);
-  };
-  if (nt == 1) {
-    work(0);
-  } else {
+  auto run = [&](auto &&fn) {
+    if (nt == 1) {
+      fn(0);
+      return;
+    }
     std::vector<std::thread> th;
-    for (int k = 1; k < nt; ++k) th.emplace_back(work, k);
-    work(0);
+    for (int k = 1; k < nt; ++k) th.emplace_back(fn, k);
+    fn(0);
     for (auto &t : th) t.join();
+  };
+  size_t region = std::min(size - off, (size_t)natoms * len1 * 2 + ((size_t)1 << 16));
+  if (region < (size_t)nt * 4096) nt = 1;  // every part past the first starts 4 KB in
+  std::vector<size_t> a((size_t)nt + 1);
+  std::vector<int64_t> lines((size_t)nt), first((size_t)nt + 1);
+  for (;;) {
+    for (int k = 0; k <= nt; ++k) a[(size_t)k] = off + region * (size_t)k / (size_t)nt;
+    // lines starting in [a_k, a_k+1): those after a newline in [a_k - 1, a_k+1 - 1)
+    // (line 0 starts at off itself)
+    run([&](int k) {
+      const size_t lo = k == 0 ? off : a[(size_t)k] - 1, hi = a[(size_t)k + 1] - 1;
+      lines[(size_t)k] = (k == 0 ? 1 : 0) + (int64_t)count_newlines(base + lo, base + std::max(lo, hi));
+    });
+    first[0] = 0;
+    for (int k = 0; k < nt; ++k) first[(size_t)k + 1] = first[(size_t)k] + lines[(size_t)k];
+    if (first[(size_t)nt] >= natoms || off + region == size) break;
+    region = std::min(size - off, region * 2);
   }
+  if (first[(size_t)nt] < natoms) return 8;  // the file ends inside the block
+  // the block ends where line natoms starts: after the (natoms - first_j + 1)-th
+  // newline from a_j - 1 for the part j holding line natoms - 1 (from off, the
+  // natoms-th, for part 0), or at the end of the file
+  size_t block_end;
+  {
+    int j = 0;
+    while (first[(size_t)j + 1] <= natoms - 1) ++j;
+    const size_t from = j == 0 ? off : a[(size_t)j] - 1;
+    block_end = nth_newline(base, size, from, natoms - first[(size_t)j] + (j == 0 ? 0 : 1));
+  }
+  std::vector<int> err((size_t)nt, 0);
+  run([&](int k) {
+    const int64_t i0 = first[(size_t)k];
+    const int64_t count = std::min<int64_t>(first[(size_t)k + 1], natoms) - i0;
+    if (count <= 0) return;
+    size_t q = off;
+    if (k > 0) {
+      const void *nl = std::memchr(base + a[(size_t)k] - 1, '\n', size - (a[(size_t)k] - 1));
+      q = (size_t)(static_cast<const char *>(nl) - base) + 1;
+    }
+    err[(size_t)k] = parse_lines(base + q, base + block_end, i0, count, c, pos, type_id, ids);
+  });
   for (int v : err)
     if (v) return v;
   *timestep = ts;

@@ -91,3 +91,31 @@ def test_end_of_file_and_rewind(tmp_path):
         assert r.next() is None
         r.rewind()
         assert r.next() is not None
+
+
+def test_coordinate_parsing_is_correctly_rounded(tmp_path):
+    """The reader's fast decimal path (Clinger's: an integer significand below
+    2^53 and a power of ten up to 22) and its fallback give the correctly rounded
+    double of every coordinate, whatever the format: fixed, %.17g, exponents,
+    signs, leading zeros, 20-digit significands, huge and tiny values."""
+    rng = np.random.default_rng(12)
+    n = 3000
+    vals = np.concatenate([rng.random(n) * 220.0, -rng.random(n) * 1e-3,
+                           rng.standard_normal(n) * 1e6, 10.0 ** rng.uniform(-30, 30, n)])
+    fmts = ["%.6f", "%.17g", "%.3e", "%+.9f", "%.20f", "%.15g", "%.1f", "%.12E"]
+    texts = [fmts[i % len(fmts)] % v for i, v in enumerate(vals)]
+    texts[:6] = ["0", "-0.0", ".5", "5.", "000123.4500", "1e22"]
+    m = len(texts) // 3
+    lines = ["%d 1 %s %s %s" % (i + 1, texts[3 * i], texts[3 * i + 1], texts[3 * i + 2])
+             for i in range(m)]
+    path = str(tmp_path / "fmt.dump")
+    with open(path, "w") as fh:
+        fh.write("ITEM: TIMESTEP\n0\nITEM: NUMBER OF ATOMS\n%d\nITEM: BOX BOUNDS pp pp pp\n"
+                 "0 1\n0 1\n0 1\nITEM: ATOMS id type x y z\n" % m)
+        fh.write("\n".join(lines) + "\n")
+    want = np.array([float(t) for t in texts[:3 * m]]).reshape(m, 3)
+    for nt in (1, 4):
+        got = all_frames(path, nt)
+        assert len(got) == 1
+        pos = got[0][3]
+        assert np.array_equal(pos.view(np.uint64), want.view(np.uint64))
