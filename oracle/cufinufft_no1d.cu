@@ -3,7 +3,7 @@
 // sm_100a crashes the CUDA 12.9 device front end (cicc segmentation fault).
 // The benchmark's reference bar only makes 3D type-1 plans, so the 1D spread
 // entry points that cufinufft.cu's dimension dispatch names answer
-// FINUFFT_ERR_DIM_NOTVALID.  TEST AND BASELINE INFRASTRUCTURE ONLY.
+// FINUFFT_ERR_DIM_NOTVALID.  Test and baseline infrastructure only.
 #include <cufinufft/spreadinterp.h>
 #include <cufinufft/types.h>
 #include <finufft_errors.h>

@@ -1,6 +1,6 @@
 """The reference's own cuFINUFFT, built from thatstar/sqcalc's vendored sources
 (external/finufft/src/cuda) for sm_100a by oracle/cufinufft.mk into
-oracle/_ref/libcufinufft.so.  TEST AND BASELINE INFRASTRUCTURE ONLY: the GPU
+oracle/_ref/libcufinufft.so.  Test and baseline infrastructure only: the GPU
 tests compare this library's type-1 transforms and S(q) with it, and the
 benchmark times it as the reference's GPU bar; the product never loads it.
 

@@ -1,6 +1,6 @@
 /*
- * CPU restatement of the NUFFT form of the static S(q) path.  TEST AND CPU-BASELINE
- * INFRASTRUCTURE ONLY: it is the timed CPU baseline of the benchmark and a second
+ * CPU restatement of the NUFFT form of the static S(q) path.  Test and CPU-baseline
+ * infrastructure only: it is the timed CPU baseline of the benchmark and a second
  * checker for the tests; the product path never links or calls it.
  *
  * The reference's CPU path is FINUFFT (sort, spread, FFTW, deconvolve; called
