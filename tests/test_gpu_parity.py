@@ -256,3 +256,47 @@ def test_stage_timing_and_reset(golden_dir):
     assert m.plan.accumulators()["nframes"] == 0
     assert float(np.max(np.abs(m.plan.accumulators()["num"]))) == 0.0
     m.close()
+
+
+@pytest.mark.parametrize("precision,tol", [("double", 1e-9), ("single", 1e-5)])
+def test_edge_shapes_against_oracle(precision, tol):
+    """Small and degenerate inputs the reference accepts: one atom (S = 1 on
+    every populated shell, exactly |rho|^2 / N = 1), two atoms of two types, a
+    5-mode grid (two shells of lattice points), a single shell, a thin q window
+    with empty shells, a triclinic cell with an offset origin -- each against
+    the FP64 direct sum (partials included)."""
+    rng = np.random.default_rng(21)
+    unit = WeightScheme.from_options("unit")
+    neutron = WeightScheme.from_options("neutron", "1:Si,2:O")
+    tri = Cell(a=np.array([[9.0, 0.0, 0.0], [2.5, 7.0, 0.0], [-1.5, 3.0, 11.0]]),
+               origin=np.array([-2.0, 1.0, 0.5]))
+    cases = [
+        # (frames, scheme, kw)
+        ([F(rng.random((1, 3)) * 10, [1], Cell.cubic(10.0))], unit,
+         dict(norm="mean", qmax=5.0, nq=40)),
+        ([F(rng.random((2, 3)) * 12, [1, 2], Cell.cubic(12.0)) for _ in range(3)], neutron,
+         dict(norm="mean", qmax=4.0, nq=25)),
+        ([F(rng.random((50, 3)) * 30, rng.integers(1, 3, 50), Cell.cubic(30.0))], unit,
+         dict(norm="n", qmax=0.3, nq=3)),   # 5 modes per axis
+        ([F(rng.random((300, 3)) * 15, rng.integers(1, 3, 300), Cell.cubic(15.0))
+          for _ in range(2)], neutron, dict(norm="self", qmin=0.0, qmax=3.0, nq=1)),
+        ([F(rng.random((300, 3)) * 15, rng.integers(1, 3, 300), Cell.cubic(15.0))], unit,
+         dict(norm="mean", qmin=2.40, qmax=2.47, nq=5)),
+        ([F(rng.random((200, 3)) @ tri.a + tri.origin, rng.integers(1, 3, 200), tri)
+          for _ in range(2)], neutron, dict(norm="mean", qmax=4.5, nq=30)),
+    ]
+    for frames, scheme, kw in cases:
+        kw = dict(kw)
+        qmin = kw.pop("qmin", 0.0)
+        S, Sp, _ = gpu_run(frames, scheme, precision=precision,
+                           eps=1e-10 if precision == "double" else 1e-6, qmin=qmin, **kw)
+        _, acc = oracle_run(frames, scheme, qmin, kw["qmax"], kw["nq"], kw["norm"])
+        ref = acc.shell_value()
+        assert rel_dev(ref, S) < tol, (kw, rel_dev(ref, S))
+        T = Sp.shape[0]
+        for a in range(1, T + 1):
+            for b in range(a, T + 1):
+                assert rel_dev(acc.partial_value(a, b), Sp[a - 1, b - 1]) < tol
+        if len(frames[0].type_id) == 1:
+            pop = acc.shell_count > 0
+            assert np.all(np.abs(S[pop] - 1.0) < tol)
