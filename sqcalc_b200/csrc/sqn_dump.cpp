@@ -23,6 +23,9 @@
 #include <unistd.h>
 
 #include <cuda_runtime.h>
+#if defined(__SSE2__)
+#include <emmintrin.h>
+#endif
 
 #include <algorithm>
 #include <cctype>
@@ -100,48 +103,75 @@ constexpr double kPow10[23] = {1e0,  1e1,  1e2,  1e3,  1e4,  1e5,  1e6,  1e7,
                                1e8,  1e9,  1e10, 1e11, 1e12, 1e13, 1e14, 1e15,
                                1e16, 1e17, 1e18, 1e19, 1e20, 1e21, 1e22};
 
+// The leading decimal digits of the eight bytes at p (p + 8 <= the readable
+// end): how many (0 .. 8) and their value.  With x = word ^ '0'...'0', a byte
+// is a digit when x < 10: the lowest flagged byte of ((x + 0x76..) | x) &
+// 0x80.. is the first non-digit (carries only flag bytes above it).  The
+// digits are moved to the top of the word (leading zero digits below) and
+// combined pairwise: 8 digits in three multiplications.
+inline int digits8(const char *p, uint64_t &val) {
+  uint64_t w;
+  std::memcpy(&w, p, 8);
+  const uint64_t x = w ^ 0x3030303030303030ull;
+  const uint64_t m = ((x + 0x7676767676767676ull) | x) & 0x8080808080808080ull;
+  const int n = m ? (__builtin_ctzll(m) >> 3) : 8;
+  if (n == 0) {
+    val = 0;
+    return 0;
+  }
+  uint64_t y = n == 8 ? x : x << (8 * (8 - n));
+  y = (y * 10) + (y >> 8);
+  y = (((y & 0x000000FF000000FFull) * (100 + (1000000ull << 32))) +
+       (((y >> 16) & 0x000000FF000000FFull) * (1 + (10000ull << 32)))) >> 32;
+  val = y;
+  return n;
+}
+
+constexpr uint64_t kPow10i[9] = {1, 10, 100, 1000, 10000, 100000, 1000000, 10000000,
+                                 100000000};
+
 // The same double as parse_double, faster for the plain decimals of a dump:
-// when the significant digits form an integer w < 2^53 and the decimal
-// exponent e satisfies |e| <= 22, w and 10^|e| are exact doubles and one IEEE
-// multiplication or division rounds w * 10^e correctly (Clinger's fast path,
-// W. D. Clinger, "How to read floating point numbers accurately", PLDI 1990).
-// Anything else (more digits, larger exponents, inf, nan, stray characters)
-// goes to std::from_chars.
-bool parse_double_fast(const char *b, const char *e, double &v) {
+// when the digits form an integer w < 2^53 (at most 19 digits read) and the
+// decimal exponent e satisfies |e| <= 22, w and 10^|e| are exact doubles and
+// one IEEE multiplication or division rounds w * 10^e correctly (Clinger's
+// fast path, W. D. Clinger, "How to read floating point numbers accurately",
+// PLDI 1990).  Digits are read eight at a time while 8 bytes stay readable
+// (before `lim`).  Anything else (more digits, larger exponents, inf, nan,
+// stray characters) goes to std::from_chars.
+bool parse_double_fast(const char *b, const char *e, const char *lim, double &v) {
   const char *p = b;
   bool neg = false;
   if (p < e && (*p == '+' || *p == '-')) neg = *p++ == '-';
   uint64_t w = 0;
-  int sig = 0, e10 = 0;
-  bool digit = false, ok = true;
-  for (; p < e && (unsigned)(*p - '0') < 10u; ++p) {
-    digit = true;
-    const int d = *p - '0';
-    if (sig == 0 && d == 0) continue;
-    if (sig < 19) {
-      w = w * 10 + (uint64_t)d;
-      ++sig;
-    } else {
-      ok = false;
-    }
-  }
-  if (p < e && *p == '.') {
-    for (++p; p < e && (unsigned)(*p - '0') < 10u; ++p) {
-      digit = true;
-      const int d = *p - '0';
-      if (sig == 0 && d == 0) {
-        --e10;
-        continue;
-      }
-      if (sig < 19) {
-        w = w * 10 + (uint64_t)d;
-        ++sig;
-        --e10;
+  int nd = 0, e10 = 0;
+  auto run = [&](bool frac) {
+    for (;;) {
+      int n;
+      uint64_t val;
+      if (p + 8 <= lim) {
+        n = digits8(p, val);
+        if (p + n > e) n = (int)(e - p), val = 0, nd = 99;  // digits past the token: give up
       } else {
-        ok = false;
+        n = 0;
+        val = 0;
+        while (p + n < e && (unsigned)(p[n] - '0') < 10u && n < 8) val = val * 10 + (uint64_t)(p[n++] - '0');
       }
+      if (n == 0) return;
+      nd += n;
+      if (nd <= 19) w = w * kPow10i[n] + val;
+      if (frac) e10 -= n;
+      p += n;
+      if (n < 8) return;
     }
+  };
+  run(false);
+  const bool int_digits = nd > 0;
+  if (p < e && *p == '.') {
+    ++p;
+    run(true);
   }
+  const bool digit = nd > 0 || int_digits;
+  bool ok = nd <= 19;
   if (ok && digit && p < e && (*p == 'e' || *p == 'E')) {
     const char *q = p + 1;
     bool eneg = false;
@@ -218,7 +248,7 @@ int parse_lines(const char *p, const char *end, int64_t first, int64_t count, co
       q = token_end(q, end);
       if (col == c.x || col == c.y || col == c.z) {
         double v;
-        if (!parse_double_fast(tb, q, v)) return 8;
+        if (!parse_double_fast(tb, q, end, v)) return 8;
         if (col == c.x) xyz[0] = v;
         if (col == c.y) xyz[1] = v;
         if (col == c.z) xyz[2] = v;
@@ -237,12 +267,19 @@ int parse_lines(const char *p, const char *end, int64_t first, int64_t count, co
   return 0;
 }
 
-// Newlines in [b, e), eight bytes at a time: for x = word ^ 0x0a0a..., a byte
-// of x is zero exactly when the high bit of ((x & 0x7f..) + 0x7f..) | x is clear
-// in it (the addition cannot carry across bytes).
+// Newlines in [b, e): sixteen bytes at a time with SSE2 (x86-64's baseline),
+// else eight at a time (for x = word ^ 0x0a0a..., a byte of x is zero exactly
+// when the high bit of ((x & 0x7f..) + 0x7f..) | x is clear in it).
 size_t count_newlines(const char *b, const char *e) {
   size_t n = 0;
   const char *p = b;
+#if defined(__SSE2__)
+  const __m128i nl = _mm_set1_epi8('\n');
+  for (; p + 16 <= e; p += 16) {
+    const __m128i v = _mm_loadu_si128(reinterpret_cast<const __m128i *>(p));
+    n += (size_t)__builtin_popcount((unsigned)_mm_movemask_epi8(_mm_cmpeq_epi8(v, nl)));
+  }
+#else
   constexpr uint64_t kNl = 0x0a0a0a0a0a0a0a0aull, k7f = 0x7f7f7f7f7f7f7f7full;
   for (; p + 8 <= e; p += 8) {
     uint64_t w;
@@ -251,6 +288,7 @@ size_t count_newlines(const char *b, const char *e) {
     const uint64_t t = ((x & k7f) + k7f) | x;
     n += (size_t)__builtin_popcountll(~t & ~k7f);
   }
+#endif
   for (; p < e; ++p) n += *p == '\n';
   return n;
 }
@@ -340,10 +378,16 @@ int read_frame(sqn_dump *d, int64_t capacity, int64_t *natoms_out, int64_t *time
   const char *base = d->base;
   const size_t size = d->size;
   if (off >= size) return 8;
+  // mean length of the first lines (up to 256), for the size of the region
   size_t len1;
   {
-    const void *nl = std::memchr(base + off, '\n', size - off);
-    len1 = nl ? (size_t)(static_cast<const char *>(nl) - (base + off)) + 1 : size - off;
+    size_t q = off;
+    int64_t k = 0;
+    for (; k < std::min<int64_t>(natoms, 256) && q < size; ++k) {
+      const void *nl = std::memchr(base + q, '\n', size - q);
+      q = nl ? (size_t)(static_cast<const char *>(nl) - base) + 1 : size;
+    }
+    len1 = std::max<size_t>(1, (q - off + (size_t)k - 1) / (size_t)std::max<int64_t>(k, 1));
   }
   auto run = [&](auto &&fn) {
     if (nt == 1) {
@@ -355,7 +399,7 @@ int read_frame(sqn_dump *d, int64_t capacity, int64_t *natoms_out, int64_t *time
     fn(0);
     for (auto &t : th) t.join();
   };
-  size_t region = std::min(size - off, (size_t)natoms * len1 * 2 + ((size_t)1 << 16));
+  size_t region = std::min(size - off, (size_t)natoms * len1 / 8 * 9 + ((size_t)1 << 16));
   if (region < (size_t)nt * 4096) nt = 1;  // every part past the first starts 4 KB in
   std::vector<size_t> a((size_t)nt + 1);
   std::vector<int64_t> lines((size_t)nt), first((size_t)nt + 1);

@@ -119,3 +119,36 @@ def test_coordinate_parsing_is_correctly_rounded(tmp_path):
         assert len(got) == 1
         pos = got[0][3]
         assert np.array_equal(pos.view(np.uint64), want.view(np.uint64))
+
+
+def test_threaded_block_split_with_ragged_lines(tmp_path):
+    """Frames large enough for several reader threads (the atom block split by
+    parallel line counts over a byte region estimated from the first lines):
+    short lines first and much longer lines later force the region to be
+    widened; extra columns, tabs and a missing final newline are handled like
+    the one-thread reader, and every frame equals the Python reader's."""
+    rng = np.random.default_rng(4)
+    n = 30000
+    path = str(tmp_path / "big.dump")
+    with open(path, "w") as fh:
+        for f in range(3):
+            fh.write("ITEM: TIMESTEP\n%d\nITEM: NUMBER OF ATOMS\n%d\nITEM: BOX BOUNDS pp pp pp\n"
+                     "0 50\n0 50\n0 50\nITEM: ATOMS id type x y z vx\n" % (f, n))
+            rows = []
+            for i in range(n):
+                x, y, z = rng.random(3) * 50
+                if i < 300:
+                    rows.append("%d 1 %.2f %.2f %.2f 0" % (i + 1, x, y, z))
+                else:
+                    rows.append("%d\t%d  %.15f %.15e %+.12f   %.9f" % (i + 1, 1 + i % 3, x, y, z,
+                                                                     rng.random()))
+            body = "\n".join(rows)
+            fh.write(body + ("\n" if f < 2 else ""))
+    ref = list(read_frames(path))
+    for nt in (1, 4, 7):
+        got = all_frames(path, nt)
+        assert len(got) == len(ref) == 3
+        for (ts, nat, bounds, pos, types, ids), fr in zip(got, ref):
+            assert ts == fr.timestep and nat == fr.natoms == n
+            assert np.array_equal(pos.view(np.uint64), fr.pos.view(np.uint64))
+            np.testing.assert_array_equal(types, fr.type_id)
