@@ -200,6 +200,19 @@ bool parse_int(const char *b, const char *e, int64_t &v) {
   return true;
 }
 
+// parse_int for the plain ids and types of a dump: up to eight digits read at
+// once (8 bytes readable before lim), anything else through parse_int.
+bool parse_int_fast(const char *b, const char *e, const char *lim, int64_t &v) {
+  if (e - b <= 8 && e > b && b + 8 <= lim) {
+    uint64_t val;
+    if (b + digits8(b, val) == e) {
+      v = (int64_t)val;
+      return true;
+    }
+  }
+  return parse_int(b, e, v);
+}
+
 std::string lower(const char *b, const char *e) {
   std::string s(b, e);
   for (char &c : s) c = (char)std::tolower((unsigned char)c);
@@ -253,8 +266,8 @@ int parse_lines(const char *p, const char *end, int64_t first, int64_t count, co
         if (col == c.y) xyz[1] = v;
         if (col == c.z) xyz[2] = v;
       }
-      if (col == c.type && !parse_int(tb, q, t)) return 8;
-      if (ids && col == c.id && !parse_int(tb, q, id)) return 8;
+      if (col == c.type && !parse_int_fast(tb, q, end, t)) return 8;
+      if (ids && col == c.id && !parse_int_fast(tb, q, end, id)) return 8;
     }
     pos[3 * i + 0] = xyz[0];
     pos[3 * i + 1] = xyz[1];
