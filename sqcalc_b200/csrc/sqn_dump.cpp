@@ -245,11 +245,24 @@ const char *token_end(const char *q, const char *e) {
   }
 }
 
+constexpr int kMaxActCols = 32;
+inline int column_action(const Columns &c, int col, bool want_id) {
+  if (col == c.x) return 1;
+  if (col == c.y) return 2;
+  if (col == c.z) return 3;
+  if (col == c.type) return 4;
+  if (want_id && col == c.id) return 5;
+  return 0;
+}
+
 // Parse lines [first, first + count) of a block, the first starting at p: the
 // columns are walked in one pass (a line needs at least ncol tokens; later
 // tokens are ignored) and only id, type and the coordinates are converted.
 int parse_lines(const char *p, const char *end, int64_t first, int64_t count, const Columns &c,
                 double *pos, int32_t *type_id, int64_t *ids) {
+  // what each column is: 1..3 a coordinate, 4 the type, 5 the id, 0 skipped
+  int act_of[kMaxActCols];
+  for (int k = 0; k < kMaxActCols; ++k) act_of[k] = column_action(c, k, ids != nullptr);
   for (int64_t i = first; i < first + count; ++i) {
     double xyz[3] = {0.0, 0.0, 0.0};
     int64_t t = 0, id = i + 1;
@@ -259,15 +272,14 @@ int parse_lines(const char *p, const char *end, int64_t first, int64_t count, co
       if (q >= end || *q == '\n') return 8;
       const char *tb = q;
       q = token_end(q, end);
-      if (col == c.x || col == c.y || col == c.z) {
-        double v;
-        if (!parse_double_fast(tb, q, end, v)) return 8;
-        if (col == c.x) xyz[0] = v;
-        if (col == c.y) xyz[1] = v;
-        if (col == c.z) xyz[2] = v;
+      const int act = col < kMaxActCols ? act_of[col] : column_action(c, col, ids != nullptr);
+      if (act >= 1 && act <= 3) {
+        if (!parse_double_fast(tb, q, end, xyz[act - 1])) return 8;
+      } else if (act == 4) {
+        if (!parse_int_fast(tb, q, end, t)) return 8;
+      } else if (act == 5) {
+        if (!parse_int_fast(tb, q, end, id)) return 8;
       }
-      if (col == c.type && !parse_int_fast(tb, q, end, t)) return 8;
-      if (ids && col == c.id && !parse_int_fast(tb, q, end, id)) return 8;
     }
     pos[3 * i + 0] = xyz[0];
     pos[3 * i + 1] = xyz[1];
