@@ -883,7 +883,9 @@ int setup_plan(sqn_plan *p, const sqn_plan_desc *d) {
     p->bg512 = b;
     p->bg512.nf[1] = 2 * p->hm[1] + 1;
     p->bg512.nf[2] = 2 * p->hm[2] + 1;
-    p->bg512.c1 = p->hm[0] + 1;
+    // rows of the compact spectrum padded to 16 complex values (128-byte
+    // aligned segments for the column passes); h1 = 0 .. hm0 used
+    p->bg512.c1 = ((p->hm[0] + 1) + 15) / 16 * 16;
     p->bg512.vol_cplx = p->bg512.c1 * p->bg512.nf[1] * p->bg512.nf[2];
     p->fft512 = true;
   }
@@ -1052,7 +1054,7 @@ template <typename R> int run_frame(sqn_plan *p, const double *dpos, int slot) {
   if (p->fft512) {
     // x pass into d_G, y pass back into the (consumed) grid, z pass into d_G
     e = launch_fft512<R>((const R *)grid, p->d_G, grid, p->d_G, p->ntr, g.pitch, p->hm[0] + 1,
-                         p->hm[1], p->hm[2], p->d_tw512, p->nsm, s);
+                         (int)p->bg512.c1, p->hm[1], p->hm[2], p->d_tw512, p->nsm, s);
     if (e != cudaSuccess) return SQN_ERR_CUDA;
     p->launches += 3;
   } else if (exec_forward(p, s, grid, p->d_G) != CUFFT_SUCCESS) {
@@ -1693,8 +1695,8 @@ template <typename R> int batch_frame_multi(sqn_batch *b) {
     if (cudaStreamWaitEvent(p->stream, b->fork, 0) != cudaSuccess) return SQN_ERR_CUDA;
     if (p->fft512) {
       if (launch_fft512<R>((const R *)p->d_grid, p->d_G, p->d_grid, p->d_G, p->ntr, p->fg.pitch,
-                           p->hm[0] + 1, p->hm[1], p->hm[2], p->d_tw512, p->nsm,
-                           p->stream) != cudaSuccess)
+                           p->hm[0] + 1, (int)p->bg512.c1, p->hm[1], p->hm[2], p->d_tw512,
+                           p->nsm, p->stream) != cudaSuccess)
         return SQN_ERR_CUDA;
       own += 3;
     } else if (exec_forward(p, p->stream, p->d_grid, p->d_G) != CUFFT_SUCCESS) {

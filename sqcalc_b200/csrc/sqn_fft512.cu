@@ -21,7 +21,7 @@
 //                  (A1 -> A2[t][z][h2][h1]) and the z pass
 //                  (A2 -> G[t][h3][h2][h1]) are the same kernel with other strides.
 // The result is the compact half spectrum that k_bin reads with nf1 = 2 hm1 + 1,
-// nf2 = 2 hm2 + 1 and a row length of H1.
+// nf2 = 2 hm2 + 1 and a row pitch of P1 >= H1.
 #include <cmath>
 #include <cstdint>
 #include <vector>
@@ -208,7 +208,7 @@ template <typename R> __host__ __device__ constexpr int x_warps() {
 template <typename R>
 __global__ void __launch_bounds__(32 * x_warps<R>())
     k_fft512_x(const R *__restrict__ grid, typename Cplx<R>::T *__restrict__ A1, int64_t nrows,
-               int64_t pitch, int H1, const typename Cplx<R>::T *__restrict__ tw) {
+               int64_t pitch, int H1, int P1, const typename Cplx<R>::T *__restrict__ tw) {
   using C = typename Cplx<R>::T;
   constexpr int X_WARPS = x_warps<R>();
   __shared__ C s_tw[TW_LEN];
@@ -235,7 +235,7 @@ __global__ void __launch_bounds__(32 * x_warps<R>())
     for (int a = 0; a < 16; ++a) line[k2 + 16 * a + 256 * b] = v[a];
     __syncwarp();
     // X1[h] = (Z[h] + conj Z[512-h]) / 2, X2[h] = (Z[h] - conj Z[512-h]) / (2i)
-    C *o0 = A1 + (2 * pr) * H1;
+    C *o0 = A1 + (2 * pr) * P1;
     for (int h = lane; h < H1; h += 32) {
       const C zh = line[h];
       const C zm = line[(512 - h) & 511];
@@ -245,7 +245,7 @@ __global__ void __launch_bounds__(32 * x_warps<R>())
       x2.x = R(0.5) * (zh.y + zm.y);
       x2.y = R(0.5) * (zm.x - zh.x);
       o0[h] = x1;
-      if (two) o0[H1 + h] = x2;
+      if (two) o0[P1 + h] = x2;
     }
     __syncwarp();
   }
@@ -361,29 +361,34 @@ void fft512_twiddles(std::vector<double> &tw) {
   }
 }
 
-// grid [ntr][nf2][nf1][pitch] real -> A1 [ntr][nf2][nf1][H1] -> A2 [ntr][nf2][M2][H1]
-// -> G [ntr][M3][M2][H1] (A2 may share the grid's storage; A1 and G share one buffer).
+// grid [ntr][nf2][nf1][pitch] real -> A1 [ntr][nf2][nf1][P1] -> A2 [ntr][nf2][M2][P1]
+// -> G [ntr][M3][M2][P1] with h1 = 0 .. H1 - 1 of each P1-long row used (A2 may share
+// the grid's storage; A1 and G share one buffer).  A row pitch P1 of 16 complex
+// values makes every 16-column segment the column passes move start on a 128-byte
+// boundary.
 template <typename R>
 cudaError_t launch_fft512(const R *grid, void *A1, void *A2, void *G, int ntr, int64_t pitch,
-                          int H1, int hm1, int hm2, const void *tw, int nsm, cudaStream_t s) {
+                          int H1, int P1, int hm1, int hm2, const void *tw, int nsm,
+                          cudaStream_t s) {
   using C = typename Cplx<R>::T;
   const int n = 512;
   const int M2 = 2 * hm1 + 1, M3 = 2 * hm2 + 1;
   const int64_t nrows = (int64_t)ntr * n * n;
-  if ((int64_t)ntr * n * ((H1 + COLS - 1) / COLS) >= ((int64_t)1 << 31)) return cudaErrorInvalidValue;
-  k_fft512_x<R><<<nsm * 8, 32 * x_warps<R>(), 0, s>>>(grid, (C *)A1, nrows, pitch, H1,
+  if (P1 < H1 || (int64_t)ntr * n * ((H1 + COLS - 1) / COLS) >= ((int64_t)1 << 31))
+    return cudaErrorInvalidValue;
+  k_fft512_x<R><<<nsm * 8, 32 * x_warps<R>(), 0, s>>>(grid, (C *)A1, nrows, pitch, H1, P1,
                                                       (const C *)tw);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   const size_t sm = cols_smem<R>();
   const int cta = sizeof(R) == 4 ? 2 : 1;
   ColPass y;
-  y.in_t = (int64_t)n * n * H1;
-  y.in_p = (int64_t)n * H1;
-  y.in_r = H1;
-  y.out_t = (int64_t)n * M2 * H1;
-  y.out_p = (int64_t)M2 * H1;
-  y.out_r = H1;
+  y.in_t = (int64_t)n * n * P1;
+  y.in_p = (int64_t)n * P1;
+  y.in_r = P1;
+  y.out_t = (int64_t)n * M2 * P1;
+  y.out_p = (int64_t)M2 * P1;
+  y.out_r = P1;
   y.planes_per_t = n;
   y.nplanes = (int64_t)ntr * n;
   y.ncols = H1;
@@ -396,12 +401,12 @@ cudaError_t launch_fft512(const R *grid, void *A1, void *A2, void *G, int ntr, i
   e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   ColPass z;
-  z.in_t = (int64_t)n * M2 * H1;
-  z.in_p = H1;
-  z.in_r = (int64_t)M2 * H1;
-  z.out_t = (int64_t)M3 * M2 * H1;
-  z.out_p = H1;
-  z.out_r = (int64_t)M2 * H1;
+  z.in_t = (int64_t)n * M2 * P1;
+  z.in_p = P1;
+  z.in_r = (int64_t)M2 * P1;
+  z.out_t = (int64_t)M3 * M2 * P1;
+  z.out_p = P1;
+  z.out_r = (int64_t)M2 * P1;
   z.planes_per_t = M2;
   z.nplanes = (int64_t)ntr * M2;
   z.ncols = H1;
@@ -410,8 +415,8 @@ cudaError_t launch_fft512(const R *grid, void *A1, void *A2, void *G, int ntr, i
   return cudaGetLastError();
 }
 template cudaError_t launch_fft512<float>(const float *, void *, void *, void *, int, int64_t,
-                                          int, int, int, const void *, int, cudaStream_t);
+                                          int, int, int, int, const void *, int, cudaStream_t);
 template cudaError_t launch_fft512<double>(const double *, void *, void *, void *, int, int64_t,
-                                           int, int, int, const void *, int, cudaStream_t);
+                                           int, int, int, int, const void *, int, cudaStream_t);
 
 }  // namespace sqn
