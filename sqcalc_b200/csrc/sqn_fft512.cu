@@ -279,24 +279,40 @@ __global__ void __launch_bounds__(32 * COLS, sizeof(R) == 4 ? 2 : 1)
   C *tile = s_tw + TW_LEN;  // [512][COL_LD]
   for (int i = threadIdx.x; i < TW_LEN; i += blockDim.x) s_tw[i] = tw[i];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int nblk = (cp.ncols + COLS - 1) / COLS;
   const int M = 2 * cp.hm + 1;
-  // 32-bit step indices (the host keeps nplanes * nblk below 2^31): the
-  // divisions below are then a few instructions, not a 64-bit division routine
-  const unsigned nsteps = (unsigned)cp.nplanes * (unsigned)nblk;
+  // Steps: the full 16-column blocks of every plane, then the partial last
+  // blocks (rem columns) of G = 16 / rem planes at a time, so that no step
+  // leaves most of its warps idle.  32-bit step indices (the host keeps the
+  // step count below 2^31): the divisions are a few instructions.
+  const int nfull = cp.ncols / COLS, rem = cp.ncols - nfull * COLS;
+  const int G = rem > 0 ? COLS / rem : 1;
+  const unsigned nfs = (unsigned)cp.nplanes * (unsigned)nfull;
+  const unsigned nsteps =
+      nfs + (rem > 0 ? (unsigned)((cp.nplanes + G - 1) / G) : 0u);
+  // thread -> (tile column c, rows r0 + 32 k)
+  const int c = threadIdx.x & (COLS - 1), r0 = threadIdx.x >> 4;
   for (unsigned st = blockIdx.x; st < nsteps; st += gridDim.x) {
-    const unsigned plane = st / (unsigned)nblk;
-    const int c0 = (int)(st - plane * (unsigned)nblk) * COLS;
-    const int nc = min(COLS, cp.ncols - c0);
+    // the plane and column of tile column cc of this step (false: no column)
+    auto where = [&](int cc, unsigned &plane, int &col) {
+      if (st < nfs) {
+        plane = st / (unsigned)nfull;
+        col = (int)(st - plane * (unsigned)nfull) * COLS + cc;
+        return true;
+      }
+      const int sub = cc / rem;
+      plane = (st - nfs) * (unsigned)G + (unsigned)sub;
+      col = nfull * COLS + (cc - sub * rem);
+      return sub < G && plane < (unsigned)cp.nplanes;
+    };
+    unsigned plane;
+    int col;
+    const bool mine = where(c, plane, col);
     const unsigned t = plane / (unsigned)cp.planes_per_t, p = plane - t * cp.planes_per_t;
-    const C *ib = in + t * cp.in_t + p * cp.in_p + c0;
-    C *ob = out + t * cp.out_t + p * cp.out_p + c0;
-    // a thread's loads (column c, rows r0 + 32 k) go out eight at a time
-    const int c = threadIdx.x & (COLS - 1), r0 = threadIdx.x >> 4;
-    const C *src = ib + (int64_t)r0 * cp.in_r + c;
-    const int64_t step = 32 * cp.in_r;
     __syncthreads();  // the previous step's stores have read the tile
-    if (c < nc) {
+    if (mine) {
+      // a thread's loads (rows r0 + 32 k) go out eight at a time
+      const C *src = in + t * cp.in_t + p * cp.in_p + col + (int64_t)r0 * cp.in_r;
+      const int64_t step = 32 * cp.in_r;
 #pragma unroll
       for (int k0 = 0; k0 < 512 / 32; k0 += 8) {
         C ld[8];
@@ -310,24 +326,26 @@ __global__ void __launch_bounds__(32 * COLS, sizeof(R) == 4 ? 2 : 1)
       }
     }
     __syncthreads();
-    if (warp < nc) {
-      C *col = tile + warp;
+    unsigned wplane;
+    int wcol;
+    if (where(warp, wplane, wcol)) {
+      C *colp = tile + warp;
       C v[16];
 #pragma unroll
-      for (int j = 0; j < 16; ++j) v[j] = col[(lane + 32 * j) * COL_LD];
+      for (int j = 0; j < 16; ++j) v[j] = colp[(lane + 32 * j) * COL_LD];
       __syncwarp();
       // the column itself is the scratch line (slot i at row i)
-      warp_fft512(v, col, COL_LD, s_tw, lane);
+      warp_fft512(v, colp, COL_LD, s_tw, lane);
       const int k2 = lane & 15, b = lane >> 4;
 #pragma unroll
-      for (int a = 0; a < 16; ++a) col[(k2 + 16 * a + 256 * b) * COL_LD] = v[a];
+      for (int a = 0; a < 16; ++a) colp[(k2 + 16 * a + 256 * b) * COL_LD] = v[a];
     }
     __syncthreads();
     // output rows hw = 0 .. hm come from tile rows hw, rows hm + 1 .. M - 1
     // (h = hw - M < 0) from tile rows 512 + hw - M
-    if (c < nc) {
+    if (mine) {
       const int64_t ostep = 32 * cp.out_r;
-      C *dst = ob + (int64_t)r0 * cp.out_r + c;
+      C *dst = out + t * cp.out_t + p * cp.out_p + col + (int64_t)r0 * cp.out_r;
       const C *tp = tile + r0 * COL_LD + c;
       int hw = r0;
       for (; hw <= cp.hm; hw += 32, tp += 32 * COL_LD, dst += ostep) *dst = *tp;
@@ -374,7 +392,7 @@ cudaError_t launch_fft512(const R *grid, void *A1, void *A2, void *G, int ntr, i
   const int n = 512;
   const int M2 = 2 * hm1 + 1, M3 = 2 * hm2 + 1;
   const int64_t nrows = (int64_t)ntr * n * n;
-  if (P1 < H1 || (int64_t)ntr * n * ((H1 + COLS - 1) / COLS) >= ((int64_t)1 << 31))
+  if (P1 < H1 || (int64_t)ntr * n * (H1 / COLS + 1) >= ((int64_t)1 << 31))
     return cudaErrorInvalidValue;
   k_fft512_x<R><<<nsm * 8, 32 * x_warps<R>(), 0, s>>>(grid, (C *)A1, nrows, pitch, H1, P1,
                                                       (const C *)tw);
