@@ -271,6 +271,7 @@ struct sqn_plan_s {
   // pruned 512-point passes (every axis 512): compact half spectrum in d_G
   bool fft512 = false;
   void *d_tw512 = nullptr;
+  int *d_h1end = nullptr;  // per h2 (FFT order): one past the largest kept h1 of any h3
   BinGeom bg512{};
   // density amplitudes (sqn_density_modes): request buffers, grown on demand
   int *d_hkl = nullptr;
@@ -887,6 +888,20 @@ int setup_plan(sqn_plan *p, const sqn_plan_desc *d) {
     // aligned segments for the column passes); h1 = 0 .. hm0 used
     p->bg512.c1 = ((p->hm[0] + 1) + 15) / 16 * 16;
     p->bg512.vol_cplx = p->bg512.c1 * p->bg512.nf[1] * p->bg512.nf[2];
+    // columns (h1, h2) the binning reads: h1 <= the largest kept h1 over the rows
+    // with that h2 (the rows' h1 ranges are conservative supersets)
+    {
+      const int M2 = 2 * p->hm[1] + 1;
+      std::vector<int> h1end((size_t)M2, 0);
+      for (const int4 &r : build_rows(p->recip, p->hm, d->qmax)) {
+        const int h2w = r.x >= 0 ? r.x : M2 + r.x;
+        h1end[(size_t)h2w] = std::max(h1end[(size_t)h2w], r.w + 1);
+      }
+      if ((st = dalloc(p, &p->d_h1end, h1end.size()))) return st;
+      if (cudaMemcpy(p->d_h1end, h1end.data(), h1end.size() * sizeof(int),
+                     cudaMemcpyHostToDevice) != cudaSuccess)
+        return SQN_ERR_CUDA;
+    }
     p->fft512 = true;
   }
 
@@ -1054,7 +1069,8 @@ template <typename R> int run_frame(sqn_plan *p, const double *dpos, int slot) {
   if (p->fft512) {
     // x pass into d_G, y pass back into the (consumed) grid, z pass into d_G
     e = launch_fft512<R>((const R *)grid, p->d_G, grid, p->d_G, p->ntr, g.pitch, p->hm[0] + 1,
-                         (int)p->bg512.c1, p->hm[1], p->hm[2], p->d_tw512, p->nsm, s);
+                         (int)p->bg512.c1, p->hm[1], p->hm[2], p->d_tw512, p->d_h1end,
+                         p->nsm, s);
     if (e != cudaSuccess) return SQN_ERR_CUDA;
     p->launches += 3;
   } else if (exec_forward(p, s, grid, p->d_G) != CUFFT_SUCCESS) {
@@ -1696,7 +1712,7 @@ template <typename R> int batch_frame_multi(sqn_batch *b) {
     if (p->fft512) {
       if (launch_fft512<R>((const R *)p->d_grid, p->d_G, p->d_grid, p->d_G, p->ntr, p->fg.pitch,
                            p->hm[0] + 1, (int)p->bg512.c1, p->hm[1], p->hm[2], p->d_tw512,
-                           p->nsm, p->stream) != cudaSuccess)
+                           p->d_h1end, p->nsm, p->stream) != cudaSuccess)
         return SQN_ERR_CUDA;
       own += 3;
     } else if (exec_forward(p, p->stream, p->d_grid, p->d_G) != CUFFT_SUCCESS) {

@@ -267,6 +267,9 @@ struct ColPass {
   int64_t nplanes;
   int ncols;  // columns per plane (H1)
   int hm;     // kept band -hm .. hm
+  // optional, per plane p of a transform: columns >= col_end[p] are neither
+  // transformed nor written (nothing reads them)
+  const int *col_end;
 };
 
 template <typename R>
@@ -304,9 +307,13 @@ __global__ void __launch_bounds__(32 * COLS, sizeof(R) == 4 ? 2 : 1)
       col = nfull * COLS + (cc - sub * rem);
       return sub < G && plane < (unsigned)cp.nplanes;
     };
+    auto used = [&](int cc, unsigned &plane, int &col) {
+      if (!where(cc, plane, col)) return false;
+      return !cp.col_end || col < __ldg(cp.col_end + plane % (unsigned)cp.planes_per_t);
+    };
     unsigned plane;
     int col;
-    const bool mine = where(c, plane, col);
+    const bool mine = used(c, plane, col);
     const unsigned t = plane / (unsigned)cp.planes_per_t, p = plane - t * cp.planes_per_t;
     __syncthreads();  // the previous step's stores have read the tile
     if (mine) {
@@ -328,7 +335,7 @@ __global__ void __launch_bounds__(32 * COLS, sizeof(R) == 4 ? 2 : 1)
     __syncthreads();
     unsigned wplane;
     int wcol;
-    if (where(warp, wplane, wcol)) {
+    if (used(warp, wplane, wcol)) {
       C *colp = tile + warp;
       C v[16];
 #pragma unroll
@@ -381,13 +388,15 @@ void fft512_twiddles(std::vector<double> &tw) {
 
 // grid [ntr][nf2][nf1][pitch] real -> A1 [ntr][nf2][nf1][P1] -> A2 [ntr][nf2][M2][P1]
 // -> G [ntr][M3][M2][P1] with h1 = 0 .. H1 - 1 of each P1-long row used (A2 may share
-// the grid's storage; A1 and G share one buffer).  A row pitch P1 of 16 complex
+// the grid's storage; A1 and G share one buffer).  h1_end (optional, [M2] in FFT
+// order of h2): the z pass skips the columns (h1, h2) with h1 >= h1_end[h2], which
+// hold no kept mode for any h3; G's entries there are left unwritten.  A row pitch P1 of 16 complex
 // values makes every 16-column segment the column passes move start on a 128-byte
 // boundary.
 template <typename R>
 cudaError_t launch_fft512(const R *grid, void *A1, void *A2, void *G, int ntr, int64_t pitch,
-                          int H1, int P1, int hm1, int hm2, const void *tw, int nsm,
-                          cudaStream_t s) {
+                          int H1, int P1, int hm1, int hm2, const void *tw,
+                          const int *h1_end, int nsm, cudaStream_t s) {
   using C = typename Cplx<R>::T;
   const int n = 512;
   const int M2 = 2 * hm1 + 1, M3 = 2 * hm2 + 1;
@@ -411,6 +420,7 @@ cudaError_t launch_fft512(const R *grid, void *A1, void *A2, void *G, int ntr, i
   y.nplanes = (int64_t)ntr * n;
   y.ncols = H1;
   y.hm = hm1;
+  y.col_end = nullptr;
   auto cols = [&](const void *src, void *dst, const ColPass &cp) {
     k_fft512_cols<R><<<nsm * cta, 32 * COLS, sm, s>>>((const C *)src, (C *)dst, cp,
                                                       (const C *)tw);
@@ -429,12 +439,15 @@ cudaError_t launch_fft512(const R *grid, void *A1, void *A2, void *G, int ntr, i
   z.nplanes = (int64_t)ntr * M2;
   z.ncols = H1;
   z.hm = hm2;
+  z.col_end = h1_end;  // plane p = h2 in FFT order
   cols(A2, G, z);
   return cudaGetLastError();
 }
 template cudaError_t launch_fft512<float>(const float *, void *, void *, void *, int, int64_t,
-                                          int, int, int, int, const void *, int, cudaStream_t);
+                                          int, int, int, int, const void *, const int *, int,
+                                          cudaStream_t);
 template cudaError_t launch_fft512<double>(const double *, void *, void *, void *, int, int64_t,
-                                           int, int, int, int, const void *, int, cudaStream_t);
+                                           int, int, int, int, const void *, const int *, int,
+                                           cudaStream_t);
 
 }  // namespace sqn

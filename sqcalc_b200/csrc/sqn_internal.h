@@ -154,13 +154,13 @@ std::vector<double> kernel_ft(int64_t nf, int w, double beta, int kmax);
 
 // Pruned 512-point FFT passes (sqn_fft512.cu): grid -> A1 (x) -> A2 (y) -> G
 // (z), G the compact half spectrum [ntr][2 hm2 + 1][2 hm1 + 1][P1] (rows of P1 >= H1
-// complex values, h1 < H1 used).
+// complex values, h1 < H1 used; with h1_end, only h1 < h1_end[h2] written).
 template <typename R> cudaError_t fft512_set_attributes();
 void fft512_twiddles(std::vector<double> &tw);  // the passes' table, interleaved re, im
 template <typename R>
 cudaError_t launch_fft512(const R *grid, void *A1, void *A2, void *G, int ntr, int64_t pitch,
-                          int H1, int P1, int hm1, int hm2, const void *tw, int nsm,
-                          cudaStream_t s);
+                          int H1, int P1, int hm1, int hm2, const void *tw, const int *h1_end,
+                          int nsm, cudaStream_t s);
 
 // Density amplitudes of requested lattice points from the half spectra.
 template <typename R>
