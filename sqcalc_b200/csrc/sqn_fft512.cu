@@ -270,6 +270,9 @@ struct ColPass {
   // optional, per plane p of a transform: columns >= col_end[p] are neither
   // transformed nor written (nothing reads them)
   const int *col_end;
+  // optional, per output row hw: columns >= row_col_end[hw] of that row are not
+  // written (nothing reads them)
+  const int *row_col_end;
 };
 
 template <typename R>
@@ -355,9 +358,17 @@ __global__ void __launch_bounds__(32 * COLS, sizeof(R) == 4 ? 2 : 1)
       C *dst = out + t * cp.out_t + p * cp.out_p + col + (int64_t)r0 * cp.out_r;
       const C *tp = tile + r0 * COL_LD + c;
       int hw = r0;
-      for (; hw <= cp.hm; hw += 32, tp += 32 * COL_LD, dst += ostep) *dst = *tp;
-      tp += (512 - M) * COL_LD;
-      for (; hw < M; hw += 32, tp += 32 * COL_LD, dst += ostep) *dst = *tp;
+      if (cp.row_col_end) {
+        for (; hw <= cp.hm; hw += 32, tp += 32 * COL_LD, dst += ostep)
+          if (col < __ldg(cp.row_col_end + hw)) *dst = *tp;
+        tp += (512 - M) * COL_LD;
+        for (; hw < M; hw += 32, tp += 32 * COL_LD, dst += ostep)
+          if (col < __ldg(cp.row_col_end + hw)) *dst = *tp;
+      } else {
+        for (; hw <= cp.hm; hw += 32, tp += 32 * COL_LD, dst += ostep) *dst = *tp;
+        tp += (512 - M) * COL_LD;
+        for (; hw < M; hw += 32, tp += 32 * COL_LD, dst += ostep) *dst = *tp;
+      }
     }
   }
 }
@@ -390,7 +401,8 @@ void fft512_twiddles(std::vector<double> &tw) {
 // -> G [ntr][M3][M2][P1] with h1 = 0 .. H1 - 1 of each P1-long row used (A2 may share
 // the grid's storage; A1 and G share one buffer).  h1_end (optional, [M2] in FFT
 // order of h2): the z pass skips the columns (h1, h2) with h1 >= h1_end[h2], which
-// hold no kept mode for any h3; G's entries there are left unwritten.  A row pitch P1 of 16 complex
+// hold no kept mode for any h3, and the FP64 y pass does not write them; A2's and
+// G's entries there are left unwritten.  A row pitch P1 of 16 complex
 // values makes every 16-column segment the column passes move start on a 128-byte
 // boundary.
 template <typename R>
@@ -421,6 +433,9 @@ cudaError_t launch_fft512(const R *grid, void *A1, void *A2, void *G, int ntr, i
   y.ncols = H1;
   y.hm = hm1;
   y.col_end = nullptr;
+  // output row hw = h2 in FFT order; FP64 only: the FP32 pass is issue-bound
+  // enough that the per-row test cost more than the writes it saved (measured)
+  y.row_col_end = sizeof(R) == 8 ? h1_end : nullptr;
   auto cols = [&](const void *src, void *dst, const ColPass &cp) {
     k_fft512_cols<R><<<nsm * cta, 32 * COLS, sm, s>>>((const C *)src, (C *)dst, cp,
                                                       (const C *)tw);
@@ -440,6 +455,7 @@ cudaError_t launch_fft512(const R *grid, void *A1, void *A2, void *G, int ntr, i
   z.ncols = H1;
   z.hm = hm2;
   z.col_end = h1_end;  // plane p = h2 in FFT order
+  z.row_col_end = nullptr;
   cols(A2, G, z);
   return cudaGetLastError();
 }
