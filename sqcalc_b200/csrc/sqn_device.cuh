@@ -243,7 +243,9 @@ __device__ __forceinline__ void bin_mode(const BinGeom &b, int ntr, bool inrange
                                          const double *__restrict__ amp,
                                          const double *__restrict__ xcoef, double *hist,
                                          double *__restrict__ gnum, int64_t gidx, int lane,
-                                         double *xhist = nullptr) {
+                                         double *xhist = nullptr, int hq = -1, int hs = 1) {
+  // sum p of shell s at hist[p hq + s hs] (hq < 0: hq = nq, the accumulators' layout)
+  if (hq < 0) hq = b.nq;
   double ql = 0.0;
   int s = 0;
   const bool keep = inrange && classify_mode(b, crow, h1, h2, h3, s, ql);
@@ -274,7 +276,7 @@ __device__ __forceinline__ void bin_mode(const BinGeom &b, int ntr, bool inrange
   if (b.want_grid && keep) gnum[gidx] += I;
   const int s0 = __shfl_sync(FULL, s, __ffs(act) - 1);
   const bool uni = __all_sync(FULL, !keep || s == s0);
-  hist_add(hist, s, mult * I, keep, uni, s0, lane);
+  hist_add(hist, s * hs, mult * I, keep, uni, s0 * hs, lane);
   if (b.partials) {
     int p = 1;
 #pragma unroll
@@ -282,8 +284,8 @@ __device__ __forceinline__ void bin_mode(const BinGeom &b, int ntr, bool inrange
 #pragma unroll
       for (int c = a; c < TM; ++c) {
         if (c < ntr) {
-          hist_add(hist + p * b.nq, s, mult * (re[a] * re[c] + im[a] * im[c]), keep, uni, s0,
-                   lane);
+          hist_add(hist + p * hq, s * hs, mult * (re[a] * re[c] + im[a] * im[c]), keep, uni,
+                   s0 * hs, lane);
           ++p;
         }
       }

@@ -484,7 +484,7 @@ __device__ __forceinline__ void bin_rows(const int4 *__restrict__ rows, int nrow
                                          const double *__restrict__ amp,
                                          const double *__restrict__ xcoef, double *hist,
                                          double *xhist, double *__restrict__ gnum, int r0,
-                                         int rstep, int lane) {
+                                         int rstep, int lane, int hq = -1, int hs = 1) {
   const int ntr = NT > 0 ? NT : b.ntr;
   constexpr int TM = NT > 0 ? NT : MAX_FAST_T;
   for (int r = r0; r < nrows; r += rstep) {
@@ -510,7 +510,7 @@ __device__ __forceinline__ void bin_rows(const int4 *__restrict__ rows, int nrow
         if (t < ntr && inrow) v[t] = G[(int64_t)t * b.vol_cplx + rowbase + h1];
       const R dec = inrow ? inv1[h1] * dyz : R(0);
       bin_mode<R, TM, XR, XD>(b, ntr, inrow, h1, h2, h3, crow, v, dec, amp, xcoef, hist, gnum,
-                              gbase + h1, lane, xhist);
+                              gbase + h1, lane, xhist, hq, hs);
     }
   }
 }
@@ -531,13 +531,19 @@ __global__ void __launch_bounds__(256, 2)
     for (int i = tid; i < nhist; i += blockDim.x) s_hist[i] = 0.0;
     __syncthreads();
   }
+  // the shared sums are shell-major (the nquant sums of a shell side by side,
+  // fewer bank collisions between the lanes' atomics); the flush restores the
+  // accumulators' quantity-major layout
+  const int nsh = b.nquant * b.nq;
   bin_rows<R, NT, XR, XD>(rows, nrows, G, b, inv1, inv2, inv3, amp, xcoef, hist, xhist, gnum,
-                          blockIdx.x * nwarps + warp, gridDim.x * nwarps, lane);
+                          blockIdx.x * nwarps + warp, gridDim.x * nwarps, lane,
+                          SMEM ? 1 : b.nq, SMEM ? b.nquant : 1);
   if (SMEM) {
     __syncthreads();
     for (int i = tid; i < nhist; i += blockDim.x) {
       const double v = s_hist[i];
-      if (v != 0.0) atomicAdd(&acc[i], v);
+      const int g = i < nsh ? (i % b.nquant) * b.nq + i / b.nquant : i;
+      if (v != 0.0) atomicAdd(&acc[g], v);
     }
   }
 }
@@ -743,11 +749,12 @@ __global__ void __launch_bounds__(256, 2)
   bin_rows<R, NT, XR, false>(S.rows, S.nrows, (const typename Cplx<R>::T *)S.G, s_b,
                              (const R *)S.inv[0], (const R *)S.inv[1], (const R *)S.inv[2],
                              S.amp, S.xcoef, s_hist, nullptr, S.gnum, s_lb * nwarps + warp,
-                             s_nb * nwarps, lane);
+                             s_nb * nwarps, lane, 1, s_b.nquant);
   __syncthreads();
+  // shell-major shared sums back to the quantity-major accumulators
   for (int i = tid; i < nhist; i += blockDim.x) {
     const double v = s_hist[i];
-    if (v != 0.0) atomicAdd(&S.acc[i], v);
+    if (v != 0.0) atomicAdd(&S.acc[(i % s_b.nquant) * s_b.nq + i / s_b.nquant], v);
   }
 }
 
