@@ -272,6 +272,7 @@ struct sqn_plan_s {
   bool fft512 = false;
   void *d_tw512 = nullptr;
   int *d_h1end = nullptr;  // per h2 (FFT order): one past the largest kept h1 of any h3
+  short2 *d_h2band = nullptr;  // per 16-column block of h1: the h2 band it needs
   BinGeom bg512{};
   // density amplitudes (sqn_density_modes): request buffers, grown on demand
   int *d_hkl = nullptr;
@@ -901,6 +902,22 @@ int setup_plan(sqn_plan *p, const sqn_plan_desc *d) {
       if (cudaMemcpy(p->d_h1end, h1end.data(), h1end.size() * sizeof(int),
                      cudaMemcpyHostToDevice) != cudaSuccess)
         return SQN_ERR_CUDA;
+      // per 16-column block of h1 (from h1 = 16 j): the h2 some column of it needs
+      // (h1end[h2] > 16 j), as one band [lo, hi] (empty: lo > hi)
+      const int nblk = (p->hm[0] + 1 + 15) / 16;
+      std::vector<short2> band((size_t)nblk, make_short2(1, 0));
+      for (int j = 0; j < nblk; ++j)
+        for (int hw = 0; hw < M2; ++hw)
+          if (h1end[(size_t)hw] > 16 * j) {
+            const short h2 = (short)(hw <= p->hm[1] ? hw : hw - M2);
+            short2 &e = band[(size_t)j];
+            if (e.x > e.y) e = make_short2(h2, h2);
+            else e = make_short2(std::min(e.x, h2), std::max(e.y, h2));
+          }
+      if ((st = dalloc(p, &p->d_h2band, band.size()))) return st;
+      if (cudaMemcpy(p->d_h2band, band.data(), band.size() * sizeof(short2),
+                     cudaMemcpyHostToDevice) != cudaSuccess)
+        return SQN_ERR_CUDA;
     }
     p->fft512 = true;
   }
@@ -1070,7 +1087,7 @@ template <typename R> int run_frame(sqn_plan *p, const double *dpos, int slot) {
     // x pass into d_G, y pass back into the (consumed) grid, z pass into d_G
     e = launch_fft512<R>((const R *)grid, p->d_G, grid, p->d_G, p->ntr, g.pitch, p->hm[0] + 1,
                          (int)p->bg512.c1, p->hm[1], p->hm[2], p->d_tw512, p->d_h1end,
-                         p->nsm, s);
+                         p->d_h2band, p->nsm, s);
     if (e != cudaSuccess) return SQN_ERR_CUDA;
     p->launches += 3;
   } else if (exec_forward(p, s, grid, p->d_G) != CUFFT_SUCCESS) {
@@ -1712,7 +1729,7 @@ template <typename R> int batch_frame_multi(sqn_batch *b) {
     if (p->fft512) {
       if (launch_fft512<R>((const R *)p->d_grid, p->d_G, p->d_grid, p->d_G, p->ntr, p->fg.pitch,
                            p->hm[0] + 1, (int)p->bg512.c1, p->hm[1], p->hm[2], p->d_tw512,
-                           p->d_h1end, p->nsm, p->stream) != cudaSuccess)
+                           p->d_h1end, p->d_h2band, p->nsm, p->stream) != cudaSuccess)
         return SQN_ERR_CUDA;
       own += 3;
     } else if (exec_forward(p, p->stream, p->d_grid, p->d_G) != CUFFT_SUCCESS) {

@@ -270,9 +270,10 @@ struct ColPass {
   // optional, per plane p of a transform: columns >= col_end[p] are neither
   // transformed nor written (nothing reads them)
   const int *col_end;
-  // optional, per output row hw: columns >= row_col_end[hw] of that row are not
-  // written (nothing reads them)
-  const int *row_col_end;
+  // optional, per 16-column block of a plane: the band of output rows h in
+  // [lo, hi] that is read later (h < 0 at row 2 hm + 1 + h); other rows of the
+  // block are not written
+  const short2 *blk_rows;
 };
 
 template <typename R>
@@ -358,12 +359,18 @@ __global__ void __launch_bounds__(32 * COLS, sizeof(R) == 4 ? 2 : 1)
       C *dst = out + t * cp.out_t + p * cp.out_p + col + (int64_t)r0 * cp.out_r;
       const C *tp = tile + r0 * COL_LD + c;
       int hw = r0;
-      if (cp.row_col_end) {
-        for (; hw <= cp.hm; hw += 32, tp += 32 * COL_LD, dst += ostep)
-          if (col < __ldg(cp.row_col_end + hw)) *dst = *tp;
-        tp += (512 - M) * COL_LD;
-        for (; hw < M; hw += 32, tp += 32 * COL_LD, dst += ostep)
-          if (col < __ldg(cp.row_col_end + hw)) *dst = *tp;
+      if (cp.blk_rows) {
+        // rows h in [lo, hi] only (positive h at row h, negative at row M + h of
+        // the output and 512 + h of the tile), as per-thread loop bounds
+        const short2 rr = __ldg(cp.blk_rows + col / COLS);
+        const int lo = rr.x, hi = rr.y;
+        C *obase = out + t * cp.out_t + p * cp.out_p + col;
+        const int pl = max(lo, 0), ph = min(hi, cp.hm);
+        for (int h = pl + (((r0 - pl) % 32) + 32) % 32; h <= ph; h += 32)
+          obase[(int64_t)h * cp.out_r] = tile[h * COL_LD + c];
+        const int nl = max(lo, -cp.hm), nh = min(hi, -1);
+        for (int h = nl + (((r0 - (M + nl)) % 32) + 32) % 32; h <= nh; h += 32)
+          obase[(int64_t)(M + h) * cp.out_r] = tile[(512 + h) * COL_LD + c];
       } else {
         for (; hw <= cp.hm; hw += 32, tp += 32 * COL_LD, dst += ostep) *dst = *tp;
         tp += (512 - M) * COL_LD;
@@ -401,14 +408,15 @@ void fft512_twiddles(std::vector<double> &tw) {
 // -> G [ntr][M3][M2][P1] with h1 = 0 .. H1 - 1 of each P1-long row used (A2 may share
 // the grid's storage; A1 and G share one buffer).  h1_end (optional, [M2] in FFT
 // order of h2): the z pass skips the columns (h1, h2) with h1 >= h1_end[h2], which
-// hold no kept mode for any h3, and the FP64 y pass does not write them; A2's and
-// G's entries there are left unwritten.  A row pitch P1 of 16 complex
+// hold no kept mode for any h3; h2_band (optional, short2 per 16-column block of
+// h1): the y pass writes only the h2 rows [lo, hi] of a block that some of its
+// columns need.  A2's and G's entries elsewhere are left unwritten.  A row pitch P1 of 16 complex
 // values makes every 16-column segment the column passes move start on a 128-byte
 // boundary.
 template <typename R>
 cudaError_t launch_fft512(const R *grid, void *A1, void *A2, void *G, int ntr, int64_t pitch,
                           int H1, int P1, int hm1, int hm2, const void *tw,
-                          const int *h1_end, int nsm, cudaStream_t s) {
+                          const int *h1_end, const void *h2_band, int nsm, cudaStream_t s) {
   using C = typename Cplx<R>::T;
   const int n = 512;
   const int M2 = 2 * hm1 + 1, M3 = 2 * hm2 + 1;
@@ -433,9 +441,7 @@ cudaError_t launch_fft512(const R *grid, void *A1, void *A2, void *G, int ntr, i
   y.ncols = H1;
   y.hm = hm1;
   y.col_end = nullptr;
-  // output row hw = h2 in FFT order; FP64 only: the FP32 pass is issue-bound
-  // enough that the per-row test cost more than the writes it saved (measured)
-  y.row_col_end = sizeof(R) == 8 ? h1_end : nullptr;
+  y.blk_rows = static_cast<const short2 *>(h2_band);  // per 16-column block of h1
   auto cols = [&](const void *src, void *dst, const ColPass &cp) {
     k_fft512_cols<R><<<nsm * cta, 32 * COLS, sm, s>>>((const C *)src, (C *)dst, cp,
                                                       (const C *)tw);
@@ -455,15 +461,15 @@ cudaError_t launch_fft512(const R *grid, void *A1, void *A2, void *G, int ntr, i
   z.ncols = H1;
   z.hm = hm2;
   z.col_end = h1_end;  // plane p = h2 in FFT order
-  z.row_col_end = nullptr;
+  z.blk_rows = nullptr;
   cols(A2, G, z);
   return cudaGetLastError();
 }
 template cudaError_t launch_fft512<float>(const float *, void *, void *, void *, int, int64_t,
-                                          int, int, int, int, const void *, const int *, int,
-                                          cudaStream_t);
+                                          int, int, int, int, const void *, const int *,
+                                          const void *, int, cudaStream_t);
 template cudaError_t launch_fft512<double>(const double *, void *, void *, void *, int, int64_t,
-                                           int, int, int, int, const void *, const int *, int,
-                                           cudaStream_t);
+                                           int, int, int, int, const void *, const int *,
+                                           const void *, int, cudaStream_t);
 
 }  // namespace sqn

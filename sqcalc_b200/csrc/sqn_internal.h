@@ -160,7 +160,7 @@ void fft512_twiddles(std::vector<double> &tw);  // the passes' table, interleave
 template <typename R>
 cudaError_t launch_fft512(const R *grid, void *A1, void *A2, void *G, int ntr, int64_t pitch,
                           int H1, int P1, int hm1, int hm2, const void *tw, const int *h1_end,
-                          int nsm, cudaStream_t s);
+                          const void *h2_band, int nsm, cudaStream_t s);
 
 // Density amplitudes of requested lattice points from the half spectra.
 template <typename R>
